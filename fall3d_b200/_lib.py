@@ -1,0 +1,101 @@
+"""ctypes binding of libfall3d_ads.so (the C ABI declared in include/fall3d_ads.h).
+
+The library is built in-tree by fall3d_b200/build.py.  There is no fallback:
+if the shared library is missing or cannot be loaded, importing the binding
+raises, so nothing silently runs on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfall3d_ads.so")
+
+# Every function the header declares, with its ctypes signature.
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+
+
+class F3DDims(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nbins", C.c_int)]
+
+
+class F3DEnsMember(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("grid_class", C.c_int),
+                ("wind_factor", C.c_double)]
+
+
+SIGNATURES = {
+    "f3d_ads_create": [C.POINTER(F3DDims), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)],
+    "f3d_ads_destroy": [_vp],
+    "f3d_last_error": [C.c_char_p, C.c_int],
+    "f3d_ads_set_grid": [_vp] + [_dp] * 9,
+    "f3d_ads_set_meteo": [_vp] + [_dp] * 7 + [C.c_double, C.c_double],
+    "f3d_ads_set_source": [_vp, C.c_int, _ip, _dp],
+    "f3d_ads_set_source_dense": [_vp, _dp],
+    "f3d_ads_upload_state": [_vp, _dp, _dp],
+    "f3d_ads_download_state": [_vp, _dp, _dp],
+    "f3d_ads_step": [_vp, C.c_double, C.c_double, C.c_int, _dp],
+    "f3d_ads_step_async": [_vp, C.c_double, C.c_double, C.c_int],
+    "f3d_ads_get_fluxes": [_vp, _dp],
+    "f3d_ads_synchronize": [_vp],
+    "f3d_ads_get_stream": [_vp, C.POINTER(_vp)],
+    "f3d_ads_update_vcomps": [_vp, C.c_double],
+    "f3d_ads_solve_along_x": [_vp, C.c_double, _dp, _dp],
+    "f3d_ads_solve_along_y": [_vp, C.c_double, _dp, _dp],
+    "f3d_ads_solve_along_z": [_vp, C.c_double, C.c_double, _dp, _dp],
+    "f3d_ads_add_source": [_vp, C.c_double],
+    "f3d_ads_get_time_step": [_vp, C.c_double, C.c_int, C.c_double, C.c_double, _dp, _dp],
+    "f3d_ads_mass_volume": [_vp, _dp, _dp],
+    "f3d_ads_mass_boundaries": [_dp, _dp, _dp],
+    "f3d_vset_points": [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip],
+    "f3d_ads_compute_vset": [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_double, _dp],
+    "f3d_host_alloc": [C.c_size_t, C.POINTER(_vp)],
+    "f3d_host_free": [_vp],
+}
+
+_lib = None
+
+
+class F3DError(RuntimeError):
+    pass
+
+
+class F3DNoConvergence(F3DError):
+    """Settling-velocity iteration did not converge (MY_ERR%flag = 2)."""
+
+
+def lib():
+    """Load libfall3d_ads.so; raises if it is absent (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m fall3d_b200.build` "
+                "(nvcc, sm_100a). The FALL3D ADS step has no CPU fallback.")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue  # optional entry points resolved lazily by callers
+            fn.argtypes = args
+            fn.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().f3d_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, what: str = "") -> int:
+    if rc == 0:
+        return rc
+    msg = last_error()
+    if rc == 2:
+        raise F3DNoConvergence(f"{what}: {msg}")
+    raise F3DError(f"{what}: {msg}")

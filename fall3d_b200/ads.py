@@ -1,0 +1,203 @@
+"""Python host mirror of the reference's ADS operator interface on top of the
+C ABI (libfall3d_ads.so).  Names and argument meaning follow mod_ADS /
+mod_F3D / mod_Grid / mod_Phys so a FALL3D user finds the same entry points:
+
+  Domain(...)                       ADS_initialize        mod_ADS.F90:98
+  Domain.ADS_update_horizontal_vcomps                     mod_ADS.F90:187
+  Domain.ADS_solve_along_x/y/z                            mod_ADS.F90:233/422/612
+  Domain.F3D_time_step                                    mod_F3D.F90:1397
+  Domain.grid_get_time_step                               mod_Grid.F90:1026
+  Domain.grid_get_mass_volume                             mod_Grid.F90:1340
+  Domain.phys_get_vset                                    mod_Phys.F90:673
+  phys_get_vset_point (batched)                           mod_Phys.F90:757
+  Domain.close()                    ADS_release           mod_ADS.F90:208
+
+Arrays are numpy float64 in the reference (Fortran, halo-inclusive) layouts.
+Errors raise F3DError; a settling-velocity non-convergence raises
+F3DNoConvergence (the reference's MY_ERR%flag = 2).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import F3DDims, F3DError, F3DNoConvergence, check, lib
+from .grid import ArakawaCGrid
+
+PREC_FP64, PREC_FP32 = 0, 1
+_dp = C.POINTER(C.c_double)
+
+
+def _p(a):
+    if a is None:
+        return None
+    if not (a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim <= 1)):
+        raise F3DError("arrays must be Fortran-contiguous float64")
+    return a.ctypes.data_as(_dp)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class Domain:
+    """One model domain on one GPU (an f3d_ctx)."""
+
+    def __init__(self, grid: ArakawaCGrid, nbins: int, limiter: int = 2, time_marching: int = 2,
+                 precision: int = PREC_FP64, device: int = 0):
+        self.grid = grid
+        self.nbins = nbins
+        self.precision = precision
+        dims = F3DDims(grid.nx, grid.ny, grid.nz, nbins)
+        h = C.c_void_p()
+        check(lib().f3d_ads_create(C.byref(dims), limiter, time_marching, precision, device,
+                                   C.byref(h)), "f3d_ads_create")
+        self._h = h
+        self._keep = [np.ascontiguousarray(getattr(grid, n), dtype=np.float64) for n in
+                      ("dX1_p", "dX1_b", "dX2_p", "dX2_b", "dX3_p", "dX3_b", "Hm1_p", "Hm2_p")]
+        self._keep.append(np.asfortranarray(grid.Hm3_p, dtype=np.float64))
+        check(lib().f3d_ads_set_grid(self._h, *[_p(a) for a in self._keep]), "f3d_ads_set_grid")
+        self.fluxes = np.zeros(6)  # {W,E,S,N,U,D}
+
+    # ---- lifetime
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().f3d_ads_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- inputs
+    def set_meteo(self, u12, v12, w12, k1, k2, k3, vs, t_its, t_ite):
+        check(lib().f3d_ads_set_meteo(self._h, _p(u12), _p(v12), _p(w12), _p(k1), _p(k2), _p(k3),
+                                      _p(vs), float(t_its), float(t_ite)), "f3d_ads_set_meteo")
+
+    def set_source(self, ijk, vals):
+        ijk = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
+        vals = np.ascontiguousarray(vals, dtype=np.float64).reshape(-1, self.nbins)
+        check(lib().f3d_ads_set_source(self._h, len(ijk), _ip(ijk), vals.ctypes.data_as(_dp)),
+              "f3d_ads_set_source")
+
+    def set_source_dense(self, my_s):
+        check(lib().f3d_ads_set_source_dense(self._h, _p(my_s)), "f3d_ads_set_source_dense")
+
+    def upload_state(self, my_c=None, my_acum=None):
+        check(lib().f3d_ads_upload_state(self._h, _p(my_c), _p(my_acum)), "f3d_ads_upload_state")
+
+    def download_state(self, my_c=None, my_acum=None):
+        g = self.grid
+        if my_c is None:
+            my_c = np.zeros((g.nx + 4, g.ny + 4, g.nz + 4, self.nbins), order="F")
+        if my_acum is None:
+            my_acum = np.zeros((g.nx + 4, g.ny + 4, self.nbins), order="F")
+        check(lib().f3d_ads_download_state(self._h, _p(my_c), _p(my_acum)), "f3d_ads_download_state")
+        return my_c, my_acum
+
+    # ---- step
+    def F3D_time_step(self, dt, time, iiter, fluxes=None):
+        f = self.fluxes if fluxes is None else fluxes
+        check(lib().f3d_ads_step(self._h, float(dt), float(time), int(iiter), _p(f)), "f3d_ads_step")
+        return f
+
+    def step_async(self, dt, time, iiter):
+        check(lib().f3d_ads_step_async(self._h, float(dt), float(time), int(iiter)),
+              "f3d_ads_step_async")
+
+    def get_fluxes(self, fluxes=None):
+        f = self.fluxes if fluxes is None else fluxes
+        check(lib().f3d_ads_get_fluxes(self._h, _p(f)), "f3d_ads_get_fluxes")
+        return f
+
+    def synchronize(self):
+        check(lib().f3d_ads_synchronize(self._h), "f3d_ads_synchronize")
+
+    @property
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        check(lib().f3d_ads_get_stream(self._h, C.byref(s)), "f3d_ads_get_stream")
+        return s.value or 0
+
+    def ADS_update_horizontal_vcomps(self, stime):
+        check(lib().f3d_ads_update_vcomps(self._h, float(stime)), "f3d_ads_update_vcomps")
+
+    def ADS_solve_along_x(self, dt, W=0.0, E=0.0):
+        a, b = C.c_double(W), C.c_double(E)
+        check(lib().f3d_ads_solve_along_x(self._h, float(dt), C.byref(a), C.byref(b)),
+              "f3d_ads_solve_along_x")
+        return a.value, b.value
+
+    def ADS_solve_along_y(self, dt, S=0.0, N=0.0):
+        a, b = C.c_double(S), C.c_double(N)
+        check(lib().f3d_ads_solve_along_y(self._h, float(dt), C.byref(a), C.byref(b)),
+              "f3d_ads_solve_along_y")
+        return a.value, b.value
+
+    def ADS_solve_along_z(self, dt, stime, D=0.0, U=0.0):
+        a, b = C.c_double(D), C.c_double(U)
+        check(lib().f3d_ads_solve_along_z(self._h, float(dt), float(stime), C.byref(a), C.byref(b)),
+              "f3d_ads_solve_along_z")
+        return a.value, b.value
+
+    def add_source(self, dt):
+        check(lib().f3d_ads_add_source(self._h, float(dt)), "f3d_ads_add_source")
+
+    # ---- diagnostics
+    def grid_get_time_step(self, stime, criterion=2, cfl=0.9, run_end=1e30):
+        a, b = C.c_double(), C.c_double()
+        check(lib().f3d_ads_get_time_step(self._h, float(stime), int(criterion), float(cfl),
+                                          float(run_end), C.byref(a), C.byref(b)),
+              "f3d_ads_get_time_step")
+        return a.value, b.value
+
+    def grid_get_mass_volume(self, per_bin=False):
+        m = C.c_double()
+        pb = np.zeros(self.nbins)
+        check(lib().f3d_ads_mass_volume(self._h, C.byref(m), _p(pb)), "f3d_ads_mass_volume")
+        return (m.value, pb) if per_bin else m.value
+
+    def phys_get_vset(self, model, rhoc, tc, diam, rhop, psi, bin_cat, is_aggregate=None,
+                      vset_fac=1.0, want_host=False):
+        g = self.grid
+        vs = np.zeros((g.nx, g.ny, g.nz + 3, self.nbins), order="F") if want_host else None
+        cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
+        agg = None if is_aggregate is None else np.ascontiguousarray(is_aggregate, dtype=np.int32)
+        rc = lib().f3d_ads_compute_vset(
+            self._h, int(model), _p(np.asfortranarray(rhoc, dtype=np.float64)),
+            _p(np.asfortranarray(tc, dtype=np.float64)), _p(np.ascontiguousarray(diam, np.float64)),
+            _p(np.ascontiguousarray(rhop, np.float64)), _p(np.ascontiguousarray(psi, np.float64)),
+            _ip(cat), _ip(agg), float(vset_fac), _p(vs))
+        check(rc, "f3d_ads_compute_vset")
+        return vs
+
+
+def grid_get_mass_boundaries(fluxes):
+    g, l = C.c_double(), C.c_double()
+    check(lib().f3d_ads_mass_boundaries(_p(np.asarray(fluxes, dtype=np.float64)), C.byref(g),
+                                        C.byref(l)), "f3d_ads_mass_boundaries")
+    return g.value, l.value
+
+
+def phys_get_vset_point(diam, rhop, psi, rhoa, visc, model=2, want_iters=False):
+    """Batched phys_get_vset_point on the GPU.  Returns (vset, flags[, iters])."""
+    arrs = [np.ascontiguousarray(np.broadcast_to(a, np.broadcast(diam, rhop, psi, rhoa, visc).shape),
+                                 dtype=np.float64).ravel() for a in (diam, rhop, psi, rhoa, visc)]
+    n = arrs[0].size
+    out = np.zeros(n)
+    flags = np.zeros(n, dtype=np.int32)
+    iters = np.zeros(n, dtype=np.int32)
+    rc = lib().f3d_vset_points(int(model), n, *[a.ctypes.data_as(_dp) for a in arrs],
+                               out.ctypes.data_as(_dp), _ip(flags), _ip(iters))
+    if rc not in (0, 2):
+        check(rc, "f3d_vset_points")
+    return (out, flags, iters) if want_iters else (out, flags)

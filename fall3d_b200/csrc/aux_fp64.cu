@@ -1,0 +1,499 @@
+// aux_fp64.cu -- FP64 kernels around the sweeps: layout conversion of the
+// reference arrays, per-step parameters, boundary-flux reduction, the CFL
+// reduction, the mass budget and the settling-velocity solve.  Compiled with
+// --fmad=false: every expression keeps the reference's rounding.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "f3d_common.cuh"
+
+namespace f3d {
+
+#define GRID_STRIDE(e, total)                                                  \
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (total); \
+       e += (long long)gridDim.x * blockDim.x)
+
+// ---- reference layout -> device layout ------------------------------------
+// u (ibs-1:ibe+1, jps:jpe, kps:kpe, 2) -> ux[s][k][f=0..nx][j]
+__global__ void k_conv_u(const double* __restrict__ in, double* __restrict__ out, int nx, int ny,
+                         int nz) {
+  const long long tot = 2LL * nz * (nx + 1) * ny;
+  GRID_STRIDE(e, tot) {
+    int j = (int)(e % ny);
+    long long t = e / ny;
+    int f = (int)(t % (nx + 1));
+    t /= (nx + 1);
+    int k = (int)(t % nz);
+    int s = (int)(t / nz);
+    out[e] = in[(f + 1) + (long long)(nx + 3) * (j + (long long)ny * (k + (long long)nz * s))];
+  }
+}
+// v (jbs-1:jbe+1, ips:ipe, kps:kpe, 2) -> vy[s][k][f=0..ny][i]
+__global__ void k_conv_v(const double* __restrict__ in, double* __restrict__ out, int nx, int ny,
+                         int nz) {
+  const long long tot = 2LL * nz * (ny + 1) * nx;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int f = (int)(t % (ny + 1));
+    t /= (ny + 1);
+    int k = (int)(t % nz);
+    int s = (int)(t / nz);
+    out[e] = in[(f + 1) + (long long)(ny + 3) * (i + (long long)nx * (k + (long long)nz * s))];
+  }
+}
+// w (kbs-1:kbe+1, ips:ipe, jps:jpe, 2) -> wz[s][f=0..nz][j][i]
+__global__ void k_conv_w(const double* __restrict__ in, double* __restrict__ out, int nx, int ny,
+                         int nz) {
+  const long long tot = 2LL * (nz + 1) * ny * nx;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    t /= ny;
+    int f = (int)(t % (nz + 1));
+    int s = (int)(t / (nz + 1));
+    out[e] = in[(f + 1) + (long long)(nz + 3) * (i + (long long)nx * (j + (long long)ny * s))];
+  }
+}
+// k1 (ips-2:ipe+2, jps:jpe, kps:kpe) -> k1x[k][p=-1..nx][j]
+__global__ void k_conv_k1(const double* __restrict__ in, double* __restrict__ out, int nx, int ny,
+                          int nz) {
+  const long long tot = (long long)nz * (nx + 2) * ny;
+  GRID_STRIDE(e, tot) {
+    int j = (int)(e % ny);
+    long long t = e / ny;
+    int p1 = (int)(t % (nx + 2));
+    int k = (int)(t / (nx + 2));
+    out[e] = in[(p1 + 1) + (long long)(nx + 4) * (j + (long long)ny * k)];
+  }
+}
+// k2 (jps-2:jpe+2, ips:ipe, kps:kpe) -> k2y[k][p=-1..ny][i]
+__global__ void k_conv_k2(const double* __restrict__ in, double* __restrict__ out, int nx, int ny,
+                          int nz) {
+  const long long tot = (long long)nz * (ny + 2) * nx;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int p1 = (int)(t % (ny + 2));
+    int k = (int)(t / (ny + 2));
+    out[e] = in[(p1 + 1) + (long long)(ny + 4) * (i + (long long)nx * k)];
+  }
+}
+// k3 (kps-2:kpe+2, ips:ipe, jps:jpe) -> k3z[p=-1..nz][j][i]
+__global__ void k_conv_k3(const double* __restrict__ in, double* __restrict__ out, int nx, int ny,
+                          int nz) {
+  const long long tot = (long long)(nz + 2) * ny * nx;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    int p1 = (int)(t / ny);
+    out[e] = in[(p1 + 1) + (long long)(nz + 4) * (i + (long long)nx * j)];
+  }
+}
+// vs (ips:ipe, jps:jpe, kbs-1:kbe+1, nb) -> vs[b][f=0..nz][j][i]
+__global__ void k_conv_vs(const double* __restrict__ in, double* __restrict__ out, int nx, int ny,
+                          int nz, int nb) {
+  const long long tot = (long long)nb * (nz + 1) * ny * nx;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    t /= ny;
+    int f = (int)(t % (nz + 1));
+    int b = (int)(t / (nz + 1));
+    out[e] = in[i + (long long)nx * (j + (long long)ny * ((f + 1) + (long long)(nz + 3) * b))];
+  }
+}
+// c (ips-2:ipe+2, jps-2:jpe+2, kps-2:kpe+2, nb) -> c[b][k][j][i]
+__global__ void k_conv_c_in(const double* __restrict__ in, double* __restrict__ out, int nx,
+                            int ny, int nz, int nb) {
+  const long long tot = (long long)nb * nz * ny * nx;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    t /= ny;
+    int k = (int)(t % nz);
+    int b = (int)(t / nz);
+    out[e] = in[(i + 2) + (long long)(nx + 4) *
+                              ((j + 2) + (long long)(ny + 4) * ((k + 2) + (long long)(nz + 4) * b))];
+  }
+}
+// acum (ips-2:ipe+2, jps-2:jpe+2, nb) -> acum[b][j][i]
+__global__ void k_conv_acum_in(const double* __restrict__ in, double* __restrict__ out, int nx,
+                               int ny, int nb) {
+  const long long tot = (long long)nb * ny * nx;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    int b = (int)(t / ny);
+    out[e] = in[(i + 2) + (long long)(nx + 4) * ((j + 2) + (long long)(ny + 4) * b)];
+  }
+}
+// device settling velocity [b][f][j][i] -> reference layout with the halo faces
+__global__ void k_conv_vs_out(const double* __restrict__ in, double* __restrict__ out, int nx,
+                              int ny, int nz, int nb) {
+  const long long tot = (long long)nb * (nz + 3) * ny * nx;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    t /= ny;
+    int f1 = (int)(t % (nz + 3));
+    int b = (int)(t / (nz + 3));
+    int f = f1 - 1;
+    if (f < 0) f = 0;
+    if (f > nz) f = nz;
+    out[e] = in[(((long long)b * (nz + 1) + f) * ny + j) * nx + i];
+  }
+}
+
+void launch_conv(int which, const double* in, double* out, int nx, int ny, int nz, int nb,
+                 cudaStream_t st) {
+  dim3 g(2048), b(256);
+  switch (which) {
+    case 0: k_conv_u<<<g, b, 0, st>>>(in, out, nx, ny, nz); break;
+    case 1: k_conv_v<<<g, b, 0, st>>>(in, out, nx, ny, nz); break;
+    case 2: k_conv_w<<<g, b, 0, st>>>(in, out, nx, ny, nz); break;
+    case 3: k_conv_k1<<<g, b, 0, st>>>(in, out, nx, ny, nz); break;
+    case 4: k_conv_k2<<<g, b, 0, st>>>(in, out, nx, ny, nz); break;
+    case 5: k_conv_k3<<<g, b, 0, st>>>(in, out, nx, ny, nz); break;
+    case 6: k_conv_vs<<<g, b, 0, st>>>(in, out, nx, ny, nz, nb); break;
+    case 7: k_conv_c_in<<<g, b, 0, st>>>(in, out, nx, ny, nz, nb); break;
+    case 8: k_conv_acum_in<<<g, b, 0, st>>>(in, out, nx, ny, nb); break;
+    case 9: k_conv_vs_out<<<g, b, 0, st>>>(in, out, nx, ny, nz, nb); break;
+    default: break;
+  }
+}
+
+// ---- per-step parameters (kernel arguments are captured at launch) -------
+__global__ void k_set_step(MemberDev* members, int mi, double dt, double time, int iiter) {
+  MemberDev& m = members[mi];
+  m.dt = dt;
+  m.time = time;
+  m.iiter = iiter;
+  m.stime = (time - m.t_its) / (m.t_ite - m.t_its);  // mod_F3D.F90:1437
+}
+__global__ void k_set_dt_stime(MemberDev* members, int mi, double dt, double stime) {
+  members[mi].dt = dt;
+  members[mi].stime = stime;
+}
+void launch_set_step(MemberDev* members, int mi, double dt, double time, int iiter,
+                     cudaStream_t st) {
+  k_set_step<<<1, 1, 0, st>>>(members, mi, dt, time, iiter);
+}
+void launch_set_dt_stime(MemberDev* members, int mi, double dt, double stime, cudaStream_t st) {
+  k_set_dt_stime<<<1, 1, 0, st>>>(members, mi, dt, stime);
+}
+
+// ---- boundary flux reduction: one block per member ------------------------
+// partial slots of each direction are summed pairwise; the step increments go
+// to flux_step {W,E,S,N,U,D} and are added to the running totals with a
+// Kahan-compensated update.
+__global__ void k_flux_reduce(const MemberDev* __restrict__ members, int dirmask) {
+  const MemberDev& m = members[blockIdx.x];
+  __shared__ double sa[256], sb[256];
+  double res[6] = {0, 0, 0, 0, 0, 0};
+  for (int d = 0; d < 3; ++d) {
+    if (!(dirmask & (1 << d))) continue;
+    double a = 0.0, b = 0.0;
+    const double* p = m.flux_part + 2LL * m.part_base[d];
+    // strided first pass: thread t sums slots t, t+256, ... in order
+    for (int s = threadIdx.x; s < m.part_count[d]; s += blockDim.x) {
+      a = a + p[2 * s];
+      b = b + p[2 * s + 1];
+    }
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) {
+        sa[threadIdx.x] = sa[threadIdx.x] + sa[threadIdx.x + s];
+        sb[threadIdx.x] = sb[threadIdx.x] + sb[threadIdx.x + s];
+      }
+      __syncthreads();
+    }
+    // x -> (W,E) = 0,1 ; y -> (S,N) = 2,3 ; z -> (D,U) = 5,4
+    if (d == 0) { res[0] = sa[0]; res[1] = sb[0]; }
+    if (d == 1) { res[2] = sa[0]; res[3] = sb[0]; }
+    if (d == 2) { res[5] = sa[0]; res[4] = sb[0]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 6; ++q) {
+      bool on = (q < 2) ? (dirmask & 1) : (q < 4) ? (dirmask & 2) : (dirmask & 4);
+      if (!on) continue;
+      m.flux_step[q] = res[q];
+      // Kahan: tot[q] + comp[q]
+      double y = res[q] - m.flux_tot[6 + q];
+      double t = m.flux_tot[q] + y;
+      m.flux_tot[6 + q] = (t - m.flux_tot[q]) - y;
+      m.flux_tot[q] = t;
+    }
+  }
+}
+__global__ void k_zero_step(const MemberDev* __restrict__ members) {
+  const MemberDev& m = members[blockIdx.x];
+  if (threadIdx.x < 6) m.flux_step[threadIdx.x] = 0.0;
+}
+void launch_flux_reduce(const MemberDev* members, int nmembers, int dirmask, cudaStream_t st) {
+  k_flux_reduce<<<nmembers, 256, 0, st>>>(members, dirmask);
+}
+void launch_zero_step(const MemberDev* members, int nmembers, cudaStream_t st) {
+  k_zero_step<<<nmembers, 32, 0, st>>>(members);
+}
+
+// ---- CFL: grid_get_time_step (mod_Grid.F90:1026-1141) -----------------------
+// Non-negative doubles order like their bit patterns, so an integer atomicMax
+// gives the exact maximum independently of the reduction order.
+__device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void k_cfl(const MemberDev* __restrict__ members, int mi, double s, int criterion,
+                      double* out3) {
+  const MemberDev& m = members[mi];
+  const int nx = m.nx, ny = m.ny, nz = m.nz, nb = m.nb;
+  const long long tot = (long long)nx * ny * nz;
+  double d1 = 0.0, d2 = 0.0, d3 = 0.0;
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    int k = (int)(t / ny);
+    long long iu = ((long long)k * (nx + 1) + i) * ny + j;
+    long long iv = ((long long)k * (ny + 1) + j) * nx + i;
+    long long iw = ((long long)k * ny + j) * nx + i;
+    double u = (1.0 - s) * m.ux[0][iu] + s * m.ux[1][iu];
+    double v = (1.0 - s) * m.vy[0][iv] + s * m.vy[1][iv];
+    double w = (1.0 - s) * m.wz[0][iw] + s * m.wz[1][iw];
+    double k1 = m.k1x[((long long)k * (nx + 2) + (i + 1)) * ny + j];
+    double k2 = m.k2y[((long long)k * (ny + 2) + (j + 1)) * nx + i];
+    double k3 = m.k3z[((long long)(k + 1) * ny + j) * nx + i];
+    double w_max = -INFINITY;
+    for (int b = 0; b < nb; ++b)
+      w_max = fmax(w_max, fabs(w - m.vs[(((long long)b * (nz + 1) + k) * ny + j) * nx + i]));
+    double dx = m.dx1p[i + 2], dy = m.dx2p[j + 2], dz = m.dx3p[k + 2];
+    if (criterion == 1) {
+      d1 = fmax(d1, 2.0 * k1 / (dx * dx) + fabs(u) / dx);
+      d2 = fmax(d2, 2.0 * k2 / (dy * dy) + fabs(v) / dy);
+      d3 = fmax(d3, 2.0 * k3 / (dz * dz) + w_max / dz);
+    } else {
+      double dtinv = 2.0 * k1 / (dx * dx) + fabs(u) / dx + 2.0 * k2 / (dy * dy) + fabs(v) / dy +
+                     2.0 * k3 / (dz * dz) + w_max / dz;
+      d1 = fmax(d1, dtinv);
+    }
+  }
+  // warp max then atomics
+  for (int o = 16; o > 0; o >>= 1) {
+    d1 = fmax(d1, __shfl_xor_sync(0xffffffffu, d1, o));
+    d2 = fmax(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+    d3 = fmax(d3, __shfl_xor_sync(0xffffffffu, d3, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(out3 + 0, d1);
+    atomic_max_pos(out3 + 1, d2);
+    atomic_max_pos(out3 + 2, d3);
+  }
+}
+void launch_cfl(const MemberDev* members, int mi, double s, int criterion, double* out3,
+                cudaStream_t st) {
+  k_cfl<<<1184, 256, 0, st>>>(members, mi, s, criterion, out3);
+}
+
+// ---- mass in the volume: grid_get_mass_volume (mod_Grid.F90:1340-1389) ------
+// per bin: pairwise block sums into partials[b][block], then a second pass.
+__global__ void k_mass_partial(const MemberDev* __restrict__ members, int mi, int fp32,
+                               double* partials) {
+  const MemberDev& m = members[mi];
+  const int nx = m.nx, ny = m.ny, nz = m.nz;
+  const long long ncell = (long long)nx * ny * nz;
+  const int b = blockIdx.y;
+  __shared__ double sm[256];
+  double acc = 0.0, comp = 0.0;  // Neumaier compensated
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < ncell;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    int k = (int)(t / ny);
+    double c = fp32 ? (double)m.c32[(long long)b * ncell + e] : m.c64[(long long)b * ncell + e];
+    double x = c * m.dx1p[i + 2] * m.dx2p[j + 2] * m.dx3p[k + 2];
+    double tt = acc + x;
+    if (fabs(acc) >= fabs(x)) comp += (acc - tt) + x; else comp += (x - tt) + acc;
+    acc = tt;
+  }
+  sm[threadIdx.x] = acc + comp;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[(long long)b * gridDim.x + blockIdx.x] = sm[0];
+}
+__global__ void k_mass_final(const double* partials, int nblk, int nb, double* out) {
+  __shared__ double sm[256];
+  for (int b = 0; b < nb; ++b) {
+    double acc = 0.0, comp = 0.0;
+    for (int s = threadIdx.x; s < nblk; s += blockDim.x) {
+      double x = partials[(long long)b * nblk + s];
+      double tt = acc + x;
+      if (fabs(acc) >= fabs(x)) comp += (acc - tt) + x; else comp += (x - tt) + acc;
+      acc = tt;
+    }
+    sm[threadIdx.x] = acc + comp;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) sm[threadIdx.x] = sm[threadIdx.x] + sm[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[b] = sm[0];
+    __syncthreads();
+  }
+}
+void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* partials, int nblk,
+                 double* out, cudaStream_t st) {
+  dim3 g(nblk, nb);
+  k_mass_partial<<<g, 256, 0, st>>>(members, mi, fp32, partials);
+  k_mass_final<<<1, 256, 0, st>>>(partials, nblk, nb, out);
+}
+
+// ---- settling velocity: phys_get_vset_point (mod_Phys.F90:757-954) -----------
+__device__ int vset_point_dev(double diam, double rhop, double psi, double rhoa, double visc,
+                              int model, double* vset_out, int* iters) {
+  const double GI = 9.81, atol = 1e-12, rtol = 1e-6;
+  const int maxit = 1000;
+  double cd = 1.0, vset = 0.0, vold, rey;
+  *iters = 0;
+  if (model == 4) {  // Dellino: closed form
+    double d3 = diam * diam * diam;
+    vset = pow(d3 * GI * rhop * rhoa * pow(psi, 1.6) / (visc * visc), 0.5206);
+    vset = 1.2065 * visc * vset / (diam * rhoa);
+    *vset_out = vset;
+    return 0;
+  }
+  if (model < 1 || model > 7) {
+    *vset_out = 0.0;
+    return 1;
+  }
+  double rk1 = 0, rk2 = 0, cd100 = 0, a = 0, b = 0;
+  if (model == 2) {
+    rk1 = 3.0 / (1.0 + 2.0 / sqrt(psi));
+    rk2 = pow(10.0, 1.8148 * pow(-log10(psi), 0.5743));
+  }
+  if (model == 5) {
+    cd100 = 0.24 * pow(psi, -0.828) + 2.0 * sqrt(1.07 - psi);
+    a = (1.0 - cd100) / 900.0;
+    b = 1.0 - 1000.0 * a;
+  }
+  vset = sqrt(4.0 * GI * diam * rhop / (3.0 * cd * rhoa));
+  vold = vset;
+  for (int it = 1; it <= maxit; ++it) {
+    rey = rhoa * vset * diam / visc;
+    switch (model) {
+      case 1:
+        if (rey <= 988.947) cd = 24.0 / rey * (1.0 + 0.15 * pow(rey, 0.687));
+        else cd = 0.44;
+        break;
+      case 2:
+        cd = 24.0 / (rey * rk1) * (1.0 + 0.1118 * pow(rey * rk1 * rk2, 0.6567)) +
+             0.4305 * rk2 / (1.0 + 3305.0 / (rey * rk1 * rk2));
+        break;
+      case 3:
+        cd = 24.0 / rey * pow(psi, -0.828) + 2.0 * sqrt(1.07 - psi);
+        break;
+      case 5:
+        if (rey <= 100.0) cd = 24.0 / rey * pow(psi, -0.828) + 2.0 * sqrt(1.07 - psi);
+        else if (rey > 100.0 && rey < 1000.0) cd = a * rey + b;
+        else cd = 1.0;
+        break;
+      case 6:
+        cd = 24.0 * (1.0 + 0.15 * pow(rey, 0.687)) / rey + 0.42 / (1.0 + 42500.0 / pow(rey, 1.16));
+        cd = 0.74533 * pow(rey, 0.146012) * cd / pow(psi, 0.5134 / pow(fmax(rey, 0.01), 0.2));
+        break;
+      case 7:
+        cd = 24.0 / rey * (pow((1.0 - psi) / rey + 1.0, 0.25) +
+                           (0.1806 * pow(rey, 0.6459)) * pow(psi, -pow(rey, 0.08))) +
+             0.4251 / (1.0 + 6880.95 / rey * pow(psi, 5.03));
+        break;
+    }
+    vset = sqrt(4.0 * GI * diam * rhop / (3.0 * cd * rhoa));
+    *iters = it;
+    if (fabs(vset - vold) <= atol + rtol * fabs(vset)) {
+      *vset_out = vset;
+      return 0;
+    }
+    vold = vset;
+  }
+  *vset_out = vset;
+  return 2;
+}
+
+__global__ void k_vset_points(int model, int n, const double* diam, const double* rhop,
+                              const double* psi, const double* rhoa, const double* visc,
+                              double* vset, int* flags, int* iters, int* nfail) {
+  GRID_STRIDE(q, (long long)n) {
+    int it;
+    double v;
+    int fl = vset_point_dev(diam[q], rhop[q], psi[q], rhoa[q], visc[q], model, &v, &it);
+    vset[q] = v;
+    flags[q] = fl;
+    if (iters) iters[q] = it;
+    if (fl) atomicAdd(nfail, 1);
+  }
+}
+void launch_vset_points(int model, int n, const double* diam, const double* rhop,
+                        const double* psi, const double* rhoa, const double* visc, double* vset,
+                        int* flags, int* iters, int* nfail, cudaStream_t st) {
+  k_vset_points<<<592, 128, 0, st>>>(model, n, diam, rhop, psi, rhoa, visc, vset, flags, iters,
+                                      nfail);
+}
+
+// phys_get_vset (mod_Phys.F90:673-740) + vs/Hm3 (mod_Grid.F90:996-1005).
+// rhoc, tc corners (nx+1)(ny+1)(nz+1), i fastest.  bins: [diam, rhop, psi]
+// in bin_par[3*b..], bin_flags[b] = cat | (aggregate << 8).
+__global__ void k_vset_field(MemberDev* members, int mi, int model, const double* rhoc,
+                             const double* tc, const double* bin_par, const int* bin_flags,
+                             double vset_fac, int* nfail) {
+  const MemberDev& m = members[mi];
+  const int nx = m.nx, ny = m.ny, nz = m.nz, nb = m.nb;
+  const long long cx = nx + 1, cy = ny + 1;
+  const long long tot = (long long)(nz + 1) * ny * nx * nb;
+  double* vs = const_cast<double*>(m.vs);
+  GRID_STRIDE(e, tot) {
+    int i = (int)(e % nx);
+    long long t = e / nx;
+    int j = (int)(t % ny);
+    t /= ny;
+    int k = (int)(t % (nz + 1));
+    int b = (int)(t / (nz + 1));
+#define CO(a, ii, jj) a[(ii) + cx * ((jj) + cy * (long long)k)]
+    double rhoa = 0.25 * (CO(rhoc, i, j) + CO(rhoc, i + 1, j) + CO(rhoc, i + 1, j + 1) + CO(rhoc, i, j + 1));
+    double ta = 0.25 * (CO(tc, i, j) + CO(tc, i + 1, j) + CO(tc, i + 1, j + 1) + CO(tc, i, j + 1));
+#undef CO
+    double visa = 1.827e-5 * ((291.15 + 120.0) / (ta + 120.0)) * pow(ta / 291.15, 1.5);
+    int fl = bin_flags[b];
+    double v = 0.0;
+    if ((fl & 0xff) != 2) {
+      int it;
+      int f = vset_point_dev(bin_par[3 * b], bin_par[3 * b + 1], bin_par[3 * b + 2], rhoa, visa,
+                             model, &v, &it);
+      if (f) atomicAdd(nfail, 1);
+    }
+    if (fl >> 8) v = vset_fac * v;
+    v = v / m.hm3[i + (long long)nx * j];
+    vs[(((long long)b * (nz + 1) + k) * ny + j) * nx + i] = v;
+  }
+}
+void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc,
+                       const double* tc, const double* bin_par, const int* bin_flags,
+                       double vset_fac, int* nfail, cudaStream_t st) {
+  k_vset_field<<<1184, 128, 0, st>>>(members, mi, model, rhoc, tc, bin_par, bin_flags, vset_fac,
+                                     nfail);
+}
+
+}  // namespace f3d

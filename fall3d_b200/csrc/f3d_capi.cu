@@ -1,0 +1,803 @@
+// f3d_capi.cu -- host side of libfall3d_ads.so: contexts, device buffers,
+// uploads in the reference layouts and the step sequence of F3D_time_step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fall3d_ads.h"
+#include "f3d_common.cuh"
+
+namespace f3d {
+// ads_fp64.cu
+void launch_sweep64(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
+                    int nblocks, cudaStream_t st);
+void launch_prep64(const MemberDev* members, const int* blk_member, const int* blk_first,
+                   int nblocks, int mask, cudaStream_t st);
+void launch_source64(const MemberDev* members, int nmembers, cudaStream_t st);
+// aux_fp64.cu
+void launch_conv(int which, const double* in, double* out, int nx, int ny, int nz, int nb,
+                 cudaStream_t st);
+void launch_set_step(MemberDev* members, int mi, double dt, double time, int iiter,
+                     cudaStream_t st);
+void launch_set_dt_stime(MemberDev* members, int mi, double dt, double stime, cudaStream_t st);
+void launch_flux_reduce(const MemberDev* members, int nmembers, int dirmask, cudaStream_t st);
+void launch_zero_step(const MemberDev* members, int nmembers, cudaStream_t st);
+void launch_cfl(const MemberDev* members, int mi, double s, int criterion, double* out3,
+                cudaStream_t st);
+void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* partials, int nblk,
+                 double* out, cudaStream_t st);
+void launch_vset_points(int model, int n, const double* diam, const double* rhop,
+                        const double* psi, const double* rhoa, const double* visc, double* vset,
+                        int* flags, int* iters, int* nfail, cudaStream_t st);
+void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc,
+                       const double* tc, const double* bin_par, const int* bin_flags,
+                       double vset_fac, int* nfail, cudaStream_t st);
+// ads_fp32.cu
+void launch_sweep32(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
+                    int nblocks, cudaStream_t st);
+void launch_prep32(const MemberDev* members, const int* blk_member, const int* blk_first,
+                   int nblocks, int mask, cudaStream_t st);
+void launch_source32(const MemberDev* members, int nmembers, cudaStream_t st);
+void launch_fp32_fields(MemberDev* members, int mi, cudaStream_t st);
+}  // namespace f3d
+
+using namespace f3d;
+
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int set_err(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return 1;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                     __LINE__);                                                         \
+  } while (0)
+
+#define CKL()                                                                          \
+  do {                                                                                 \
+    cudaError_t e_ = cudaGetLastError();                                               \
+    if (e_ != cudaSuccess)                                                             \
+      return set_err("kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, \
+                     __LINE__);                                                        \
+  } while (0)
+
+static const int kSweepBlock = 128;
+static const int kPrepBlock = 256;
+
+struct f3d_ctx {
+  int nx = 0, ny = 0, nz = 0, nb = 0, lim = 2, tm = 2, prec = 0, device = 0;
+  cudaStream_t st = nullptr;
+  MemberDev hm;            // host mirror of the member descriptor
+  MemberDev* dm = nullptr; // device copy
+  WorkItem* dwork[3] = {nullptr, nullptr, nullptr};
+  int nblk[3] = {0, 0, 0};
+  int* dprep_member = nullptr;
+  int* dprep_first = nullptr;
+  int nprep = 0;
+  std::vector<void*> allocs;
+  double* staging = nullptr;
+  size_t staging_elems = 0;
+  double* d_red = nullptr;    // reduction scratch (CFL 3 doubles, mass partials)
+  int mass_nblk = 148 * 2;
+  double* h_pin = nullptr;    // pinned host scratch (fluxes, reductions)
+  int* d_nfail = nullptr;
+  double t_its = 0.0, t_ite = 1.0;
+  bool grid_set = false, meteo_set = false;
+  // host copies of the grid (source volumes)
+  std::vector<double> dX1_p, dX2_p, dX3_p, Hm1_p, Hm2_p, Hm3_p;
+  int src_cap = 0;
+  double* d_rhoc_tc = nullptr;
+  size_t rhoc_cap = 0;
+};
+
+template <class T>
+static int dalloc(f3d_ctx* c, T** p, size_t n) {
+  void* q = nullptr;
+  if (n == 0) n = 1;
+  CK(cudaMalloc(&q, n * sizeof(T)));
+  c->allocs.push_back(q);
+  *p = reinterpret_cast<T*>(q);
+  return 0;
+}
+
+static int upload_member(f3d_ctx* c) {
+  CK(cudaMemcpyAsync(c->dm, &c->hm, sizeof(MemberDev), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// Build the work lists: blocks of 128 pencils per direction, one partial
+// slot per block.
+static int build_work(f3d_ctx* c) {
+  long long npen[3] = {(long long)c->ny * c->nz * c->nb, (long long)c->nx * c->nz * c->nb,
+                       (long long)c->nx * c->ny * c->nb};
+  int slot = 0;
+  for (int d = 0; d < 3; ++d) {
+    int nb = (int)((npen[d] + kSweepBlock - 1) / kSweepBlock);
+    std::vector<WorkItem> w(nb);
+    for (int q = 0; q < nb; ++q) w[q] = WorkItem{0, q * kSweepBlock, slot + q, 0};
+    c->hm.part_base[d] = slot;
+    c->hm.part_count[d] = nb;
+    slot += nb;
+    if (dalloc(c, &c->dwork[d], (size_t)nb)) return 1;
+    CK(cudaMemcpy(c->dwork[d], w.data(), sizeof(WorkItem) * nb, cudaMemcpyHostToDevice));
+    c->nblk[d] = nb;
+  }
+  if (dalloc(c, &c->hm.flux_part, 2 * (size_t)slot)) return 1;
+  long long nprep = ((long long)(c->nx + 1) * c->ny * c->nz + (long long)(c->ny + 1) * c->nx * c->nz +
+                     (long long)(c->nz + 1) * c->nx * c->ny + kPrepBlock - 1) /
+                    kPrepBlock;
+  std::vector<int> bm(nprep, 0);
+  int first = 0;
+  if (dalloc(c, &c->dprep_member, (size_t)nprep)) return 1;
+  if (dalloc(c, &c->dprep_first, 1)) return 1;
+  CK(cudaMemcpy(c->dprep_member, bm.data(), sizeof(int) * nprep, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->dprep_first, &first, sizeof(int), cudaMemcpyHostToDevice));
+  c->nprep = (int)nprep;
+  return 0;
+}
+
+extern "C" int f3d_last_error(char* buf, int len) {
+  if (!buf || len <= 0) return 1;
+  snprintf(buf, (size_t)len, "%s", g_err.c_str());
+  return 0;
+}
+
+extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marching,
+                              int precision, int device, f3d_ctx** out) {
+  if (!dims || !out) return set_err("f3d_ads_create: null argument");
+  if (dims->nx < 1 || dims->ny < 1 || dims->nz < 1 || dims->nbins < 1)
+    return set_err("f3d_ads_create: invalid dims %d %d %d %d", dims->nx, dims->ny, dims->nz,
+                   dims->nbins);
+  if (limiter < 1 || limiter > 3) return set_err("f3d_ads_create: limiter %d not in 1..3", limiter);
+  if (time_marching < 1 || time_marching > 2)
+    return set_err("f3d_ads_create: time_marching %d not in 1..2", time_marching);
+  if (precision != F3D_PREC_FP64 && precision != F3D_PREC_FP32)
+    return set_err("f3d_ads_create: precision %d unknown", precision);
+  *out = nullptr;
+  CK(cudaSetDevice(device));
+  f3d_ctx* c = new f3d_ctx();
+  c->nx = dims->nx; c->ny = dims->ny; c->nz = dims->nz; c->nb = dims->nbins;
+  c->lim = limiter; c->tm = time_marching; c->prec = precision; c->device = device;
+  memset(&c->hm, 0, sizeof(MemberDev));
+  MemberDev& m = c->hm;
+  m.nx = c->nx; m.ny = c->ny; m.nz = c->nz; m.nb = c->nb;
+  m.wfac = 1.0f;
+  const size_t nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb;
+  const size_t ncell = nx * ny * nz;
+  int rc = 0;
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return set_err("f3d_ads_create: stream creation failed");
+  }
+  double* tmp;
+  if (precision == F3D_PREC_FP64) rc |= dalloc(c, &m.c64, ncell * nb);
+  else rc |= dalloc(c, &m.c32, ncell * nb);
+  rc |= dalloc(c, &m.acum, nx * ny * nb);
+  rc |= dalloc(c, &tmp, 2 * (nx + 1) * ny * nz); m.ux[0] = tmp; m.ux[1] = tmp + (nx + 1) * ny * nz;
+  rc |= dalloc(c, &tmp, 2 * (ny + 1) * nx * nz); m.vy[0] = tmp; m.vy[1] = tmp + (ny + 1) * nx * nz;
+  rc |= dalloc(c, &tmp, 2 * (nz + 1) * nx * ny); m.wz[0] = tmp; m.wz[1] = tmp + (nz + 1) * nx * ny;
+  rc |= dalloc(c, &tmp, (nx + 2) * ny * nz); m.k1x = tmp;
+  rc |= dalloc(c, &tmp, (ny + 2) * nx * nz); m.k2y = tmp;
+  rc |= dalloc(c, &tmp, (nz + 2) * nx * ny); m.k3z = tmp;
+  rc |= dalloc(c, &tmp, nb * (nz + 1) * nx * ny); m.vs = tmp;
+  if (precision == F3D_PREC_FP64) {
+    rc |= dalloc(c, &m.ucur, (nx + 1) * ny * nz);
+    rc |= dalloc(c, &m.vcur, (ny + 1) * nx * nz);
+    rc |= dalloc(c, &m.wcur, (nz + 1) * nx * ny);
+  } else {
+    float* f;
+    rc |= dalloc(c, &f, 2 * (nx + 1) * ny * nz); m.ux32[0] = f; m.ux32[1] = f + (nx + 1) * ny * nz;
+    rc |= dalloc(c, &f, 2 * (ny + 1) * nx * nz); m.vy32[0] = f; m.vy32[1] = f + (ny + 1) * nx * nz;
+    rc |= dalloc(c, &f, 2 * (nz + 1) * nx * ny); m.wz32[0] = f; m.wz32[1] = f + (nz + 1) * nx * ny;
+    rc |= dalloc(c, &f, (nx + 1) * ny * nz); m.kfx = f;
+    rc |= dalloc(c, &f, (ny + 1) * nx * nz); m.kfy = f;
+    rc |= dalloc(c, &f, (nz + 1) * nx * ny); m.kfz = f;
+    rc |= dalloc(c, &f, nb * (nz + 1) * nx * ny); m.vs32 = f;
+    rc |= dalloc(c, &m.ucur32, (nx + 1) * ny * nz);
+    rc |= dalloc(c, &m.vcur32, (ny + 1) * nx * nz);
+    rc |= dalloc(c, &m.wcur32, (nz + 1) * nx * ny);
+    rc |= dalloc(c, &f, nx); m.rdx1b32 = f;
+    rc |= dalloc(c, &f, ny); m.rdx2b32 = f;
+    rc |= dalloc(c, &f, nz); m.rdx3b32 = f;
+  }
+  rc |= dalloc(c, &tmp, nx + 4); m.dx1p = tmp;
+  rc |= dalloc(c, &tmp, nx + 3); m.dx1b = tmp;
+  rc |= dalloc(c, &tmp, ny + 4); m.dx2p = tmp;
+  rc |= dalloc(c, &tmp, ny + 3); m.dx2b = tmp;
+  rc |= dalloc(c, &tmp, nz + 4); m.dx3p = tmp;
+  rc |= dalloc(c, &tmp, nz + 3); m.dx3b = tmp;
+  rc |= dalloc(c, &tmp, ny); m.hm1 = tmp;
+  rc |= dalloc(c, &tmp, ny + 4); m.hm2 = tmp;
+  rc |= dalloc(c, &tmp, nx * ny); m.hm3 = tmp;
+  rc |= dalloc(c, &m.flux_tot, 12);
+  rc |= dalloc(c, &m.flux_step, 6);
+  rc |= dalloc(c, &c->d_red, (size_t)c->mass_nblk * nb + 64);
+  rc |= dalloc(c, &c->d_nfail, 4);
+  size_t stage = std::max({(nx + 4) * (ny + 4) * (nz + 4) * nb, nx * ny * (nz + 3) * nb,
+                           2 * (nx + 3) * ny * nz, 2 * (ny + 3) * nx * nz, 2 * (nz + 3) * nx * ny,
+                           (nx + 4) * ny * nz, (ny + 4) * nx * nz, (nz + 4) * nx * ny});
+  rc |= dalloc(c, &c->staging, stage);
+  c->staging_elems = stage;
+  rc |= dalloc(c, &c->dm, 1);
+  if (rc == 0) rc |= build_work(c);
+  if (rc == 0 && cudaMallocHost(&c->h_pin, 4096) != cudaSuccess) rc = set_err("pinned alloc failed");
+  if (rc) {
+    std::string keep = g_err;
+    f3d_ads_destroy(c);
+    g_err = keep;
+    return 1;
+  }
+  CK(cudaMemsetAsync(m.c64 ? (void*)m.c64 : (void*)m.c32, 0,
+                     ncell * nb * (m.c64 ? sizeof(double) : sizeof(float)), c->st));
+  CK(cudaMemsetAsync(m.acum, 0, nx * ny * nb * sizeof(double), c->st));
+  CK(cudaMemsetAsync(m.flux_tot, 0, 12 * sizeof(double), c->st));
+  CK(cudaMemsetAsync(m.flux_step, 0, 6 * sizeof(double), c->st));
+  if (upload_member(c)) return 1;
+  *out = c;
+  return 0;
+}
+
+extern "C" int f3d_ads_destroy(f3d_ctx* c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->d_rhoc_tc) cudaFree(c->d_rhoc_tc);
+  if (c->h_pin) cudaFreeHost(c->h_pin);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return 0;
+}
+
+static int h2d(f3d_ctx* c, void* dst, const void* src, size_t bytes) {
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->st));
+  return 0;
+}
+
+extern "C" int f3d_ads_set_grid(f3d_ctx* c, const double* dX1_p, const double* dX1_b,
+                                const double* dX2_p, const double* dX2_b, const double* dX3_p,
+                                const double* dX3_b, const double* Hm1_p, const double* Hm2_p,
+                                const double* Hm3_p) {
+  if (!c) return set_err("f3d_ads_set_grid: null context");
+  if (!dX1_p || !dX1_b || !dX2_p || !dX2_b || !dX3_p || !dX3_b || !Hm1_p || !Hm2_p || !Hm3_p)
+    return set_err("f3d_ads_set_grid: null array");
+  CK(cudaSetDevice(c->device));
+  MemberDev& m = c->hm;
+  const size_t nx = c->nx, ny = c->ny, nz = c->nz;
+  if (h2d(c, (void*)m.dx1p, dX1_p, (nx + 4) * 8) || h2d(c, (void*)m.dx1b, dX1_b, (nx + 3) * 8) ||
+      h2d(c, (void*)m.dx2p, dX2_p, (ny + 4) * 8) || h2d(c, (void*)m.dx2b, dX2_b, (ny + 3) * 8) ||
+      h2d(c, (void*)m.dx3p, dX3_p, (nz + 4) * 8) || h2d(c, (void*)m.dx3b, dX3_b, (nz + 3) * 8) ||
+      h2d(c, (void*)m.hm1, Hm1_p, ny * 8) || h2d(c, (void*)m.hm2, Hm2_p, (ny + 4) * 8) ||
+      h2d(c, (void*)m.hm3, Hm3_p, nx * ny * 8))
+    return 1;
+  c->dX1_p.assign(dX1_p, dX1_p + nx + 4);
+  c->dX2_p.assign(dX2_p, dX2_p + ny + 4);
+  c->dX3_p.assign(dX3_p, dX3_p + nz + 4);
+  c->Hm1_p.assign(Hm1_p, Hm1_p + ny);
+  c->Hm2_p.assign(Hm2_p, Hm2_p + ny + 4);
+  c->Hm3_p.assign(Hm3_p, Hm3_p + nx * ny);
+  if (c->prec == F3D_PREC_FP32) {
+    std::vector<float> r1(nx), r2(ny), r3(nz);
+    for (size_t i = 0; i < nx; ++i) r1[i] = (float)(1.0 / dX1_b[i + 1]);
+    for (size_t j = 0; j < ny; ++j) r2[j] = (float)(1.0 / dX2_b[j + 1]);
+    for (size_t k = 0; k < nz; ++k) r3[k] = (float)(1.0 / dX3_b[k + 1]);
+    CK(cudaMemcpy((void*)m.rdx1b32, r1.data(), nx * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)m.rdx2b32, r2.data(), ny * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)m.rdx3b32, r3.data(), nz * 4, cudaMemcpyHostToDevice));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  c->grid_set = true;
+  return 0;
+}
+
+// Upload one reference-layout array through the staging buffer and convert.
+static int upload_conv(f3d_ctx* c, int which, const double* host, size_t elems, double* dst) {
+  if (elems > c->staging_elems) return set_err("staging buffer too small");
+  CK(cudaMemcpyAsync(c->staging, host, elems * 8, cudaMemcpyHostToDevice, c->st));
+  launch_conv(which, c->staging, dst, c->nx, c->ny, c->nz, c->nb, c->st);
+  CKL();
+  CK(cudaStreamSynchronize(c->st));  // the host array may change after return
+  return 0;
+}
+
+extern "C" int f3d_ads_set_meteo(f3d_ctx* c, const double* u, const double* v, const double* w,
+                                 const double* k1, const double* k2, const double* k3,
+                                 const double* vs, double t_its, double t_ite) {
+  if (!c) return set_err("f3d_ads_set_meteo: null context");
+  if (!u || !v || !w || !k1 || !k2 || !k3) return set_err("f3d_ads_set_meteo: null array");
+  if (!(t_ite != t_its)) return set_err("f3d_ads_set_meteo: t_ite == t_its");
+  CK(cudaSetDevice(c->device));
+  MemberDev& m = c->hm;
+  const size_t nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb;
+  if (upload_conv(c, 0, u, 2 * (nx + 3) * ny * nz, const_cast<double*>(m.ux[0])) ||
+      upload_conv(c, 1, v, 2 * (ny + 3) * nx * nz, const_cast<double*>(m.vy[0])) ||
+      upload_conv(c, 2, w, 2 * (nz + 3) * nx * ny, const_cast<double*>(m.wz[0])) ||
+      upload_conv(c, 3, k1, (nx + 4) * ny * nz, const_cast<double*>(m.k1x)) ||
+      upload_conv(c, 4, k2, (ny + 4) * nx * nz, const_cast<double*>(m.k2y)) ||
+      upload_conv(c, 5, k3, (nz + 4) * nx * ny, const_cast<double*>(m.k3z)))
+    return 1;
+  if (vs && upload_conv(c, 6, vs, nx * ny * (nz + 3) * nb, const_cast<double*>(m.vs))) return 1;
+  c->t_its = t_its;
+  c->t_ite = t_ite;
+  m.t_its = t_its;
+  m.t_ite = t_ite;
+  if (upload_member(c)) return 1;
+  if (c->prec == F3D_PREC_FP32) {
+    launch_fp32_fields(c->dm, 0, c->st);
+    CKL();
+    CK(cudaStreamSynchronize(c->st));
+  }
+  c->meteo_set = true;
+  return 0;
+}
+
+extern "C" int f3d_ads_set_source(f3d_ctx* c, int n, const int* ijk, const double* s) {
+  if (!c) return set_err("f3d_ads_set_source: null context");
+  if (n < 0 || (n > 0 && (!ijk || !s))) return set_err("f3d_ads_set_source: bad arguments");
+  if (!c->grid_set) return set_err("f3d_ads_set_source: grid not set");
+  CK(cudaSetDevice(c->device));
+  MemberDev& m = c->hm;
+  std::vector<int> cell(n);
+  std::vector<double> vol(n);
+  for (int q = 0; q < n; ++q) {
+    int i = ijk[3 * q] - 1, j = ijk[3 * q + 1] - 1, k = ijk[3 * q + 2] - 1;
+    if (i < 0 || i >= c->nx || j < 0 || j >= c->ny || k < 0 || k >= c->nz)
+      return set_err("f3d_ads_set_source: cell %d (%d,%d,%d) outside the domain", q, i + 1, j + 1,
+                     k + 1);
+    cell[q] = i + c->nx * (j + c->ny * k);
+    // vol = dX*dY*dZ*(Hm1*Hm2*Hm3)   mod_F3D.F90:1466
+    double dX = c->dX1_p[i + 2], dY = c->dX2_p[j + 2], dZ = c->dX3_p[k + 2];
+    double Hm1 = c->Hm1_p[j], Hm2 = c->Hm2_p[j + 2], Hm3 = c->Hm3_p[i + (size_t)c->nx * j];
+    volatile double a = dX * dY;
+    volatile double b = a * dZ;
+    volatile double h = Hm1 * Hm2;
+    volatile double h3 = h * Hm3;
+    vol[q] = b * h3;
+  }
+  if (n > c->src_cap) {
+    int cap = std::max(n, 64);
+    int* dc;
+    double *ds, *dv;
+    if (dalloc(c, &dc, (size_t)cap) || dalloc(c, &ds, (size_t)cap * c->nb) ||
+        dalloc(c, &dv, (size_t)cap))
+      return 1;
+    m.src_cell = dc;
+    m.src_s = ds;
+    m.src_vol = dv;
+    c->src_cap = cap;
+  }
+  if (n > 0) {
+    CK(cudaMemcpyAsync((void*)m.src_cell, cell.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync((void*)m.src_s, s, sizeof(double) * n * c->nb, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync((void*)m.src_vol, vol.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  }
+  m.nsrc = n;
+  return upload_member(c);
+}
+
+extern "C" int f3d_ads_set_source_dense(f3d_ctx* c, const double* my_s) {
+  if (!c || !my_s) return set_err("f3d_ads_set_source_dense: null argument");
+  const size_t nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb, ncell = nx * ny * nz;
+  std::vector<int> ijk;
+  std::vector<double> s;
+  for (size_t q = 0; q < ncell; ++q) {
+    bool any = false;
+    for (size_t b = 0; b < nb; ++b) any |= (my_s[q + ncell * b] != 0.0);
+    if (!any) continue;
+    ijk.push_back((int)(q % nx) + 1);
+    ijk.push_back((int)((q / nx) % ny) + 1);
+    ijk.push_back((int)(q / (nx * ny)) + 1);
+    for (size_t b = 0; b < nb; ++b) s.push_back(my_s[q + ncell * b]);
+  }
+  return f3d_ads_set_source(c, (int)(ijk.size() / 3), ijk.data(), s.data());
+}
+
+extern "C" int f3d_ads_upload_state(f3d_ctx* c, const double* my_c, const double* my_acum) {
+  if (!c) return set_err("f3d_ads_upload_state: null context");
+  CK(cudaSetDevice(c->device));
+  MemberDev& m = c->hm;
+  const size_t nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb;
+  if (my_c) {
+    if (c->prec == F3D_PREC_FP64) {
+      if (upload_conv(c, 7, my_c, (nx + 4) * (ny + 4) * (nz + 4) * nb, m.c64)) return 1;
+    } else {
+      // convert on the host, rounding to nearest FP32
+      std::vector<float> tmp(nx * ny * nz * nb);
+      for (size_t b = 0; b < nb; ++b)
+        for (size_t k = 0; k < nz; ++k)
+          for (size_t j = 0; j < ny; ++j)
+            for (size_t i = 0; i < nx; ++i)
+              tmp[((b * nz + k) * ny + j) * nx + i] =
+                  (float)my_c[(i + 2) + (nx + 4) * ((j + 2) + (ny + 4) * ((k + 2) + (nz + 4) * b))];
+      CK(cudaMemcpy(m.c32, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice));
+    }
+  }
+  if (my_acum && upload_conv(c, 8, my_acum, (nx + 4) * (ny + 4) * nb, m.acum)) return 1;
+  return 0;
+}
+
+extern "C" int f3d_ads_download_state(f3d_ctx* c, double* my_c, double* my_acum) {
+  if (!c) return set_err("f3d_ads_download_state: null context");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  MemberDev& m = c->hm;
+  const size_t nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb;
+  if (my_c) {
+    std::vector<double> tmp(nx * ny * nz * nb);
+    if (c->prec == F3D_PREC_FP64) {
+      CK(cudaMemcpy(tmp.data(), m.c64, tmp.size() * 8, cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> t32(tmp.size());
+      CK(cudaMemcpy(t32.data(), m.c32, t32.size() * 4, cudaMemcpyDeviceToHost));
+      for (size_t q = 0; q < t32.size(); ++q) tmp[q] = t32[q];
+    }
+    const size_t X = nx + 4, Y = ny + 4, Z = nz + 4;
+    for (size_t b = 0; b < nb; ++b)
+      for (size_t k = 0; k < nz; ++k)
+        for (size_t j = 0; j < ny; ++j) {
+          const double* row = &tmp[((b * nz + k) * ny + j) * nx];
+          double* dst = &my_c[2 + X * ((j + 2) + Y * ((k + 2) + Z * b))];
+          memcpy(dst, row, nx * 8);
+          // zero-gradient face ghosts of the final state
+          dst[-1] = dst[-2] = row[0];
+          dst[nx] = dst[nx + 1] = row[nx - 1];
+        }
+    for (size_t b = 0; b < nb; ++b)
+      for (size_t k = 0; k < nz; ++k)
+        for (size_t i = 0; i < nx; ++i) {
+          double lo = tmp[((b * nz + k) * ny + 0) * nx + i];
+          double hi = tmp[((b * nz + k) * ny + (ny - 1)) * nx + i];
+          for (int g = 0; g < 2; ++g) {
+            my_c[(i + 2) + X * (g + Y * ((k + 2) + Z * b))] = lo;
+            my_c[(i + 2) + X * ((ny + 2 + g) + Y * ((k + 2) + Z * b))] = hi;
+          }
+        }
+    for (size_t b = 0; b < nb; ++b)
+      for (size_t j = 0; j < ny; ++j)
+        for (size_t i = 0; i < nx; ++i) {
+          double lo = tmp[((b * nz + 0) * ny + j) * nx + i];
+          double hi = tmp[((b * nz + (nz - 1)) * ny + j) * nx + i];
+          for (int g = 0; g < 2; ++g) {
+            my_c[(i + 2) + X * ((j + 2) + Y * (g + Z * b))] = lo;
+            my_c[(i + 2) + X * ((j + 2) + Y * ((nz + 2 + g) + Z * b))] = hi;
+          }
+        }
+  }
+  if (my_acum) {
+    std::vector<double> tmp(nx * ny * nb);
+    CK(cudaMemcpy(tmp.data(), m.acum, tmp.size() * 8, cudaMemcpyDeviceToHost));
+    for (size_t b = 0; b < nb; ++b)
+      for (size_t j = 0; j < ny; ++j)
+        memcpy(&my_acum[2 + (nx + 4) * ((j + 2) + (ny + 4) * b)], &tmp[(b * ny + j) * nx], nx * 8);
+  }
+  return 0;
+}
+
+// ---- step ---------------------------------------------------------------
+static int enqueue_sweep(f3d_ctx* c, int dir) {
+  if (c->prec == F3D_PREC_FP64)
+    launch_sweep64(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->st);
+  else
+    launch_sweep32(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->st);
+  CKL();
+  return 0;
+}
+
+static int enqueue_prep(f3d_ctx* c, int mask) {
+  if (c->prec == F3D_PREC_FP64)
+    launch_prep64(c->dm, c->dprep_member, c->dprep_first, c->nprep, mask, c->st);
+  else
+    launch_prep32(c->dm, c->dprep_member, c->dprep_first, c->nprep, mask, c->st);
+  CKL();
+  return 0;
+}
+
+static int enqueue_source(f3d_ctx* c) {
+  if (c->hm.nsrc <= 0) return 0;
+  if (c->prec == F3D_PREC_FP64) launch_source64(c->dm, 1, c->st);
+  else launch_source32(c->dm, 1, c->st);
+  CKL();
+  return 0;
+}
+
+static int check_ready(f3d_ctx* c, const char* who) {
+  if (!c) return set_err("%s: null context", who);
+  if (!c->grid_set) return set_err("%s: grid not set", who);
+  if (!c->meteo_set) return set_err("%s: meteo not set", who);
+  return 0;
+}
+
+static int enqueue_step(f3d_ctx* c, double dt, double time, int iiter) {
+  launch_set_step(c->dm, 0, dt, time, iiter, c->st);
+  CKL();
+  if (enqueue_prep(c, 7) || enqueue_source(c)) return 1;
+  if (iiter % 2 == 0) {  // mod_F3D.F90:1477-1487
+    if (enqueue_sweep(c, DIR_X) || enqueue_sweep(c, DIR_Y)) return 1;
+  } else {
+    if (enqueue_sweep(c, DIR_Y) || enqueue_sweep(c, DIR_X)) return 1;
+  }
+  if (enqueue_sweep(c, DIR_Z)) return 1;
+  launch_flux_reduce(c->dm, 1, 7, c->st);
+  CKL();
+  return 0;
+}
+
+extern "C" int f3d_ads_step(f3d_ctx* c, double dt, double time, int iiter, double fluxes[6]) {
+  if (check_ready(c, "f3d_ads_step")) return 1;
+  if (!fluxes) return set_err("f3d_ads_step: null fluxes");
+  CK(cudaSetDevice(c->device));
+  if (enqueue_step(c, dt, time, iiter)) return 1;
+  CK(cudaMemcpyAsync(c->h_pin, c->hm.flux_step, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (int q = 0; q < 6; ++q) fluxes[q] = fluxes[q] + c->h_pin[q];
+  return 0;
+}
+
+extern "C" int f3d_ads_step_async(f3d_ctx* c, double dt, double time, int iiter) {
+  if (check_ready(c, "f3d_ads_step_async")) return 1;
+  CK(cudaSetDevice(c->device));
+  return enqueue_step(c, dt, time, iiter);
+}
+
+extern "C" int f3d_ads_get_fluxes(f3d_ctx* c, double fluxes[6]) {
+  if (!c || !fluxes) return set_err("f3d_ads_get_fluxes: null argument");
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(c->h_pin, c->hm.flux_tot, 12 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemsetAsync(c->hm.flux_tot, 0, 12 * sizeof(double), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (int q = 0; q < 6; ++q) fluxes[q] = fluxes[q] + (c->h_pin[q] - c->h_pin[6 + q]);
+  return 0;
+}
+
+extern "C" int f3d_ads_synchronize(f3d_ctx* c) {
+  if (!c) return set_err("f3d_ads_synchronize: null context");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+extern "C" int f3d_ads_get_stream(f3d_ctx* c, void** stream) {
+  if (!c || !stream) return set_err("f3d_ads_get_stream: null argument");
+  *stream = (void*)c->st;
+  return 0;
+}
+
+extern "C" int f3d_ads_update_vcomps(f3d_ctx* c, double stime) {
+  if (check_ready(c, "f3d_ads_update_vcomps")) return 1;
+  CK(cudaSetDevice(c->device));
+  c->hm.stime = stime;
+  launch_set_dt_stime(c->dm, 0, 0.0, stime, c->st);
+  CKL();
+  return enqueue_prep(c, 3);
+}
+
+static int solve_dir(f3d_ctx* c, int dir, double dt, double* a, double* b, const char* who) {
+  if (check_ready(c, who)) return 1;
+  if (!a || !b) return set_err("%s: null flux argument", who);
+  CK(cudaSetDevice(c->device));
+  if (enqueue_sweep(c, dir)) return 1;
+  launch_flux_reduce(c->dm, 1, 1 << dir, c->st);
+  CKL();
+  CK(cudaMemcpyAsync(c->h_pin, c->hm.flux_step, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  (void)dt;
+  if (dir == DIR_X) { *a = *a + c->h_pin[0]; *b = *b + c->h_pin[1]; }
+  if (dir == DIR_Y) { *a = *a + c->h_pin[2]; *b = *b + c->h_pin[3]; }
+  if (dir == DIR_Z) { *a = *a + c->h_pin[5]; *b = *b + c->h_pin[4]; }
+  return 0;
+}
+
+// The sweep kernels read dt and stime from the member descriptor; these
+// entry points set them (stime only matters for z, whose wind is rebuilt).
+extern "C" int f3d_ads_solve_along_x(f3d_ctx* c, double dt, double* W, double* E) {
+  if (check_ready(c, "f3d_ads_solve_along_x")) return 1;
+  launch_set_dt_stime(c->dm, 0, dt, c->hm.stime, c->st);
+  return solve_dir(c, DIR_X, dt, W, E, "f3d_ads_solve_along_x");
+}
+extern "C" int f3d_ads_solve_along_y(f3d_ctx* c, double dt, double* S, double* N) {
+  if (check_ready(c, "f3d_ads_solve_along_y")) return 1;
+  launch_set_dt_stime(c->dm, 0, dt, c->hm.stime, c->st);
+  return solve_dir(c, DIR_Y, dt, S, N, "f3d_ads_solve_along_y");
+}
+extern "C" int f3d_ads_solve_along_z(f3d_ctx* c, double dt, double stime, double* D, double* U) {
+  if (check_ready(c, "f3d_ads_solve_along_z")) return 1;
+  CK(cudaSetDevice(c->device));
+  // rebuild the current w at stime (mod_ADS.F90:667) without touching u, v
+  c->hm.stime = stime;
+  launch_set_dt_stime(c->dm, 0, dt, stime, c->st);
+  CKL();
+  if (enqueue_prep(c, 4)) return 1;
+  return solve_dir(c, DIR_Z, dt, D, U, "f3d_ads_solve_along_z");
+}
+
+extern "C" int f3d_ads_add_source(f3d_ctx* c, double dt) {
+  if (check_ready(c, "f3d_ads_add_source")) return 1;
+  CK(cudaSetDevice(c->device));
+  launch_set_dt_stime(c->dm, 0, dt, c->hm.stime, c->st);
+  CKL();
+  if (enqueue_source(c)) return 1;
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+extern "C" int f3d_ads_get_time_step(f3d_ctx* c, double stime, int criterion, double cfl,
+                                     double run_end, double* my_dt, double* gl_dt) {
+  if (check_ready(c, "f3d_ads_get_time_step")) return 1;
+  if (!my_dt || !gl_dt) return set_err("f3d_ads_get_time_step: null output");
+  if (criterion != 1 && criterion != 2)
+    return set_err("f3d_ads_get_time_step: criterion %d not in 1..2", criterion);
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemsetAsync(c->d_red, 0, 3 * sizeof(double), c->st));
+  launch_cfl(c->dm, 0, stime, criterion, c->d_red, c->st);
+  CKL();
+  CK(cudaMemcpyAsync(c->h_pin, c->d_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double dt1 = c->h_pin[0], dt2 = c->h_pin[1], dt3 = c->h_pin[2];
+  double m = std::max(std::max(dt1, dt2), dt3);  // mod_Grid.F90:1125-1127
+  if (m > 0.0) m = 1.0 / m;
+  m = cfl * m;
+  *my_dt = std::min(m, run_end);
+  *gl_dt = std::min(m, run_end);
+  return 0;
+}
+
+extern "C" int f3d_ads_mass_volume(f3d_ctx* c, double* mass, double* per_bin) {
+  if (!c || !mass) return set_err("f3d_ads_mass_volume: null argument");
+  if (!c->grid_set) return set_err("f3d_ads_mass_volume: grid not set");
+  CK(cudaSetDevice(c->device));
+  double* out = c->d_red + (size_t)c->mass_nblk * c->nb;
+  if (c->nb > 64) return set_err("f3d_ads_mass_volume: more than 64 bins");
+  launch_mass(c->dm, 0, c->nb, c->prec == F3D_PREC_FP32, c->d_red, c->mass_nblk, out, c->st);
+  CKL();
+  std::vector<double> pb(c->nb);
+  CK(cudaMemcpyAsync(c->h_pin, out, c->nb * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double tot = 0.0, comp = 0.0;
+  for (int b = 0; b < c->nb; ++b) {
+    double x = c->h_pin[b], t = tot + x;
+    comp += (std::fabs(tot) >= std::fabs(x)) ? (tot - t) + x : (x - t) + tot;
+    tot = t;
+    if (per_bin) per_bin[b] = x;
+  }
+  *mass = tot + comp;
+  return 0;
+}
+
+extern "C" int f3d_ads_mass_boundaries(const double fluxes[6], double* ground, double* lateral) {
+  if (!fluxes || !ground || !lateral) return set_err("f3d_ads_mass_boundaries: null argument");
+  *ground = std::fabs(fluxes[5]);
+  *lateral = std::fabs(fluxes[0]) + std::fabs(fluxes[1]) + std::fabs(fluxes[2]) +
+             std::fabs(fluxes[3]) + std::fabs(fluxes[4]);
+  return 0;
+}
+
+extern "C" int f3d_vset_points(int model, int n, const double* diam, const double* rhop,
+                               const double* psi, const double* rhoa, const double* visc,
+                               double* vset, int* flags, int* iters) {
+  if (n < 0) return set_err("f3d_vset_points: n < 0");
+  if (n == 0) return 0;
+  if (!diam || !rhop || !psi || !rhoa || !visc || !vset || !flags)
+    return set_err("f3d_vset_points: null array");
+  if (model < 1 || model > 7) return set_err("f3d_vset_points: settling velocity model %d not found", model);
+  double* d = nullptr;
+  int* fi = nullptr;
+  size_t N = (size_t)n;
+  if (cudaMalloc(&d, N * 6 * 8) != cudaSuccess) return set_err("f3d_vset_points: device alloc failed");
+  if (cudaMalloc(&fi, (N * 2 + 1) * 4) != cudaSuccess) {
+    cudaFree(d);
+    return set_err("f3d_vset_points: device alloc failed");
+  }
+  int rc = 0;
+  const double* srcs[5] = {diam, rhop, psi, rhoa, visc};
+  for (int a = 0; a < 5 && !rc; ++a)
+    if (cudaMemcpy(d + a * N, srcs[a], N * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = set_err("f3d_vset_points: copy failed");
+  if (!rc && cudaMemset(fi + 2 * N, 0, 4) != cudaSuccess) rc = set_err("memset failed");
+  if (!rc) {
+    launch_vset_points(model, n, d, d + N, d + 2 * N, d + 3 * N, d + 4 * N, d + 5 * N, fi,
+                       fi + N, fi + 2 * N, 0);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) rc = set_err("f3d_vset_points: %s", cudaGetErrorString(e));
+  }
+  int nfail = 0;
+  if (!rc && (cudaMemcpy(vset, d + 5 * N, N * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+              cudaMemcpy(flags, fi, N * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+              (iters && cudaMemcpy(iters, fi + N, N * 4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+              cudaMemcpy(&nfail, fi + 2 * N, 4, cudaMemcpyDeviceToHost) != cudaSuccess))
+    rc = set_err("f3d_vset_points: copy back failed");
+  cudaFree(d);
+  cudaFree(fi);
+  if (rc) return rc;
+  if (nfail) {
+    set_err("no convergence in vset (%d points)", nfail);
+    return 2;
+  }
+  return 0;
+}
+
+extern "C" int f3d_ads_compute_vset(f3d_ctx* c, int model, const double* rhoc, const double* tc,
+                                    const double* diam, const double* rhop, const double* psi,
+                                    const int* bin_cat, const int* is_aggregate, double vset_fac,
+                                    double* vs_out) {
+  if (!c) return set_err("f3d_ads_compute_vset: null context");
+  if (!c->grid_set) return set_err("f3d_ads_compute_vset: grid not set");
+  if (!rhoc || !tc || !diam || !rhop || !psi || !bin_cat)
+    return set_err("f3d_ads_compute_vset: null array");
+  if (model < 1 || model > 7) return set_err("setling velocity model not found");
+  CK(cudaSetDevice(c->device));
+  const size_t ncor = (size_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+  size_t need = 2 * ncor + 3 * (size_t)c->nb + (size_t)c->nb;
+  if (need > c->rhoc_cap) {
+    if (c->d_rhoc_tc) cudaFree(c->d_rhoc_tc);
+    CK(cudaMalloc(&c->d_rhoc_tc, need * 8));
+    c->rhoc_cap = need;
+  }
+  double* drho = c->d_rhoc_tc;
+  double* dt = drho + ncor;
+  double* dpar = dt + ncor;
+  int* dflags = reinterpret_cast<int*>(dpar + 3 * c->nb);
+  std::vector<double> par(3 * c->nb);
+  std::vector<int> fl(c->nb);
+  for (int b = 0; b < c->nb; ++b) {
+    par[3 * b] = diam[b];
+    par[3 * b + 1] = rhop[b];
+    par[3 * b + 2] = psi[b];
+    fl[b] = bin_cat[b] | ((is_aggregate && is_aggregate[b]) ? (1 << 8) : 0);
+  }
+  CK(cudaMemcpyAsync(drho, rhoc, ncor * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dt, tc, ncor * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dpar, par.data(), par.size() * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dflags, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemsetAsync(c->d_nfail, 0, 4, c->st));
+  launch_vset_field(c->dm, 0, model, drho, dt, dpar, dflags, vset_fac, c->d_nfail, c->st);
+  CKL();
+  if (c->prec == F3D_PREC_FP32 && c->meteo_set) {
+    launch_fp32_fields(c->dm, 0, c->st);
+    CKL();
+  }
+  int nfail = 0;
+  CK(cudaMemcpyAsync(c->h_pin, c->d_nfail, 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  memcpy(&nfail, c->h_pin, 4);
+  if (vs_out) {
+    size_t n = (size_t)c->nx * c->ny * (c->nz + 3) * c->nb;
+    if (n > c->staging_elems) return set_err("staging too small");
+    launch_conv(9, c->hm.vs, c->staging, c->nx, c->ny, c->nz, c->nb, c->st);
+    CKL();
+    CK(cudaMemcpyAsync(vs_out, c->staging, n * 8, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  if (nfail) {
+    set_err("no convergence in vset (%d points)", nfail);
+    return 2;
+  }
+  return 0;
+}
+
+extern "C" int f3d_host_alloc(size_t bytes, void** ptr) {
+  if (!ptr) return set_err("f3d_host_alloc: null pointer");
+  CK(cudaMallocHost(ptr, bytes));
+  return 0;
+}
+extern "C" int f3d_host_free(void* ptr) {
+  CK(cudaFreeHost(ptr));
+  return 0;
+}

@@ -1,0 +1,101 @@
+// f3d_common.cuh -- device-side data layout shared by all FALL3D ADS kernels.
+//
+// One "member" is one model domain (a serial FALL3D run, or one ensemble
+// member).  Every kernel takes a table of members plus a work list, so the
+// single-domain drop-in and the batched ensemble run the same code.
+//
+// HBM layout of a member (interior cells only; ghost cells are rebuilt by
+// the free-flow boundary condition inside each sweep, exactly where the
+// reference writes them before reading them, mod_ADS.F90:269-271):
+//   c     [bin][k][j][i]                     concentration (FP64 or FP32)
+//   acum  [bin][j][i]                        ground deposit, FP64 always
+//   ux    [snap][k][f=0..nx][j]              x-face wind, j fastest so a warp
+//                                            of x-pencils reads it coalesced
+//   vy    [snap][k][f=0..ny][i]              y-face wind
+//   wz    [snap][f=0..nz][j][i]              z-face wind
+//   k1x   [k][p=-1..nx][j]   k2y [k][p=-1..ny][i]   k3z [p=-1..nz][j][i]
+//   vs    [bin][f=0..nz][j][i]               settling velocity (scaled)
+// Pencils: x-pencil (j,k,bin) lanes over j; y-pencil (i,k,bin) and
+// z-pencil (i,j,bin) lanes over i, so y/z loads are fully coalesced.
+#pragma once
+#include <cstdint>
+
+namespace f3d {
+
+constexpr double kEps = 1e-12;  // EPSILON, mod_KindType.F90:42
+
+enum Dir { DIR_X = 0, DIR_Y = 1, DIR_Z = 2 };
+
+struct MemberDev {
+  int nx, ny, nz, nb;
+  // state
+  double* c64;
+  float* c32;
+  double* acum;
+  // meteo snapshots (FP64 copies, used by the exact path and the CFL)
+  const double* ux[2];
+  const double* vy[2];
+  const double* wz[2];
+  const double* k1x;
+  const double* k2y;
+  const double* k3z;
+  const double* vs;
+  // FP32 copies for the precision form (null when unused)
+  const float* ux32[2];
+  const float* vy32[2];
+  const float* wz32[2];
+  const float* kfx;   // [k][f=0..nx][j]  0.5(k(f)+k(f-1))/dxp(f-1)
+  const float* kfy;   // [k][f=0..ny][i]
+  const float* kfz;   // [f=0..nz][j][i]
+  const float* vs32;  // [bin][f][j][i]
+  // per-step current winds (written by the prep kernel)
+  double* ucur;  // [k][f][j]
+  double* vcur;  // [k][f][i]
+  double* wcur;  // [f][j][i]
+  float* ucur32;
+  float* vcur32;
+  float* wcur32;
+  float wfac;       // per-member multiplicative factor on u,v (ensemble)
+  // grid metrics (reference arrays with their halos)
+  const double* dx1p;  // (nx+4)   ips-2..ipe+2
+  const double* dx1b;  // (nx+3)   ibs-1..ibe+1
+  const double* dx2p;
+  const double* dx2b;
+  const double* dx3p;
+  const double* dx3b;
+  const double* hm1;  // ny
+  const double* hm2;  // ny+4
+  const double* hm3;  // nx*ny
+  const float* rdx1b32;  // 1/dx_b per axis, FP32 form
+  const float* rdx2b32;
+  const float* rdx3b32;
+  // sparse source: cell index (i + nx*(j + ny*k)), my_s values per bin,
+  // cell volume dX dY dZ Hm1 Hm2 Hm3
+  int nsrc;
+  const int* src_cell;
+  const double* src_s;  // [q][bin]
+  const double* src_vol;
+  // step parameters (device resident so a step can run inside a graph)
+  double dt;
+  double stime;
+  double time;
+  double t_its, t_ite;
+  int iiter;
+  int pad0;
+  // flux bookkeeping
+  double* flux_part;  // per-block partial sums, [slot][2]
+  int part_base[3];   // first partial slot of this member for x, y, z
+  int part_count[3];  // number of partial slots (blocks) per direction
+  double* flux_tot;   // running totals {W,E,S,N,U,D} and compensations [12]
+  double* flux_step;  // this step's increments {W,E,S,N,U,D}
+};
+
+// A block of one sweep: pencils [pen0, pen0 + blockDim) of one member.
+struct WorkItem {
+  int member;
+  int pen0;
+  int slot;  // flux partial slot
+  int pad;
+};
+
+}  // namespace f3d

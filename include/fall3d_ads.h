@@ -1,0 +1,190 @@
+/*
+ * fall3d_ads.h -- C ABI of libfall3d_ads.so, the B200 implementation of the
+ * FALL3D advection-diffusion-sedimentation (ADS) time step.
+ *
+ * The Fortran host (task_Fall3d / mod_F3D) reaches the GPU through these
+ * entry points with ISO_C_BINDING; every array argument is a plain pointer
+ * to the first element of the reference's own array, in the reference's own
+ * column-major layout and bounds (serial build: my_ips = 1 .. my_ipe = nx).
+ * The library copies what it needs and never keeps a host pointer.
+ *
+ * Every function returns 0 on success, 1 on error (message available from
+ * f3d_last_error) or 2 when a settling-velocity solve did not converge
+ * (the reference's MY_ERR%flag = 2, mod_Phys.F90:947-948).  Nothing aborts.
+ *
+ * One context = one model domain on one GPU with its own CUDA stream.
+ * Calls on one context must come from one host thread at a time.
+ */
+#ifndef FALL3D_ADS_H
+#define FALL3D_ADS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct f3d_ctx f3d_ctx;
+
+/* Interior mass points of the domain (my_ipe-my_ips+1, ...) and bins. */
+typedef struct {
+  int nx, ny, nz, nbins;
+} f3d_dims;
+
+/* Arithmetic forms. */
+#define F3D_PREC_FP64 0 /* FP64 state and stencil, reference operation order  */
+#define F3D_PREC_FP32 1 /* FP32 state and stencil; FP64 deposit, budget, CFL */
+
+/* Limiters (mod_Phys.F90:58-61) and time marching (mod_Phys.F90:64-65). */
+#define F3D_LIMITER_MINMOD 1
+#define F3D_LIMITER_SUPERBEE 2
+#define F3D_LIMITER_OSPRE 3
+#define F3D_TIME_MARCHING_EULER 1
+#define F3D_TIME_MARCHING_RK 2
+
+/* ---- lifetime --------------------------------------------------------- */
+
+/* ADS_initialize(limitertype, time_marching)  mod_ADS.F90:98.
+ * Allocates every device buffer of the domain (state, meteo, scratch). */
+int f3d_ads_create(const f3d_dims *dims, int limiter, int time_marching,
+                   int precision, int device, f3d_ctx **out);
+
+/* ADS_release()  mod_ADS.F90:208. */
+int f3d_ads_destroy(f3d_ctx *ctx);
+
+/* Copies the message of the last failed call on this host thread. */
+int f3d_last_error(char *buf, int len);
+
+/* ---- inputs ------------------------------------------------------------ */
+
+/* ARAKAWA_C_GRID metric arrays (mod_KindType.F90:465-502), built by
+ * grid_build_arakawa_c (mod_Grid.F90:286-676):
+ *   dX1_p(ips-2:ipe+2) dX1_b(ibs-1:ibe+1) dX2_p(jps-2:jpe+2)
+ *   dX2_b(jbs-1:jbe+1) dX3_p(kps-2:kpe+2) dX3_b(kbs-1:kbe+1)
+ *   Hm1_p(jps:jpe) Hm2_p(jps-2:jpe+2) Hm3_p(ips:ipe,jps:jpe) */
+int f3d_ads_set_grid(f3d_ctx *ctx, const double *dX1_p, const double *dX1_b,
+                     const double *dX2_p, const double *dX2_b,
+                     const double *dX3_p, const double *dX3_b,
+                     const double *Hm1_p, const double *Hm2_p,
+                     const double *Hm3_p);
+
+/* Meteo term produced by F3D_update_meteo_term (mod_F3D.F90:564-969):
+ *   u  MY_MET%my_u (ibs-1:ibe+1, jps:jpe, kps:kpe, 2)   scaled, staggered
+ *   v  MY_MET%my_v (jbs-1:jbe+1, ips:ipe, kps:kpe, 2)
+ *   w  MY_MET%my_w (kbs-1:kbe+1, ips:ipe, jps:jpe, 2)
+ *   k1 MY_MET%my_k1(ips-2:ipe+2, jps:jpe, kps:kpe)
+ *   k2 MY_MET%my_k2(jps-2:jpe+2, ips:ipe, kps:kpe)
+ *   k3 MY_MET%my_k3(kps-2:kpe+2, ips:ipe, jps:jpe)
+ *   vs MY_TRA%my_vs(ips:ipe, jps:jpe, kbs-1:kbe+1, nbins)  (scaled by 1/Hm3)
+ *   t_its, t_ite = MY_MET%timesec(its), timesec(ite)
+ * vs may be NULL to keep the field from f3d_ads_compute_vset. */
+int f3d_ads_set_meteo(f3d_ctx *ctx, const double *u, const double *v,
+                      const double *w, const double *k1, const double *k2,
+                      const double *k3, const double *vs, double t_its,
+                      double t_ite);
+
+/* Source term MY_TRA%my_s(ips:ipe,jps:jpe,kps:kpe,nbins) after
+ * F3D_set_source_term (mod_F3D.F90:349-555), given sparsely: n cells with
+ * 1-based Fortran indices ijk[3*q+0..2] and values s[nbins*q + bin] (the
+ * already Hm1*Hm2*Hm3-scaled my_s).  n = 0 clears the source. */
+int f3d_ads_set_source(f3d_ctx *ctx, int n, const int *ijk, const double *s);
+
+/* Same, from the dense my_s array; zero cells are skipped. */
+int f3d_ads_set_source_dense(f3d_ctx *ctx, const double *my_s);
+
+/* Initial condition / restart (task_Fall3d.F90:233-249):
+ *   my_c   (ips-2:ipe+2, jps-2:jpe+2, kps-2:kpe+2, nbins)
+ *   my_acum(ips-2:ipe+2, jps-2:jpe+2, nbins)            (either may be NULL) */
+int f3d_ads_upload_state(f3d_ctx *ctx, const double *my_c,
+                         const double *my_acum);
+
+/* Copies the device state back into the reference arrays (interior cells;
+ * ghost cells receive the free-flow values of the final state). */
+int f3d_ads_download_state(f3d_ctx *ctx, double *my_c, double *my_acum);
+
+/* ---- the time step ----------------------------------------------------- */
+
+/* Body of F3D_time_step (mod_F3D.F90:1397-1491): u/v time interpolation,
+ * source injection, x/y sweeps (order alternating with iiter parity), z sweep
+ * with settling, ground deposit and boundary fluxes.  fluxes[6] =
+ * {W,E,S,N,U,D} (MY_TRA%my_W_flux ...) are INOUT accumulators, as in
+ * ADS_solve_along_x/y/z.  Blocks until the step completed. */
+int f3d_ads_step(f3d_ctx *ctx, double dt, double time, int iiter,
+                 double fluxes[6]);
+
+/* Same step, enqueued without waiting; flux increments accumulate on the
+ * device and are read with f3d_ads_get_fluxes. */
+int f3d_ads_step_async(f3d_ctx *ctx, double dt, double time, int iiter);
+
+/* Adds the device-accumulated flux increments to fluxes[6] and zeroes them. */
+int f3d_ads_get_fluxes(f3d_ctx *ctx, double fluxes[6]);
+
+/* Waits for every call enqueued on the context. */
+int f3d_ads_synchronize(f3d_ctx *ctx);
+
+/* The CUDA stream (cudaStream_t) the context enqueues on, for event timing
+ * and for ordering the caller's own work after a step. */
+int f3d_ads_get_stream(f3d_ctx *ctx, void **stream);
+
+/* The pieces of the step, for unit parity with the ADS_* routines. */
+/* ADS_update_horizontal_vcomps(u1,u2,v1,v2,stime)  mod_ADS.F90:187 */
+int f3d_ads_update_vcomps(f3d_ctx *ctx, double stime);
+/* ADS_solve_along_x(W_flux,E_flux,dt,...)  mod_ADS.F90:233 */
+int f3d_ads_solve_along_x(f3d_ctx *ctx, double dt, double *W_flux,
+                          double *E_flux);
+/* ADS_solve_along_y(S_flux,N_flux,dt,...)  mod_ADS.F90:422 */
+int f3d_ads_solve_along_y(f3d_ctx *ctx, double dt, double *S_flux,
+                          double *N_flux);
+/* ADS_solve_along_z(D_flux,U_flux,dt,...,stime,my_vs,...)  mod_ADS.F90:612 */
+int f3d_ads_solve_along_z(f3d_ctx *ctx, double dt, double stime,
+                          double *D_flux, double *U_flux);
+/* Source injection loop of F3D_time_step, mod_F3D.F90:1456-1473 */
+int f3d_ads_add_source(f3d_ctx *ctx, double dt);
+
+/* ---- diagnostics ------------------------------------------------------- */
+
+/* grid_get_time_step (mod_Grid.F90:1026-1141) with winds interpolated at
+ * stime (mod_F3D.F90:957-961).  criterion 1 (ONE_DIMENSIONAL) or
+ * 2 (ALL_DIMENSIONS).  FP64 max-reduction on the device. */
+int f3d_ads_get_time_step(f3d_ctx *ctx, double stime, int criterion,
+                          double cfl, double run_end, double *my_dt,
+                          double *gl_dt);
+
+/* grid_get_mass_volume (mod_Grid.F90:1340-1389): sum c dX dY dZ over the
+ * interior.  per_bin (nbins, may be NULL) receives the per-bin masses. */
+int f3d_ads_mass_volume(f3d_ctx *ctx, double *mass, double *per_bin);
+
+/* grid_get_mass_boundaries (mod_Grid.F90:1461-1511) from fluxes {W,E,S,N,U,D}. */
+int f3d_ads_mass_boundaries(const double fluxes[6], double *ground,
+                            double *lateral);
+
+/* ---- settling velocity ---------------------------------------------------- */
+
+/* phys_get_vset_point (mod_Phys.F90:757-954) for n independent points on the
+ * GPU (host arrays).  model 1..7 (mod_Phys.F90:44-50).  flags[q] receives
+ * 0 / 2 (no convergence); iters (may be NULL) the iteration counts.
+ * Returns 2 when any point failed to converge. */
+int f3d_vset_points(int model, int n, const double *diam, const double *rhop,
+                    const double *psi, const double *rhoa, const double *visc,
+                    double *vset, int *flags, int *iters);
+
+/* phys_get_vset (mod_Phys.F90:673-740) + the vs/Hm3 scaling of
+ * grid_get_scaled_variables (mod_Grid.F90:996-1005) on the device, writing
+ * the context's settling-velocity field.  rhoc, tc: corner air density and
+ * temperature (ibs:ibe, jbs:jbe, kbs:kbe).  bin_cat: 1 particle,
+ * 2 aerosol, 3 radionuclide; is_aggregate (may be NULL) with vset_fac.
+ * vs_out (may be NULL) receives my_vs in the reference layout. */
+int f3d_ads_compute_vset(f3d_ctx *ctx, int model, const double *rhoc,
+                         const double *tc, const double *diam,
+                         const double *rhop, const double *psi,
+                         const int *bin_cat, const int *is_aggregate,
+                         double vset_fac, double *vs_out);
+
+/* ---- pinned host memory for fast transfers --------------------------------- */
+int f3d_host_alloc(size_t bytes, void **ptr);
+int f3d_host_free(void *ptr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FALL3D_ADS_H */

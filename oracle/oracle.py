@@ -1,0 +1,204 @@
+"""ctypes binding of the CPU FP64 oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the fall3d_b200 package.  See
+f3d_oracle.h for the reference routine each function restates; parity with
+the reference binary is unpinned (no Fortran compiler here) and the analytic
+known-answer tests in tests/test_oracle_kat.py pin the algorithm.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="F_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="F_CONTIGUOUS")
+
+
+class Dims(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nbins", C.c_int),
+                ("limiter", C.c_int), ("time_marching", C.c_int)]
+
+
+class Grid(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in
+                ("dX1_p", "dX1_b", "dX2_p", "dX2_b", "dX3_p", "dX3_b", "Hm1_p", "Hm2_p", "Hm3_p")]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        D = C.POINTER(Dims)
+        G = C.POINTER(Grid)
+        dp = C.POINTER(C.c_double)
+        L.or_kt_rhs.argtypes = [C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, dp]
+        L.or_ads_solve_1d.argtypes = [C.c_int, C.c_int, dp, dp, dp, dp, dp, C.c_double, dp, dp,
+                                      C.POINTER(C.c_int)]
+        L.or_solve_x.argtypes = [D, G, C.c_double, dp, dp, dp, dp, dp, C.c_int]
+        L.or_solve_y.argtypes = [D, G, C.c_double, dp, dp, dp, dp, dp, C.c_int]
+        L.or_solve_z.argtypes = [D, G, C.c_double, dp, dp, dp, dp, dp, C.c_double, dp, dp, dp,
+                                 C.c_int]
+        L.or_time_step.argtypes = [D, G, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                   dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, C.c_int]
+        L.or_get_time_step.argtypes = [D, G, C.c_int, C.c_double, C.c_double, dp, dp, dp, dp, dp,
+                                       dp, dp, dp, dp]
+        L.or_mass_volume.argtypes = [D, G, dp]
+        L.or_mass_volume.restype = C.c_double
+        L.or_mass_boundaries.argtypes = [dp, dp, dp]
+        L.or_vset_point.argtypes = [C.c_double] * 5 + [C.c_int, dp, C.POINTER(C.c_int)]
+        L.or_vset_point.restype = C.c_int
+        L.or_get_vset.argtypes = [D, C.c_int, dp, dp, dp, dp, dp, C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), C.c_double, dp]
+        L.or_get_vset.restype = C.c_int
+        L.or_suzuki.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                C.c_double, dp, dp, dp]
+        L.or_place_source.argtypes = [D, G, C.c_double, C.c_double, C.c_double, C.c_double, dp,
+                                      dp, dp, C.c_int, dp, dp, dp, dp, dp]
+        L.or_perturb.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.or_perturb.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim == 1), a.flags
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ipt(a):
+    if a is None:
+        return None
+    a = np.asfortranarray(a, dtype=np.int32)
+    return a.ctypes.data_as(C.POINTER(C.c_int)), a
+
+
+class Oracle:
+    """A single-rank model domain held in reference-layout numpy arrays."""
+
+    def __init__(self, grid, nbins: int, limiter: int = 2, time_marching: int = 2, threads: int = 1):
+        self.g = grid
+        self.dims = Dims(grid.nx, grid.ny, grid.nz, nbins, limiter, time_marching)
+        self._garrs = [np.asfortranarray(getattr(grid, n), dtype=np.float64) for n in
+                       ("dX1_p", "dX1_b", "dX2_p", "dX2_b", "dX3_p", "dX3_b", "Hm1_p", "Hm2_p", "Hm3_p")]
+        self.cgrid = Grid(*[_p(a) for a in self._garrs])
+        self.threads = threads
+
+    # ---- pieces
+    def solve_x(self, dt, c, k1, u, W=0.0, E=0.0):
+        w, e = C.c_double(W), C.c_double(E)
+        lib().or_solve_x(C.byref(self.dims), C.byref(self.cgrid), dt, _p(c), _p(k1), _p(u),
+                         C.byref(w), C.byref(e), self.threads)
+        return w.value, e.value
+
+    def solve_y(self, dt, c, k2, v, S=0.0, N=0.0):
+        s, n = C.c_double(S), C.c_double(N)
+        lib().or_solve_y(C.byref(self.dims), C.byref(self.cgrid), dt, _p(c), _p(k2), _p(v),
+                         C.byref(s), C.byref(n), self.threads)
+        return s.value, n.value
+
+    def solve_z(self, dt, c, acum, k3, w1, w2, stime, vs, D=0.0, U=0.0):
+        d, u = C.c_double(D), C.c_double(U)
+        lib().or_solve_z(C.byref(self.dims), C.byref(self.cgrid), dt, _p(c), _p(acum), _p(k3),
+                         _p(w1), _p(w2), stime, _p(vs), C.byref(d), C.byref(u), self.threads)
+        return d.value, u.value
+
+    def time_step(self, dt, time, t_its, t_ite, iiter, c, acum, s, u12, v12, w12, k1, k2, k3, vs,
+                  fluxes):
+        lib().or_time_step(C.byref(self.dims), C.byref(self.cgrid), dt, time, t_its, t_ite, iiter,
+                           _p(c), _p(acum), _p(s), _p(u12), _p(v12), _p(w12), _p(k1), _p(k2),
+                           _p(k3), _p(vs), _p(fluxes), self.threads)
+
+    def get_time_step(self, criterion, cfl, run_end, u, v, w, k1, k2, k3, vs):
+        a, b = C.c_double(), C.c_double()
+        lib().or_get_time_step(C.byref(self.dims), C.byref(self.cgrid), criterion, cfl, run_end,
+                               _p(u), _p(v), _p(w), _p(k1), _p(k2), _p(k3), _p(vs), C.byref(a),
+                               C.byref(b))
+        return a.value, b.value
+
+    def mass_volume(self, c):
+        return lib().or_mass_volume(C.byref(self.dims), C.byref(self.cgrid), _p(c))
+
+    def get_vset(self, model, rhoc, tc, diam, rhop, psi, bin_cat, is_aggregate=None, vset_fac=1.0):
+        nb = self.dims.nbins
+        vs = np.zeros((self.g.nx, self.g.ny, self.g.nz + 3, nb), order="F")
+        cat, _k1 = _ipt(bin_cat)
+        agg = _ipt(is_aggregate)
+        flag = lib().or_get_vset(C.byref(self.dims), model, _p(rhoc), _p(tc),
+                                 _p(np.asarray(diam, np.float64)), _p(np.asarray(rhop, np.float64)),
+                                 _p(np.asarray(psi, np.float64)), cat, agg[0] if agg else None,
+                                 vset_fac, _p(vs))
+        return vs, flag
+
+    def place_source(self, lonmin, latmin, dlon, dlat, lon_c, lat_c, z_c, x, y, z, M):
+        nb = self.dims.nbins
+        s = np.zeros((self.g.nx, self.g.ny, self.g.nz, nb), order="F")
+        M = np.asfortranarray(M, dtype=np.float64)
+        lib().or_place_source(C.byref(self.dims), C.byref(self.cgrid), lonmin, latmin, dlon, dlat,
+                              _p(np.asfortranarray(lon_c)), _p(np.asfortranarray(lat_c)),
+                              _p(np.asfortranarray(z_c)), len(x), _p(np.asarray(x, np.float64)),
+                              _p(np.asarray(y, np.float64)), _p(np.asarray(z, np.float64)), _p(M),
+                              _p(s))
+        return s
+
+
+def kt_rhs(c, dxp, dxb, u, k, limiter=2):
+    n = len(c) - 4
+    rhs = np.zeros(n)
+    flux = np.zeros(2)
+    lib().or_kt_rhs(n, limiter, _p(np.ascontiguousarray(c, np.float64)), _p(np.ascontiguousarray(dxp, np.float64)),
+                    _p(np.ascontiguousarray(dxb, np.float64)), _p(np.ascontiguousarray(u, np.float64)),
+                    _p(np.ascontiguousarray(k, np.float64)), _p(flux), _p(rhs))
+    return rhs, flux
+
+
+def ads_solve_1d(c, dxp, dxb, u, k, dt, bvalue=(0.0, 0.0), bcode=(2, 2), limiter=2):
+    c = np.array(c, dtype=np.float64)
+    flux = np.zeros(2)
+    bc = (C.c_int * 2)(*bcode)
+    lib().or_ads_solve_1d(len(c) - 4, limiter, _p(c), _p(np.ascontiguousarray(dxp, np.float64)),
+                          _p(np.ascontiguousarray(dxb, np.float64)), _p(np.ascontiguousarray(u, np.float64)),
+                          _p(np.ascontiguousarray(k, np.float64)), dt,
+                          _p(np.asarray(bvalue, np.float64)), _p(flux), bc)
+    return c, flux
+
+
+def vset_point(diam, rhop, psi, rhoa, visc, model=2):
+    v = C.c_double()
+    it = C.c_int()
+    flag = lib().or_vset_point(diam, rhop, psi, rhoa, visc, model, C.byref(v), C.byref(it))
+    return v.value, flag, it.value
+
+
+def suzuki(np_, nbins, M0, Havl, As, Ls, zo, bin_fc):
+    z = np.zeros(np_)
+    M = np.zeros((nbins, np_), order="F")
+    lib().or_suzuki(np_, nbins, M0, Havl, As, Ls, zo, _p(np.asarray(bin_fc, np.float64)), _p(z), _p(M))
+    return z, M
+
+
+def mass_boundaries(fluxes):
+    g, l = C.c_double(), C.c_double()
+    lib().or_mass_boundaries(_p(np.asarray(fluxes, np.float64)), C.byref(g), C.byref(l))
+    return g.value, l.value
+
+
+def perturb(var_id, ptype, var, random, range_):
+    return lib().or_perturb(var_id, ptype, var, random, range_)
