@@ -10,7 +10,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfall3d_ads.so")
+LIB_PATH = os.environ.get("F3D_LIB_PATH") or os.path.join(HERE, "libfall3d_ads.so")
 
 # Every function the header declares, with its ctypes signature.
 _dp = C.POINTER(C.c_double)
@@ -42,6 +42,8 @@ SIGNATURES = {
     "f3d_ads_get_fluxes": [_vp, _dp],
     "f3d_ads_synchronize": [_vp],
     "f3d_ads_get_stream": [_vp, C.POINTER(_vp)],
+    "f3d_ads_set_profiling": [_vp, C.c_int],
+    "f3d_ads_get_profile": [_vp, _dp, _ip],
     "f3d_ads_update_vcomps": [_vp, C.c_double],
     "f3d_ads_solve_along_x": [_vp, C.c_double, _dp, _dp],
     "f3d_ads_solve_along_y": [_vp, C.c_double, _dp, _dp],

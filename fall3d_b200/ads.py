@@ -128,6 +128,16 @@ class Domain:
         check(lib().f3d_ads_get_stream(self._h, C.byref(s)), "f3d_ads_get_stream")
         return s.value or 0
 
+    def set_profiling(self, on: bool):
+        check(lib().f3d_ads_set_profiling(self._h, int(on)), "f3d_ads_set_profiling")
+
+    def get_profile(self):
+        """Accumulated ms per phase {prep, x, y, z, reduce, step} and steps."""
+        ms = np.zeros(6)
+        n = C.c_int()
+        check(lib().f3d_ads_get_profile(self._h, _p(ms), C.byref(n)), "f3d_ads_get_profile")
+        return ms, n.value
+
     def ADS_update_horizontal_vcomps(self, stime):
         check(lib().f3d_ads_update_vcomps(self._h, float(stime)), "f3d_ads_update_vcomps")
 

@@ -13,206 +13,108 @@
 #include <cuda_runtime.h>
 
 #include "f3d_common.cuh"
+#include "march.cuh"
 
 namespace f3d {
 
-// Limiter r(i) from d1 = c(i)-c(i-1), d0 = c(i+1)-c(i)  (mod_ADS.F90:1124-1223)
+// Limiter r(i) from d1 = c(i)-c(i-1), d0 = c(i+1)-c(i)  (mod_ADS.F90:1124-1223).
+// The division is taken only when |d0| >= 1e-12 (a safe divisor otherwise,
+// so zero differences never reach the slow path of the division).
 template <int LIM>
 __device__ __forceinline__ double limiter64(double d1, double d0) {
+  const bool small0 = fabs(d0) < kEps;
+  const double r = d1 / (small0 ? 1.0 : d0);
   if (LIM == 1) {
-    if (fabs(d0) < kEps) return 1.0;
-    double r = d1 / d0;
-    return fmax(0.0, fmin(1.0, r));
+    return small0 ? 1.0 : fmax(0.0, fmin(1.0, r));
   } else if (LIM == 2) {
-    if (fabs(d0) < kEps) return (fabs(d1) < kEps) ? 0.0 : 2.0;
-    double r = d1 / d0;
     double a = fmin(2.0 * r, 1.0), b = fmin(r, 2.0);
-    return fmax(fmax(0.0, a), b);
+    double v = fmax(fmax(0.0, a), b);
+    return small0 ? ((fabs(d1) < kEps) ? 0.0 : 2.0) : v;
   } else {
-    if (fabs(d0) < kEps) return (fabs(d1) < kEps) ? 0.0 : 1.5;
-    double r = d1 / d0;
-    return 1.5 * (r * r + r) / (r * r + r + 1.0);
+    double v = 1.5 * (r * r + r) / (r * r + r + 1.0);
+    return small0 ? ((fabs(d1) < kEps) ? 0.0 : 1.5) : v;
   }
 }
 
-// Register state of one RK stage walking a pencil.
-struct Stage64 {
-  double a1;     // a(q-1)
-  double a2;     // a(q-2)
-  double d1;     // a(q-1) - a(q-2)
-  double r2;     // r(q-2)
-  double F1;     // advective flux at face q-2
-  double P1;     // diffusive flux at face q-2
-  double kprev;  // diffusion at cell q-2
+// Per-pencil operations of the FP64 form, reference operation order.
+template <int LIM, int DIR>
+struct Ops64 {
+  double* cp;
+  long long cs;
+  const double* vel;   // current face velocity, face f at vel[f * vs]
+  const double* vsub;  // z: settling velocity of the bin at the same faces
+  long long vs;
+  const double* kk;    // 0.5 (k(f) + k(f-1)) at face f, same stride
+  const double4* geo;  // {dxp(p), 1/dxp(p), dxb(p), 1/dxb(p)} at geo[p + 1]
+  double dt, hdt;
+  XTile<double> xt;    // x pencils: shared-memory staging of the rows
+
+  __device__ __forceinline__ double load_c(int p) const {
+    if constexpr (DIR == DIR_X) return xt.load(p);
+    else return cp[p * cs];
+  }
+  __device__ __forceinline__ void store_c(int p, double v) {
+    if constexpr (DIR == DIR_X) xt.store(p, v);
+    else cp[p * cs] = v;
+  }
+  __device__ __forceinline__ void stage_init() { if constexpr (DIR == DIR_X) xt.init(); }
+  __device__ __forceinline__ void stage_begin(int T0) { if constexpr (DIR == DIR_X) xt.block_begin(T0); }
+  __device__ __forceinline__ void stage_end(int T0) { if constexpr (DIR == DIR_X) xt.block_end(T0); }
+  __device__ __forceinline__ void stage_finish() { if constexpr (DIR == DIR_X) xt.finish(); }
+  __device__ __forceinline__ FaceV<double> face(int f) const {
+    FaceV<double> r;
+    r.u = vel[f * vs];
+    if (DIR == DIR_Z) r.u = r.u - vsub[f * vs];  // CB%w - my_vs  (mod_ADS.F90:670)
+    r.k = kk[f * vs];
+    return r;
+  }
+  // free flow (mod_ADS.F90:1227-1326) with bvalue = 0
+  __device__ __forceinline__ double ghost_l(double c0, double uL) const {
+    return (uL > 0.0) ? 2.0 * 0.0 - c0 : c0;
+  }
+  __device__ __forceinline__ double ghost_r(double cn, double uR) const {
+    return (uR < 0.0) ? 2.0 * 0.0 - cn : cn;
+  }
+  // RK4 combinations (mod_ADS.F90:326-390) and Euler (:302)
+  __device__ __forceinline__ double euler(double c, double k) const { return c + dt * k; }
+  __device__ __forceinline__ double rk_half(double c, double k) const { return c + hdt * k; }
+  __device__ __forceinline__ double rk_new1(double c, double k) const {
+    return c + div_rn_recip(dt * k, 6.0, 1.0 / 6.0);
+  }
+  __device__ __forceinline__ double rk_add3(double nw, double k) const {
+    return nw + div_rn_recip(dt * k, 3.0, 1.0 / 3.0);
+  }
+  __device__ __forceinline__ double rk_full(double c, double k) const { return c + dt * k; }
+  __device__ __forceinline__ double rk_final(double nw, double k) const {
+    return nw + div_rn_recip(dt * k, 6.0, 1.0 / 6.0);
+  }
+
+  // KT_RHS at cell q-2 on arrival of a(q) (mod_ADS.F90:1089-1117)
+  template <bool G>
+  __device__ __forceinline__ void arrive(StageS<double>& s, int q, double a0, FaceV<double> fv,
+                                         int p, double& rhs, double& flux) const {
+    const double d0 = a0 - s.a1;
+    const double r1 = limiter64<LIM>(s.d1, d0);
+    if (!G || q >= 1) {
+      const double u = fv.u;
+      const double cl = s.a2 + 0.5 * s.h2 * s.d1;
+      const double cr = s.a1 - 0.5 * r1 * d0;
+      const double F_l = cl * u;
+      const double F_r = cr * u;
+      const double F0 = 0.5 * (F_l + F_r) - 0.5 * fabs(u) * (cr - cl);
+      const double4 g = geo[p + 1];
+      const double P0 = div_rn_recip(fv.k * s.d1, g.x, g.y);
+      flux = F0 + P0;
+      if (!G || q >= 2) rhs = div_rn_recip(P0 - s.P1, g.z, g.w) - div_rn_recip(F0 - s.F1, g.z, g.w);
+      s.F1 = F0;
+      s.P1 = P0;
+    }
+    s.a2 = s.a1;
+    s.a1 = a0;
+    s.d1 = d0;
+    s.h2 = r1;
+  }
 };
-
-// Pencil accessors for one sweep direction.
-struct Pencil {
-  int n;
-  long long c_off;     // offset of element 0 in c
-  long long c_stride;  // stride between consecutive pencil elements
-  const double* vel;   // face velocity, face f at vel[f * vstride]
-  long long vstride;
-  const double* vsub;  // z only: settling velocity subtracted from vel
-  const double* kd;    // diffusion, position p at kd[(p + 1) * kstride]
-  long long kstride;
-  const double* dxp;   // reference offset: position p at dxp[p + 2]
-  const double* dxb;   // reference offset: cell i at dxb[i + 1]
-};
-
-__device__ __forceinline__ double face_vel(const Pencil& P, int f) {
-  double v = P.vel[f * P.vstride];
-  if (P.vsub) v = v - P.vsub[f * P.vstride];
-  return v;
-}
-
-// Arrival of a(q) at a stage.  Returns true when rhs(q-2) was produced;
-// fills face-flux outputs for the boundary faces.
-template <int LIM>
-__device__ __forceinline__ bool stage_arrive(Stage64& s, const Pencil& P, int q,
-                                             double a0, double& rhs,
-                                             double& face_flux) {
-  double d0 = a0 - s.a1;
-  double r1 = limiter64<LIM>(s.d1, d0);
-  bool produced = false;
-  int f = q - 1;
-  if (q >= 1) {
-    double u = face_vel(P, f);
-    double kf = P.kd[(long long)(f + 1) * P.kstride];
-    double cl = s.a2 + 0.5 * s.r2 * s.d1;
-    double cr = s.a1 - 0.5 * r1 * d0;
-    double F_l = cl * u;
-    double F_r = cr * u;
-    double F0 = 0.5 * (F_l + F_r) - 0.5 * fabs(u) * (cr - cl);
-    double P0 = 0.5 * (kf + s.kprev) * s.d1 / P.dxp[f + 1];
-    face_flux = F0 + P0;
-    if (q >= 2) {
-      double db = P.dxb[q - 1];  // dxb(i), i = q-2
-      rhs = (P0 - s.P1) / db - (F0 - s.F1) / db;
-      produced = true;
-    }
-    s.F1 = F0;
-    s.P1 = P0;
-    s.kprev = kf;
-  } else if (q == 0) {
-    s.kprev = P.kd[0];  // diffusion at cell -1
-  }
-  s.a2 = s.a1;
-  s.a1 = a0;
-  s.d1 = d0;
-  s.r2 = r1;
-  return produced;
-}
-
-// March one pencil: free-flow ghosts, RK4 (or Euler), in-place update.
-// Returns the boundary face fluxes of the last stage (flux(1), flux(2)).
-template <int LIM, int TM>
-__device__ __forceinline__ void march64(double* __restrict__ c, const Pencil& P,
-                                        double dt, double& flux_lo,
-                                        double& flux_hi) {
-  const int n = P.n;
-  double* cp = c + P.c_off;
-  const long long cs = P.c_stride;
-  // free flow ghosts (mod_ADS.F90:1227-1326), bvalue = 0
-  double c_first = cp[0];
-  double uL = face_vel(P, 0);
-  double uR = face_vel(P, n);
-  double gL = (uL > 0.0) ? 2.0 * 0.0 - c_first : c_first;
-  double gR = 0.0;
-
-  Stage64 S1 = {0, 0, 0, 0, 0, 0, 0}, S2 = S1, S3 = S1, S4 = S1;
-  double ch0 = 0, ch1 = 0, ch2 = 0, ch3 = 0, ch4 = 0, ch5 = 0, ch6 = 0;  // c(t-m)
-  double nh0 = 0, nh1 = 0, nh2 = 0, nh3 = 0, nh4 = 0, nh5 = 0, nh6 = 0;  // new(t-2-m)
-  double ff;
-  const double hdt = 0.5 * dt;
-
-  if constexpr (TM == 1) {
-    for (int t = -2; t <= n + 1; ++t) {
-      double a;
-      if (t < 0) a = gL;
-      else if (t < n) a = cp[t * cs];
-      else a = gR;
-      ch2 = ch1; ch1 = ch0; ch0 = a;
-      if (t == n - 1) gR = (uR < 0.0) ? 2.0 * 0.0 - a : a;
-      double k1;
-      if (stage_arrive<LIM>(S1, P, t, a, k1, ff)) {
-        cp[(t - 2) * cs] = ch2 + dt * k1;
-      }
-      if (t == 1) flux_lo = ff;
-      if (t == n + 1) flux_hi = ff;
-    }
-  } else {
-#pragma unroll 1
-  for (int t = -2; t <= n + 7; ++t) {
-    // shift histories
-    ch6 = ch5; ch5 = ch4; ch4 = ch3; ch3 = ch2; ch2 = ch1; ch1 = ch0;
-    nh6 = nh5; nh5 = nh4; nh4 = nh3; nh3 = nh2; nh2 = nh1; nh1 = nh0;
-    // stage 1 arrival at q = t
-    double k1 = 0.0;
-    bool have1 = false;
-    if (t <= n + 1) {
-      double a;
-      if (t < 0) a = gL;
-      else if (t < n) a = cp[t * cs];
-      else a = gR;
-      ch0 = a;
-      if (t == n - 1) gR = (uR < 0.0) ? 2.0 * 0.0 - a : a;
-      have1 = stage_arrive<LIM>(S1, P, t, a, k1, ff);
-    }
-    // stage 2 arrival at q = t-2
-    double k2 = 0.0;
-    bool have2 = false;
-    {
-      int q = t - 2;
-      if (q >= -2 && q <= n + 1) {
-        double a;
-        if (q < 0) a = gL;
-        else if (q >= n) a = gR;
-        else {
-          a = ch2 + hdt * k1;
-          nh0 = ch2 + dt * k1 / 6.0;
-        }
-        have2 = stage_arrive<LIM>(S2, P, q, a, k2, ff);
-      }
-    }
-    // stage 3 arrival at q = t-4
-    double k3 = 0.0;
-    bool have3 = false;
-    {
-      int q = t - 4;
-      if (q >= -2 && q <= n + 1) {
-        double a;
-        if (q < 0) a = gL;
-        else if (q >= n) a = gR;
-        else {
-          a = ch4 + hdt * k2;
-          nh2 = nh2 + dt * k2 / 3.0;
-        }
-        have3 = stage_arrive<LIM>(S3, P, q, a, k3, ff);
-      }
-    }
-    // stage 4 arrival at q = t-6
-    {
-      int q = t - 6;
-      if (q >= -2 && q <= n + 1) {
-        double a;
-        if (q < 0) a = gL;
-        else if (q >= n) a = gR;
-        else {
-          a = ch6 + dt * k3;
-          nh4 = nh4 + dt * k3 / 3.0;
-        }
-        double k4;
-        if (stage_arrive<LIM>(S4, P, q, a, k4, ff)) {
-          cp[(q - 2) * cs] = nh6 + dt * k4 / 6.0;
-        }
-        if (q == 1) flux_lo = ff;
-        if (q == n + 1) flux_hi = ff;
-      }
-    }
-  }
-  }
-}
 
 // Deterministic block reduction of two doubles (pairwise tree in smem).
 __device__ __forceinline__ void block_reduce2(double a, double b, double* out) {
@@ -236,79 +138,79 @@ __device__ __forceinline__ void block_reduce2(double a, double b, double* out) {
 
 template <int DIR, int LIM, int TM>
 __global__ void __launch_bounds__(128) k_sweep64(const MemberDev* __restrict__ members,
-                                                 const WorkItem* __restrict__ work) {
+                                                 const WorkItem* __restrict__ work, int bpb) {
   const WorkItem w = work[blockIdx.x];
   const MemberDev& m = members[w.member];
   const int nx = m.nx, ny = m.ny, nz = m.nz;
-  const long long npen = (DIR == DIR_X) ? (long long)ny * nz * m.nb
-                         : (DIR == DIR_Y) ? (long long)nx * nz * m.nb
-                                          : (long long)nx * ny * m.nb;
-  const long long pen = (long long)w.pen0 + threadIdx.x;
-  double lo = 0.0, hi = 0.0;
+  const long long nsp = (DIR == DIR_X) ? (long long)ny * nz
+                        : (DIR == DIR_Y) ? (long long)nx * nz : (long long)nx * ny;
+  extern __shared__ __align__(16) unsigned char f3d_smem[];
+  const int warp = threadIdx.x >> 5;
+  const long long pen_raw = (long long)w.pen0 + 32 * (warp / bpb) + (threadIdx.x & 31);
+  const long long pen0w = (long long)w.pen0 + 32 * (warp / bpb);
+  const int b = w.bin0 + warp % bpb;
+  const bool lane_ok = pen_raw < nsp && b < m.nb;
+  // x pencils march as a whole warp (the staging is warp-collective); lanes
+  // past the end replay the last pencil without storing
+  const bool run_it = (DIR == DIR_X) ? (pen0w < nsp && b < m.nb) : lane_ok;
+  const long long pen = pen_raw < nsp ? pen_raw : nsp - 1;
   double clo = 0.0, chi = 0.0;  // contributions flux*area*dt
-  if (pen < npen) {
-    Pencil P;
+  if (run_it) {
+    Ops64<LIM, DIR> o;
     double area;
-    const double dt = m.dt;
+    int n, i = 0, j = 0;
     if (DIR == DIR_X) {
-      int j = (int)(pen % ny);
-      long long t = pen / ny;
-      int k = (int)(t % nz);
-      int b = (int)(t / nz);
-      P.n = nx;
-      P.c_off = (((long long)b * nz + k) * ny + j) * nx;
-      P.c_stride = 1;
-      P.vel = m.ucur + (long long)k * (nx + 1) * ny + j;
-      P.vstride = ny;
-      P.vsub = nullptr;
-      P.kd = m.k1x + (long long)k * (nx + 2) * ny + j;
-      P.kstride = ny;
-      P.dxp = m.dx1p;
-      P.dxb = m.dx1b;
+      j = (int)(pen % ny);
+      int k = (int)(pen / ny);
+      n = nx;
+      o.cp = m.c64 + (((long long)b * nz + k) * ny + j) * nx;
+      o.xt.setup(f3d_smem + warp * XTile<double>::BYTES, lane_ok ? o.cp : nullptr,
+                 threadIdx.x & 31, nx);
+      o.cs = 1;
+      long long fo = (long long)k * (nx + 1) * ny + j;
+      o.vel = m.ucur + fo;
+      o.kk = m.kkf[0] + fo;
+      o.vs = ny;
+      o.vsub = nullptr;
       area = m.dx3b[k + 1] * m.dx2b[j + 1];
     } else if (DIR == DIR_Y) {
-      int i = (int)(pen % nx);
-      long long t = pen / nx;
-      int k = (int)(t % nz);
-      int b = (int)(t / nz);
-      P.n = ny;
-      P.c_off = ((long long)b * nz + k) * ny * (long long)nx + i;
-      P.c_stride = nx;
-      P.vel = m.vcur + (long long)k * (ny + 1) * nx + i;
-      P.vstride = nx;
-      P.vsub = nullptr;
-      P.kd = m.k2y + (long long)k * (ny + 2) * nx + i;
-      P.kstride = nx;
-      P.dxp = m.dx2p;
-      P.dxb = m.dx2b;
+      i = (int)(pen % nx);
+      int k = (int)(pen / nx);
+      n = ny;
+      o.cp = m.c64 + ((long long)b * nz + k) * ny * (long long)nx + i;
+      o.cs = nx;
+      long long fo = (long long)k * (ny + 1) * nx + i;
+      o.vel = m.vcur + fo;
+      o.kk = m.kkf[1] + fo;
+      o.vs = nx;
+      o.vsub = nullptr;
       area = m.dx3b[k + 1] * m.dx1b[i + 1];
     } else {
-      int i = (int)(pen % nx);
-      long long t = pen / nx;
-      int j = (int)(t % ny);
-      int b = (int)(t / ny);
-      P.n = nz;
-      P.c_off = (long long)b * nz * ny * nx + (long long)j * nx + i;
-      P.c_stride = (long long)nx * ny;
-      P.vel = m.wcur + (long long)j * nx + i;
-      P.vstride = (long long)nx * ny;
-      P.vsub = m.vs + (long long)b * (nz + 1) * ny * nx + (long long)j * nx + i;
-      P.kd = m.k3z + (long long)j * nx + i;
-      P.kstride = (long long)nx * ny;
-      P.dxp = m.dx3p;
-      P.dxb = m.dx3b;
+      i = (int)(pen % nx);
+      j = (int)(pen / nx);
+      n = nz;
+      o.cp = m.c64 + (long long)b * nz * ny * nx + (long long)j * nx + i;
+      o.cs = (long long)nx * ny;
+      long long fo = (long long)j * nx + i;
+      o.vel = m.wcur + fo;
+      o.kk = m.kkf[2] + fo;
+      o.vs = (long long)nx * ny;
+      o.vsub = m.vs + (long long)b * (nz + 1) * ny * nx + fo;
       area = m.dx2b[j + 1] * m.dx1b[i + 1];
     }
-    march64<LIM, TM>(m.c64, P, dt, lo, hi);
-    clo = lo * area * dt;
-    chi = hi * area * dt;
+    o.geo = m.geo[DIR];
+    o.dt = m.dt;
+    o.hdt = 0.5 * m.dt;
+    March<double, Ops64<LIM, DIR>, TM> M(o, n);
+    M.run();
+    const double dt = m.dt;
+    if (lane_ok) {
+      clo = M.flux_lo * area * dt;
+      chi = M.flux_hi * area * dt;
+    }
     if (DIR == DIR_Z) {
-      int i = (int)(pen % nx);
-      long long t = pen / nx;
-      int j = (int)(t % ny);
-      int b = (int)(t / ny);
       double* a = m.acum + ((long long)b * ny + j) * nx + i;
-      *a = *a + fabs(lo) * dt;
+      *a = *a + fabs(M.flux_lo) * dt;  // mod_ADS.F90:791
     }
   }
   block_reduce2(clo, chi, m.flux_part + 2 * (long long)w.slot);
@@ -317,9 +219,20 @@ __global__ void __launch_bounds__(128) k_sweep64(const MemberDev* __restrict__ m
 // Host launchers -------------------------------------------------------------
 template <int DIR>
 static void launch_dir64(int lim, int tm, const MemberDev* members,
-                         const WorkItem* work, int nblocks, cudaStream_t st) {
+                         const WorkItem* work, int nblocks, int bpb, cudaStream_t st) {
   dim3 g(nblocks), b(128);
-#define F3D_L(L, T) k_sweep64<DIR, L, T><<<g, b, 0, st>>>(members, work)
+  const int smem = (DIR == DIR_X) ? 4 * XTile<double>::BYTES : 0;
+  static bool attr_set = false;
+  if (!attr_set && smem > 0) {
+    cudaFuncSetAttribute(k_sweep64<DIR, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64<DIR, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64<DIR, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64<DIR, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64<DIR, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64<DIR, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr_set = true;
+  }
+#define F3D_L(L, T) k_sweep64<DIR, L, T><<<g, b, smem, st>>>(members, work, bpb)
   if (tm == 1) {
     if (lim == 1) F3D_L(1, 1); else if (lim == 2) F3D_L(2, 1); else F3D_L(3, 1);
   } else {
@@ -329,11 +242,11 @@ static void launch_dir64(int lim, int tm, const MemberDev* members,
 }
 
 void launch_sweep64(int dir, int lim, int tm, const MemberDev* members,
-                    const WorkItem* work, int nblocks, cudaStream_t st) {
+                    const WorkItem* work, int nblocks, int bpb, cudaStream_t st) {
   if (nblocks <= 0) return;
-  if (dir == DIR_X) launch_dir64<DIR_X>(lim, tm, members, work, nblocks, st);
-  else if (dir == DIR_Y) launch_dir64<DIR_Y>(lim, tm, members, work, nblocks, st);
-  else launch_dir64<DIR_Z>(lim, tm, members, work, nblocks, st);
+  if (dir == DIR_X) launch_dir64<DIR_X>(lim, tm, members, work, nblocks, bpb, st);
+  else if (dir == DIR_Y) launch_dir64<DIR_Y>(lim, tm, members, work, nblocks, bpb, st);
+  else launch_dir64<DIR_Z>(lim, tm, members, work, nblocks, bpb, st);
 }
 
 // Per-step preparation: current winds u,v,w = (1-s) x1 + s x2

@@ -170,6 +170,48 @@ void launch_conv(int which, const double* in, double* out, int nx, int ny, int n
   }
 }
 
+// ---- FP64 face diffusion 0.5 (k(f) + k(f-1)) (the P term of KT_RHS,
+// mod_ADS.F90:1111-1112), once per meteo update, for every face
+__global__ void k_face_kk(MemberDev* members, int mi) {
+  MemberDev& m = members[mi];
+  const int nx = m.nx, ny = m.ny, nz = m.nz;
+  const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)(ny + 1) * nx * nz,
+                  nw = (long long)(nz + 1) * nx * ny;
+  GRID_STRIDE(e, nu + nv + nw) {
+    long long q = e;
+    if (q < nu) {  // [k][f][j], k1x [k][p+1][j]
+      int j = (int)(q % ny);
+      long long t = q / ny;
+      int f = (int)(t % (nx + 1));
+      int k = (int)(t / (nx + 1));
+      const double* kk = m.k1x + (long long)k * (nx + 2) * ny + j;
+      const_cast<double*>(m.kkf[0])[q] = 0.5 * (kk[(long long)(f + 1) * ny] + kk[(long long)f * ny]);
+      continue;
+    }
+    q -= nu;
+    if (q < nv) {  // [k][f][i], k2y [k][p+1][i]
+      int i = (int)(q % nx);
+      long long t = q / nx;
+      int f = (int)(t % (ny + 1));
+      int k = (int)(t / (ny + 1));
+      const double* kk = m.k2y + (long long)k * (ny + 2) * nx + i;
+      const_cast<double*>(m.kkf[1])[q] = 0.5 * (kk[(long long)(f + 1) * nx] + kk[(long long)f * nx]);
+      continue;
+    }
+    q -= nv;
+    {  // [f][j][i], k3z [p+1][j][i]
+      long long plane = (long long)nx * ny;
+      long long ij = q % plane;
+      int f = (int)(q / plane);
+      const double* kk = m.k3z + ij;
+      const_cast<double*>(m.kkf[2])[q] = 0.5 * (kk[(long long)(f + 1) * plane] + kk[(long long)f * plane]);
+    }
+  }
+}
+void launch_face_kk(MemberDev* members, int mi, cudaStream_t st) {
+  k_face_kk<<<1184, 256, 0, st>>>(members, mi);
+}
+
 // ---- per-step parameters (kernel arguments are captured at launch) -------
 __global__ void k_set_step(MemberDev* members, int mi, double dt, double time, int iiter) {
   MemberDev& m = members[mi];

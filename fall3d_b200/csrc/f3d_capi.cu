@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -16,7 +17,7 @@
 namespace f3d {
 // ads_fp64.cu
 void launch_sweep64(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
-                    int nblocks, cudaStream_t st);
+                    int nblocks, int bpb, cudaStream_t st);
 void launch_prep64(const MemberDev* members, const int* blk_member, const int* blk_first,
                    int nblocks, int mask, cudaStream_t st);
 void launch_source64(const MemberDev* members, int nmembers, cudaStream_t st);
@@ -38,9 +39,10 @@ void launch_vset_points(int model, int n, const double* diam, const double* rhop
 void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc,
                        const double* tc, const double* bin_par, const int* bin_flags,
                        double vset_fac, int* nfail, cudaStream_t st);
+void launch_face_kk(MemberDev* members, int mi, cudaStream_t st);
 // ads_fp32.cu
 void launch_sweep32(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
-                    int nblocks, cudaStream_t st);
+                    int nblocks, int bpb, cudaStream_t st);
 void launch_prep32(const MemberDev* members, const int* blk_member, const int* blk_first,
                    int nblocks, int mask, cudaStream_t st);
 void launch_source32(const MemberDev* members, int nmembers, cudaStream_t st);
@@ -78,7 +80,7 @@ static int set_err(const char* fmt, ...) {
                      __LINE__);                                                        \
   } while (0)
 
-static const int kSweepBlock = 128;
+static const int kSweepWarps = 4;  // warps per sweep block (128 threads)
 static const int kPrepBlock = 256;
 
 struct f3d_ctx {
@@ -91,6 +93,7 @@ struct f3d_ctx {
   int* dprep_member = nullptr;
   int* dprep_first = nullptr;
   int nprep = 0;
+  int bpb = 4;  // bins per sweep block (1, 2 or 4); warps of a block share a spatial tile
   std::vector<void*> allocs;
   double* staging = nullptr;
   size_t staging_elems = 0;
@@ -105,6 +108,11 @@ struct f3d_ctx {
   int src_cap = 0;
   double* d_rhoc_tc = nullptr;
   size_t rhoc_cap = 0;
+  // per-phase profiling
+  bool prof = false;
+  cudaEvent_t ev[8] = {};
+  double prof_ms[6] = {0, 0, 0, 0, 0, 0};
+  int prof_steps = 0;
 };
 
 template <class T>
@@ -126,13 +134,18 @@ static int upload_member(f3d_ctx* c) {
 // Build the work lists: blocks of 128 pencils per direction, one partial
 // slot per block.
 static int build_work(f3d_ctx* c) {
-  long long npen[3] = {(long long)c->ny * c->nz * c->nb, (long long)c->nx * c->nz * c->nb,
-                       (long long)c->nx * c->ny * c->nb};
+  long long nsp[3] = {(long long)c->ny * c->nz, (long long)c->nx * c->nz,
+                      (long long)c->nx * c->ny};
+  const int bpb = c->bpb;
+  const int span = 32 * (kSweepWarps / bpb);  // spatial pencils per block
+  const int nbg = (c->nb + bpb - 1) / bpb;
   int slot = 0;
   for (int d = 0; d < 3; ++d) {
-    int nb = (int)((npen[d] + kSweepBlock - 1) / kSweepBlock);
+    const int ng = (int)((nsp[d] + span - 1) / span);
+    const int nb = ng * nbg;
     std::vector<WorkItem> w(nb);
-    for (int q = 0; q < nb; ++q) w[q] = WorkItem{0, q * kSweepBlock, slot + q, 0};
+    for (int g = 0, q = 0; g < ng; ++g)
+      for (int bg = 0; bg < nbg; ++bg, ++q) w[q] = WorkItem{0, span * g, bg * bpb, slot + q};
     c->hm.part_base[d] = slot;
     c->hm.part_count[d] = nb;
     slot += nb;
@@ -176,6 +189,10 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
   f3d_ctx* c = new f3d_ctx();
   c->nx = dims->nx; c->ny = dims->ny; c->nz = dims->nz; c->nb = dims->nbins;
   c->lim = limiter; c->tm = time_marching; c->prec = precision; c->device = device;
+  if (const char* e = getenv("F3D_BINS_PER_BLOCK")) {
+    int v = atoi(e);
+    if (v == 1 || v == 2 || v == 4) c->bpb = v;
+  }
   memset(&c->hm, 0, sizeof(MemberDev));
   MemberDev& m = c->hm;
   m.nx = c->nx; m.ny = c->ny; m.nz = c->nz; m.nb = c->nb;
@@ -202,6 +219,13 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
     rc |= dalloc(c, &m.ucur, (nx + 1) * ny * nz);
     rc |= dalloc(c, &m.vcur, (ny + 1) * nx * nz);
     rc |= dalloc(c, &m.wcur, (nz + 1) * nx * ny);
+    rc |= dalloc(c, &tmp, (nx + 1) * ny * nz); m.kkf[0] = tmp;
+    rc |= dalloc(c, &tmp, (ny + 1) * nx * nz); m.kkf[1] = tmp;
+    rc |= dalloc(c, &tmp, (nz + 1) * nx * ny); m.kkf[2] = tmp;
+    double4* g4;
+    rc |= dalloc(c, &g4, nx + 1); m.geo[0] = g4;
+    rc |= dalloc(c, &g4, ny + 1); m.geo[1] = g4;
+    rc |= dalloc(c, &g4, nz + 1); m.geo[2] = g4;
   } else {
     float* f;
     rc |= dalloc(c, &f, 2 * (nx + 1) * ny * nz); m.ux32[0] = f; m.ux32[1] = f + (nx + 1) * ny * nz;
@@ -211,9 +235,6 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
     rc |= dalloc(c, &f, (ny + 1) * nx * nz); m.kfy = f;
     rc |= dalloc(c, &f, (nz + 1) * nx * ny); m.kfz = f;
     rc |= dalloc(c, &f, nb * (nz + 1) * nx * ny); m.vs32 = f;
-    rc |= dalloc(c, &m.ucur32, (nx + 1) * ny * nz);
-    rc |= dalloc(c, &m.vcur32, (ny + 1) * nx * nz);
-    rc |= dalloc(c, &m.wcur32, (nz + 1) * nx * ny);
     rc |= dalloc(c, &f, nx); m.rdx1b32 = f;
     rc |= dalloc(c, &f, ny); m.rdx2b32 = f;
     rc |= dalloc(c, &f, nz); m.rdx3b32 = f;
@@ -262,6 +283,8 @@ extern "C" int f3d_ads_destroy(f3d_ctx* c) {
   for (void* p : c->allocs) cudaFree(p);
   if (c->d_rhoc_tc) cudaFree(c->d_rhoc_tc);
   if (c->h_pin) cudaFreeHost(c->h_pin);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return 0;
@@ -294,6 +317,24 @@ extern "C" int f3d_ads_set_grid(f3d_ctx* c, const double* dX1_p, const double* d
   c->Hm1_p.assign(Hm1_p, Hm1_p + ny);
   c->Hm2_p.assign(Hm2_p, Hm2_p + ny + 4);
   c->Hm3_p.assign(Hm3_p, Hm3_p + nx * ny);
+  if (c->prec == F3D_PREC_FP64) {
+    // geo[p+1] = {dxp(p), RN(1/dxp(p)), dxb(p), RN(1/dxb(p))}, p = -1..n-1
+    // (reference offsets +2 / +1); the reciprocals feed div_rn_recip
+    const double* dp[3] = {dX1_p, dX2_p, dX3_p};
+    const double* db[3] = {dX1_b, dX2_b, dX3_b};
+    const size_t nn[3] = {nx, ny, nz};
+    for (int d = 0; d < 3; ++d) {
+      std::vector<double4> g(nn[d] + 1);
+      for (size_t q = 0; q <= nn[d]; ++q) {
+        double a = dp[d][q + 1], b = db[d][q];
+        if (!(std::fabs(a) >= 0x1p-100 && std::fabs(a) <= 0x1p100 && std::fabs(b) >= 0x1p-100 &&
+              std::fabs(b) <= 0x1p100))
+          return set_err("f3d_ads_set_grid: grid spacing %g / %g outside [2^-100, 2^100]", a, b);
+        g[q] = make_double4(a, 1.0 / a, b, 1.0 / b);
+      }
+      CK(cudaMemcpy((void*)m.geo[d], g.data(), g.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    }
+  }
   if (c->prec == F3D_PREC_FP32) {
     std::vector<float> r1(nx), r2(ny), r3(nz);
     for (size_t i = 0; i < nx; ++i) r1[i] = (float)(1.0 / dX1_b[i + 1]);
@@ -342,9 +383,11 @@ extern "C" int f3d_ads_set_meteo(f3d_ctx* c, const double* u, const double* v, c
   if (upload_member(c)) return 1;
   if (c->prec == F3D_PREC_FP32) {
     launch_fp32_fields(c->dm, 0, c->st);
-    CKL();
-    CK(cudaStreamSynchronize(c->st));
+  } else {
+    launch_face_kk(c->dm, 0, c->st);
   }
+  CKL();
+  CK(cudaStreamSynchronize(c->st));
   c->meteo_set = true;
   return 0;
 }
@@ -494,9 +537,9 @@ extern "C" int f3d_ads_download_state(f3d_ctx* c, double* my_c, double* my_acum)
 // ---- step ---------------------------------------------------------------
 static int enqueue_sweep(f3d_ctx* c, int dir) {
   if (c->prec == F3D_PREC_FP64)
-    launch_sweep64(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->st);
+    launch_sweep64(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
   else
-    launch_sweep32(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->st);
+    launch_sweep32(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
   CKL();
   return 0;
 }
@@ -526,17 +569,55 @@ static int check_ready(f3d_ctx* c, const char* who) {
 }
 
 static int enqueue_step(f3d_ctx* c, double dt, double time, int iiter) {
+  // event slots: 0 start, 1 after prep+source, 2..4 after the 1st/2nd/z sweep, 5 end
+  auto rec = [&](int k) { if (c->prof) cudaEventRecord(c->ev[k], c->st); };
+  rec(0);
   launch_set_step(c->dm, 0, dt, time, iiter, c->st);
   CKL();
   if (enqueue_prep(c, 7) || enqueue_source(c)) return 1;
-  if (iiter % 2 == 0) {  // mod_F3D.F90:1477-1487
-    if (enqueue_sweep(c, DIR_X) || enqueue_sweep(c, DIR_Y)) return 1;
-  } else {
-    if (enqueue_sweep(c, DIR_Y) || enqueue_sweep(c, DIR_X)) return 1;
-  }
+  rec(1);
+  const bool xfirst = (iiter % 2 == 0);  // mod_F3D.F90:1477-1487
+  if (enqueue_sweep(c, xfirst ? DIR_X : DIR_Y)) return 1;
+  rec(2);
+  if (enqueue_sweep(c, xfirst ? DIR_Y : DIR_X)) return 1;
+  rec(3);
   if (enqueue_sweep(c, DIR_Z)) return 1;
+  rec(4);
   launch_flux_reduce(c->dm, 1, 7, c->st);
   CKL();
+  rec(5);
+  if (c->prof) {
+    CK(cudaEventSynchronize(c->ev[5]));
+    float t[5];
+    for (int k = 0; k < 5; ++k) CK(cudaEventElapsedTime(&t[k], c->ev[k], c->ev[k + 1]));
+    c->prof_ms[0] += t[0];
+    c->prof_ms[xfirst ? 1 : 2] += t[1];
+    c->prof_ms[xfirst ? 2 : 1] += t[2];
+    c->prof_ms[3] += t[3];
+    c->prof_ms[4] += t[4];
+    float tot;
+    CK(cudaEventElapsedTime(&tot, c->ev[0], c->ev[5]));
+    c->prof_ms[5] += tot;
+    c->prof_steps += 1;
+  }
+  return 0;
+}
+
+extern "C" int f3d_ads_set_profiling(f3d_ctx* c, int on) {
+  if (!c) return set_err("f3d_ads_set_profiling: null context");
+  CK(cudaSetDevice(c->device));
+  if (on && !c->ev[0])
+    for (auto& e : c->ev) CK(cudaEventCreate(&e));
+  c->prof = on != 0;
+  for (double& x : c->prof_ms) x = 0.0;
+  c->prof_steps = 0;
+  return 0;
+}
+
+extern "C" int f3d_ads_get_profile(f3d_ctx* c, double ms[6], int* nsteps) {
+  if (!c || !ms) return set_err("f3d_ads_get_profile: null argument");
+  for (int k = 0; k < 6; ++k) ms[k] = c->prof_ms[k];
+  if (nsteps) *nsteps = c->prof_steps;
   return 0;
 }
 

@@ -18,6 +18,8 @@
 // Pencils: x-pencil (j,k,bin) lanes over j; y-pencil (i,k,bin) and
 // z-pencil (i,j,bin) lanes over i, so y/z loads are fully coalesced.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 namespace f3d {
@@ -40,6 +42,11 @@ struct MemberDev {
   const double* k2y;
   const double* k3z;
   const double* vs;
+  // FP64 face data of the exact form, per direction (0 x, 1 y, 2 z):
+  //   geo[d][p+1] = {dxp(p), 1/dxp(p), dxb(p), 1/dxb(p)} for p = -1..n-1
+  //   kkf[d] = 0.5 (k(f) + k(f-1)) at every face, laid out like the winds
+  const double4* geo[3];
+  const double* kkf[3];
   // FP32 copies for the precision form (null when unused)
   const float* ux32[2];
   const float* vy32[2];
@@ -90,12 +97,35 @@ struct MemberDev {
   double* flux_step;  // this step's increments {W,E,S,N,U,D}
 };
 
-// A block of one sweep: pencils [pen0, pen0 + blockDim) of one member.
+// A block of one sweep: 32 consecutive spatial pencils [pen0, pen0+32) of
+// one member, one warp per bin [bin0, bin0 + blockDim/32).  Spatial pencil
+// index: x (j + ny k), y (i + nx k), z (i + nx j).  Blocks of the same
+// spatial tile are adjacent in the work list, so the face data they share
+// is served from L1/L2 instead of DRAM once per bin.
 struct WorkItem {
   int member;
   int pen0;
+  int bin0;
   int slot;  // flux partial slot
-  int pad;
 };
+
+// Correctly rounded a/b for a divisor with precomputed y = RN(1/b)
+// (Markstein's correction, applied twice so that the second correction
+// starts from a faithful quotient; P. Markstein, IBM J. Res. Dev. 34(1),
+// 1990).  Branch-free: numerators below 2^-800 are first scaled by 2^400
+// (exact) so no intermediate is subnormal, and zero numerators return the
+// correctly signed zero a*y.  Exact IEEE round-to-nearest whenever the
+// quotient is a normal number and |b| is in [2^-100, 2^100].
+__device__ __forceinline__ double div_rn_recip(double a, double b, double y) {
+  const bool tiny = fabs(a) < 0x1p-800;
+  const double sa = tiny ? a * 0x1p400 : a;
+  double q = sa * y;
+  double r = fma(-q, b, sa);
+  q = fma(r, y, q);
+  r = fma(-q, b, sa);
+  q = fma(r, y, q);
+  q = tiny ? q * 0x1p-400 : q;
+  return (a == 0.0) ? a * y : q;
+}
 
 }  // namespace f3d

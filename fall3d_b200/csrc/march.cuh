@@ -1,0 +1,262 @@
+// march.cuh -- the pipelined single-pass RK pencil march shared by the FP64
+// and FP32 sweep kernels.
+//
+// One thread owns one pencil of one bin.  KT_RHS at cell i reads cells
+// i-2..i+2 (mod_ADS.F90:1057-1120), so RK stage s can run two cells behind
+// stage s-1: at march time t, stage s receives its input at q = t - 2(s-1)
+// and emits its right-hand side at q - 2.  The pencil is read once and
+// written once; the stage inputs the reference keeps in whole-pencil arrays
+// (c0, new_c, ini_c) live in registers.
+//
+// The march runs in blocks of 8 time steps with compile-time ring indices,
+// so the per-position histories (input c, new_c accumulator, face data)
+// rotate by register renaming.  Blocks entirely inside the steady range
+// [8, n-2] (every stage interior) run without edge guards.
+#pragma once
+#ifndef F3D_COMMON_SKIP
+#include "f3d_common.cuh"
+#endif
+
+namespace f3d {
+
+template <class T>
+struct FaceV {
+  T u;  // face-normal velocity (z: w - vs of the bin)
+  T k;  // diffusion at the face (FP64: 0.5 (k_f + k_f-1); FP32: that / dxp)
+};
+
+// Per-warp shared-memory staging of x pencils.  The 32 lanes of a warp own
+// 32 rows of the x-contiguous concentration; lanes read their own row from a
+// transposed tile while the warp moves whole 128-byte row segments between
+// HBM and the tile (coalesced), double-buffered in both directions.
+template <class T>
+struct XTile {
+  static constexpr int W = 128 / (int)sizeof(T);  // positions per chunk
+  static constexpr int LDW = W + 1;               // padded row pitch
+  static constexpr int RPI = 32 / W;              // rows per warp instruction
+  static constexpr int BYTES = 4 * 32 * LDW * (int)sizeof(T) + 32 * 8;
+  T* in;            // [2][32][LDW]
+  T* out;           // [2][32][LDW]
+  T* const* rows;   // [32] row base pointers, null for lanes without a pencil
+  int lane, n, next_flush;
+
+  __device__ __forceinline__ void setup(void* base, T* my_row, int lane_, int n_) {
+    in = reinterpret_cast<T*>(base);
+    out = in + 2 * 32 * LDW;
+    T** r = reinterpret_cast<T**>(out + 2 * 32 * LDW);
+    r[lane_] = my_row;
+    rows = r;
+    lane = lane_;
+    n = n_;
+    next_flush = 0;
+    __syncwarp();
+  }
+  __device__ __forceinline__ void load_chunk(int m) {
+    const int p0 = m * W, sub = lane / W, col = lane % W;
+    T* dst = in + (m & 1) * 32 * LDW;
+#pragma unroll 8
+    for (int r0 = 0; r0 < 32; r0 += RPI) {
+      const int r = r0 + sub, p = p0 + col;
+      const T* rp = rows[r];
+      T v = T(0);
+      if (rp && p < n) v = rp[p];
+      dst[r * LDW + col] = v;
+    }
+  }
+  __device__ __forceinline__ void flush_chunk(int m) {
+    const int p0 = m * W, sub = lane / W, col = lane % W;
+    const T* src = out + (m & 1) * 32 * LDW;
+#pragma unroll 8
+    for (int r0 = 0; r0 < 32; r0 += RPI) {
+      const int r = r0 + sub, p = p0 + col;
+      T* rp = rows[r];
+      if (rp && p < n) rp[p] = src[r * LDW + col];
+    }
+  }
+  __device__ __forceinline__ T load(int p) const {
+    return in[((p / W) & 1) * 32 * LDW + lane * LDW + (p % W)];
+  }
+  __device__ __forceinline__ void store(int p, T v) const {
+    out[((p / W) & 1) * 32 * LDW + lane * LDW + (p % W)] = v;
+  }
+  // hooks driven by the march (warp-uniform)
+  __device__ __forceinline__ void init() {
+    load_chunk(0);
+    __syncwarp();
+  }
+  __device__ __forceinline__ void block_begin(int T0) {
+    if (T0 >= 0 && T0 % W == 0 && (T0 / W + 1) * W < n) load_chunk(T0 / W + 1);
+    __syncwarp();
+  }
+  __device__ __forceinline__ void block_end(int T0) {
+    // chunk m is complete after block (m+1)W and its buffer is rewritten from
+    // block (m+2)W on (RK4 writes position p at t = p+8, Euler at t = p+2)
+    if (T0 >= W && T0 % W == 0) {
+      __syncwarp();
+      flush_chunk(T0 / W - 1);
+      next_flush = T0 / W;
+    }
+  }
+  __device__ __forceinline__ void finish() {
+    __syncwarp();
+    for (int m = next_flush; m * W < n; ++m) flush_chunk(m);
+  }
+};
+
+// Default (no staging) hooks for y and z pencils.
+struct NoStage {
+  __device__ __forceinline__ void init() {}
+  __device__ __forceinline__ void block_begin(int) {}
+  __device__ __forceinline__ void block_end(int) {}
+  __device__ __forceinline__ void finish() {}
+};
+
+template <class T>
+struct StageS {
+  T a1, a2, d1, h2, F1, P1;  // a(q-1), a(q-2), a(q-1)-a(q-2), limiter at q-2, fluxes at face q-2
+};
+
+// Pipeline over a pencil.  Ops supplies (all __device__ __forceinline__):
+//   T    load_c(int p)                     concentration at pencil position p
+//   void store_c(int p, T v)
+//   FaceV<T> face(int f)                   face data, f in [0, n]
+//   T    arrive<G>(StageS&, int q, T a0, FaceV<T> fv, int p, T& rhs, T& flux)
+//        -> returns nothing; sets rhs (valid when q >= 2) and flux (face q-1)
+//   T    ghost_l(T c0, T uL) / ghost_r(T cn, T uR)  free-flow ghost values
+//   rk:  a2 = c + hdt k, new = c + dt6 k, ... provided as methods
+template <class T, class Ops, int TM>
+struct March {
+  Ops& o;
+  const int n;
+  T ch[8];           // c(p) at ch[p & 7]
+  T nh[8];           // new_c(p) at nh[p & 7]
+  FaceV<T> fw[8];    // face(f) at fw[f & 7]
+  StageS<T> S1, S2, S3, S4;
+  T gL, gR, uR, cn1, cn2;
+  T flux_lo, flux_hi;
+
+  __device__ __forceinline__ March(Ops& ops, int n_) : o(ops), n(n_) {}
+
+  template <int U, bool G>
+  __device__ __forceinline__ void iter(int t) {
+    constexpr int m1 = (U + 7) & 7, m2 = (U + 6) & 7, m3 = (U + 5) & 7, m4 = (U + 4) & 7,
+                  m5 = (U + 3) & 7, m6 = (U + 2) & 7, m7 = (U + 1) & 7;
+    T k1 = T(0), k2 = T(0), k3 = T(0), k4 = T(0), ff = T(0);
+    // ---- stage 1: arrival at q = t
+    if (!G || (t >= -2 && t <= n + 1)) {
+      T a;
+      if (G) {
+        a = (t < 0) ? gL : ((t < n) ? cn1 : gR);
+        cn1 = cn2;
+        if (t + 2 >= 0 && t + 2 < n) cn2 = o.load_c(t + 2);
+        if (t == n - 1) gR = o.ghost_r(a, uR);
+        if (t >= 0 && t <= n) fw[U] = o.face(t);
+      } else {
+        a = cn1;
+        cn1 = cn2;
+        cn2 = o.load_c(min(t + 2, n - 1));
+        fw[U] = o.face(t);
+      }
+      ch[U] = a;
+      o.template arrive<G>(S1, t, a, fw[m1], t - 2, k1, ff);
+    }
+    if constexpr (TM == 1) {
+      if (!G || (t >= 2 && t <= n + 1)) o.store_c(t - 2, o.euler(ch[m2], k1));
+      if (G && t == 1) flux_lo = ff;
+      if (G && t == n + 1) flux_hi = ff;
+      return;
+    } else {
+    // ---- stage 2: q = t-2
+    {
+      const int q = t - 2;
+      if (!G || (q >= -2 && q <= n + 1)) {
+        T a;
+        if (G && q < 0) a = gL;
+        else if (G && q >= n) a = gR;
+        else {
+          a = o.rk_half(ch[m2], k1);
+          nh[m2] = o.rk_new1(ch[m2], k1);
+        }
+        o.template arrive<G>(S2, q, a, fw[m3], q - 2, k2, ff);
+      }
+    }
+    // ---- stage 3: q = t-4
+    {
+      const int q = t - 4;
+      if (!G || (q >= -2 && q <= n + 1)) {
+        T a;
+        if (G && q < 0) a = gL;
+        else if (G && q >= n) a = gR;
+        else {
+          a = o.rk_half(ch[m4], k2);
+          nh[m4] = o.rk_add3(nh[m4], k2);
+        }
+        o.template arrive<G>(S3, q, a, fw[m5], q - 2, k3, ff);
+      }
+    }
+    // ---- stage 4: q = t-6, output at t-8
+    {
+      const int q = t - 6;
+      if (!G || (q >= -2 && q <= n + 1)) {
+        T a;
+        if (G && q < 0) a = gL;
+        else if (G && q >= n) a = gR;
+        else {
+          a = o.rk_full(ch[m6], k3);
+          nh[m6] = o.rk_add3(nh[m6], k3);
+        }
+        o.template arrive<G>(S4, q, a, fw[m7], q - 2, k4, ff);
+        if (!G || (q >= 2)) o.store_c(q - 2, o.rk_final(nh[U], k4));
+        if (G && q == 1) flux_lo = ff;
+        if (G && q == n + 1) flux_hi = ff;
+      }
+    }
+    }
+  }
+
+  template <bool G>
+  __device__ __forceinline__ void block8(int T0) {
+    iter<0, G>(T0);
+    iter<1, G>(T0 + 1);
+    iter<2, G>(T0 + 2);
+    iter<3, G>(T0 + 3);
+    iter<4, G>(T0 + 4);
+    iter<5, G>(T0 + 5);
+    iter<6, G>(T0 + 6);
+    iter<7, G>(T0 + 7);
+  }
+
+  __device__ __forceinline__ void run() {
+    o.stage_init();
+    T c0 = o.load_c(0);
+    T uL = o.face(0).u;
+    uR = o.face(n).u;
+    gL = o.ghost_l(c0, uL);
+    gR = T(0);
+    cn1 = T(0);
+    cn2 = c0;  // position 0 arrives at t = 0 through the two-slot queue
+    flux_lo = flux_hi = T(0);
+    S1 = StageS<T>{T(0), T(0), T(0), T(0), T(0), T(0)};
+    S2 = S1;
+    S3 = S1;
+    S4 = S1;
+    const int t_last = (TM == 1) ? n + 1 : n + 7;
+    // blocks of 8 starting at t = -8 (ring index = t & 7); positions before
+    // -2 are skipped inside the guarded body.
+    int T0 = -8;
+    // the queue must hold c(t+1) when t >= -1: prime it for t = -2
+    // (cn2 = c0 is consumed as cn1 at t = -1 -> a at t = 0)
+#pragma unroll 1
+    for (; T0 <= t_last; T0 += 8) {
+      // steady blocks end by n-2: t = n-1 captures the right ghost value
+      const bool steady = (TM == 2) ? (T0 >= 8 && T0 + 7 <= n - 2) : (T0 >= 2 && T0 + 7 <= n - 2);
+      o.stage_begin(T0);
+      if (steady) block8<false>(T0);
+      else block8<true>(T0);
+      o.stage_end(T0);
+    }
+    o.stage_finish();
+  }
+};
+
+}  // namespace f3d

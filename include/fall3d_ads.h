@@ -126,6 +126,13 @@ int f3d_ads_synchronize(f3d_ctx *ctx);
  * and for ordering the caller's own work after a step. */
 int f3d_ads_get_stream(f3d_ctx *ctx, void **stream);
 
+/* Per-phase device timing with CUDA events on the context stream.  When on,
+ * every step records events around its phases and waits for them; the
+ * accumulated milliseconds are ms[0] prep+source, ms[1] x sweep, ms[2] y
+ * sweep, ms[3] z sweep, ms[4] flux reduction, ms[5] whole step. */
+int f3d_ads_set_profiling(f3d_ctx *ctx, int on);
+int f3d_ads_get_profile(f3d_ctx *ctx, double ms[6], int *nsteps);
+
 /* The pieces of the step, for unit parity with the ADS_* routines. */
 /* ADS_update_horizontal_vcomps(u1,u2,v1,v2,stime)  mod_ADS.F90:187 */
 int f3d_ads_update_vcomps(f3d_ctx *ctx, double stime);
