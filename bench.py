@@ -1,0 +1,434 @@
+#!/usr/bin/env python3
+"""Benchmark of the FALL3D ADS time step on B200 (cell*bin*steps/s).
+
+python bench.py --gpus N --steps K --warmup W [--impl reference] [--workload ...]
+
+One process per GPU (torchrun for N > 1).  Ensemble members are independent
+replicas, so each rank advances its own members with no data-path
+collective ("scaling": "weak"); torch.distributed only provides the barrier
+around the timed region and the max-over-ranks of the device time.
+
+Workloads (seeded synthetic inputs standing in for a meteo database):
+  c2        400x300x60 grid, 20 bins, random-phase winds, log-normal K, two
+            Suzuki sources (one domain per GPU), FP32 precision form timed,
+            FP64 form timed on the same inputs for the ratio
+  ensemble  the 64-member ensemble on uneven grids, 12 bins (see
+            fall3d_b200.ensemble); FP32 + learned settling velocity timed,
+            plain FP64 timed on the same members
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell·bin·steps/s on 1 B200: FP32+ensemble+MLP vs plain FP64, ≤1e-5 rel L2"
+UNIT = "cell*bin*steps/s"
+L2_BYTES = 126 * 2**20
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cuda_events(stream_ptr: int, device: int):
+    import torch
+    s = torch.cuda.ExternalStream(stream_ptr, device=torch.device("cuda", device))
+    return s, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+# ---------------------------------------------------------------------------
+def sweep_bytes(wl, prec_bytes: int, d: str) -> float:
+    """Algorithmic HBM bytes of one sweep launch (per the roofline model):
+    c read+write per cell*bin, the per-face fields once, and for z the
+    per-bin settling velocity."""
+    g = wl.grid
+    nx, ny, nz, nb = g.nx, g.ny, g.nz, wl.nbins
+    cells = nx * ny * nz
+    c_rw = 2.0 * prec_bytes * cells * nb
+    if prec_bytes == 4:
+        face = 12.0  # two wind snapshots + face diffusion coefficient
+    else:
+        face = 16.0  # current wind + face diffusion
+    if d == "x":
+        return c_rw + face * (nx + 1) * ny * nz
+    if d == "y":
+        return c_rw + face * (ny + 1) * nx * nz
+    return c_rw + face * (nz + 1) * nx * ny + prec_bytes * (nz + 1) * nx * ny * nb
+
+
+def load_traffic(kernel: str, workload: str):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        e = d.get(workload, {}).get(kernel)
+        return float(e) if e is not None else None
+    except Exception:
+        return None
+
+
+def setup_domain(wl, prec, device):
+    from fall3d_b200.ads import Domain
+    dom = Domain(wl.grid, wl.nbins, wl.limiter, wl.time_marching, prec, device=device)
+    dom.set_meteo(wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3, None, wl.t_its, wl.t_ite)
+    dom.phys_get_vset(wl.vset_model, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi, wl.bin_cat)
+    dom.set_source(wl.src_ijk, wl.src_vals)
+    s_mid = 0.5
+    _, dt = dom.grid_get_time_step(s_mid, wl.criterion, wl.cfl, wl.run_end)
+    return dom, dt
+
+
+def time_steps(dom, dt, K, W, device, pg, t0=0.0):
+    """W warm-up steps then K timed steps; device time by CUDA events."""
+    import torch
+    t = t0
+    for it in range(W):
+        dom.step_async(dt, t, it)
+        t += dt
+    dom.synchronize()
+    s, e0, e1 = cuda_events(dom.stream_ptr, device)
+    torch.cuda.synchronize(device)
+    barrier(pg)
+    n0 = dom.launch_count()
+    e0.record(s)
+    for it in range(W, W + K):
+        dom.step_async(dt, t, it)
+        t += dt
+    e1.record(s)
+    dom.synchronize()
+    torch.cuda.synchronize(device)
+    barrier(pg)
+    launches = dom.launch_count() - n0
+    return e0.elapsed_time(e1), launches, t
+
+
+def run_c2(args, ws, rank, local, pg):
+    import torch
+    from fall3d_b200 import workloads as W
+    from fall3d_b200.ads import PREC_FP32, PREC_FP64
+    torch.cuda.set_device(local)
+    wl = W.random_c2(seed=rank)
+    g = wl.grid
+    cbs = float(g.nx * g.ny * g.nz * wl.nbins)
+    K, Wu = args.steps, args.warmup
+    out = {}
+    # ---- FP64 plain form (ratio denominator), same steps from the same state
+    dom64, dt = setup_domain(wl, PREC_FP64, local)
+    ms64, _, _ = time_steps(dom64, dt, K, Wu, local, pg)
+    ms64 = max_over_ranks(pg, ms64)
+    fp64_value = ws * cbs * K / (ms64 / 1e3)
+    c64 = dom64.download_state()[0] if rank == 0 else None
+    dom64.close()
+    # ---- FP32 precision form (headline on this workload)
+    dom, dt32 = setup_domain(wl, PREC_FP32, local)
+    with ClockSampler(local) as clk:
+        ms, launches, t_end = time_steps(dom, dt32, K, Wu, local, pg)
+    ms = max_over_ranks(pg, ms)
+    value = ws * cbs * K / (ms / 1e3)
+    out.update(value=value, ms_per_step=ms / K, fp64_value=fp64_value, launches=launches,
+               clocks=clk.summary(), fp64_ms_per_step=ms64 / K)
+    if c64 is not None:
+        # FP32 form against the FP64 form after the same W+K steps (dt of the
+        # FP64 CFL reduction in both)
+        c32 = dom.download_state()[0]
+        a, b = c64[2:-2, 2:-2, 2:-2, :], c32[2:-2, 2:-2, 2:-2, :]
+        out["fp32_rel_l2_vs_fp64"] = float(np.linalg.norm(b - a) / np.linalg.norm(a))
+        out["fp32_rel_l2_vs_fp64_worst_bin"] = float(max(
+            np.linalg.norm(b[..., q] - a[..., q]) / max(np.linalg.norm(a[..., q]), 1e-300)
+            for q in range(a.shape[-1])))
+        del c32
+    # ---- per-kernel profile (event-timed phases) for the roofline
+    dom.set_profiling(True)
+    t = t_end
+    for it in range(3):
+        dom.step_async(dt32, t, K + Wu + it)
+        t += dt32
+    prof, n = dom.get_profile()
+    dom.set_profiling(False)
+    per = {"x": prof[1] / n, "y": prof[2] / n, "z": prof[3] / n}
+    dom_k = max(per, key=per.get)
+    byts = sweep_bytes(wl, 4, dom_k)
+    peak, kind = hbm_peak()
+    achieved = byts / (per[dom_k] / 1e3) / 1e9
+    out["roofline"] = {"bound": "hbm", "kernel": f"k_sweep32<{ 'xyz'.index(dom_k)},2,2> ({dom_k} sweep)",
+                       "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                       "frac": round(achieved / peak, 4), "peak_kind": kind,
+                       "traffic": load_traffic(f"sweep32_{dom_k}", "c2"),
+                       "algorithmic_bytes": byts, "launch_ms": round(per[dom_k], 4),
+                       "sweep_ms": {k: round(v, 4) for k, v in per.items()}}
+    # ---- e2e through the C ABI with host buffers
+    out["e2e"] = e2e_c2(dom, wl, dt32, K, local, pg, ws, cbs)
+    dom.close()
+    out["workload"] = wl
+    return out
+
+
+def e2e_c2(dom, wl, dt, K, device, pg, ws, cbs):
+    """Same metric end to end through the public API: every step crosses the
+    C ABI from host scalars and reads the boundary fluxes back (48 B); the
+    meteo term is uploaded from pinned host memory and charged per step at
+    the FALL3D coupling interval (3600 s of model time / dt steps)."""
+    from fall3d_b200.ads import Domain  # noqa: F401  (API in use)
+    pinned = [np.asfortranarray(a) for a in (wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3)]
+    meteo_bytes = sum(a.nbytes for a in pinned)
+    barrier(pg)
+    t0 = time.perf_counter()
+    dom.set_meteo(*pinned, None, wl.t_its, wl.t_ite)
+    t1 = time.perf_counter()
+    f = np.zeros(6)
+    t = 0.0
+    for it in range(K):
+        dom.F3D_time_step(dt, t, it, f)
+        t += dt
+    t2 = time.perf_counter()
+    steps_per_meteo = max(1.0, 3600.0 / dt)
+    t_meteo = t1 - t0
+    t_steps = t2 - t1
+    t_tot = max_over_ranks(pg, t_steps + t_meteo * K / steps_per_meteo)
+    return {"value": ws * cbs * K / t_tot, "unit": UNIT,
+            "h2d_bytes_per_step": int(meteo_bytes / steps_per_meteo + 20),
+            "d2h_bytes_per_step": 48,
+            "meteo_upload_s": round(t_meteo, 4), "steps_per_meteo_interval": round(steps_per_meteo, 1)}
+
+
+def cpu_baseline_c2(wl, steps=2):
+    """The CPU FP64 oracle (restatement of the reference path) with all host
+    threads, on a bounded sample of the same workload."""
+    from oracle import oracle as O
+    from fall3d_b200.source import dense_source
+    g = wl.grid
+    threads = os.cpu_count() or 1
+    orc = O.Oracle(g, wl.nbins, wl.limiter, wl.time_marching, threads=threads)
+    vs = column_vset(O, wl)
+    c = np.zeros((g.nx + 4, g.ny + 4, g.nz + 4, wl.nbins), order="F")
+    a = np.zeros((g.nx + 4, g.ny + 4, wl.nbins), order="F")
+    s = dense_source(g, wl.src_ijk, wl.src_vals, wl.nbins)
+    f = np.zeros(6)
+    t0 = time.perf_counter()
+    t = 0.0
+    for it in range(steps):
+        orc.time_step(6.5, t, wl.t_its, wl.t_ite, it, c, a, s, wl.u12, wl.v12, wl.w12, wl.k1,
+                      wl.k2, wl.k3, vs, f)
+        t += 6.5
+    el = time.perf_counter() - t0
+    return {"value": g.nx * g.ny * g.nz * wl.nbins * steps / el, "unit": UNIT, "cores": threads,
+            "kind": "port", "sample": f"{steps} steps of the full {g.nx}x{g.ny}x{g.nz}x{wl.nbins} "
+                                      f"case, CPU FP64 oracle, OpenMP over pencils"}
+
+
+def column_vset(O, wl):
+    """Settling velocity from the oracle per level (air properties of these
+    synthetic workloads vary with height only), broadcast over the columns."""
+    g = wl.grid
+    vs = np.zeros((g.nx, g.ny, g.nz + 3, wl.nbins), order="F")
+    T = wl.tc[0, 0, :]
+    rho = wl.rhoc[0, 0, :]
+    for k in range(g.nz + 1):
+        visa = 1.827e-5 * ((291.15 + 120.0) / (T[k] + 120.0)) * (T[k] / 291.15) ** 1.5
+        for b in range(wl.nbins):
+            v, _, _ = O.vset_point(wl.diam[b], wl.rhop[b], wl.psi[b], rho[k], visa, wl.vset_model)
+            vs[:, :, k + 1, b] = v
+    vs[:, :, 0, :] = vs[:, :, 1, :]
+    vs[:, :, g.nz + 2, :] = vs[:, :, g.nz + 1, :]
+    return vs
+
+
+def run_reference(args, ws, rank):
+    """Reference arm: the CPU restatement of the reference path (the Fortran
+    reference cannot be built here) on the host cores, same metric/config."""
+    if rank != 0:
+        return
+    from fall3d_b200 import workloads as W
+    wl = W.random_c2(seed=0)
+    from oracle import oracle as O
+    from fall3d_b200.source import dense_source
+    g = wl.grid
+    threads = os.cpu_count() or 1
+    orc = O.Oracle(g, wl.nbins, wl.limiter, wl.time_marching, threads=threads)
+    vs = column_vset(O, wl)
+    c = np.zeros((g.nx + 4, g.ny + 4, g.nz + 4, wl.nbins), order="F")
+    a = np.zeros((g.nx + 4, g.ny + 4, wl.nbins), order="F")
+    s = dense_source(g, wl.src_ijk, wl.src_vals, wl.nbins)
+    f = np.zeros(6)
+    t = 0.0
+    for it in range(args.warmup):
+        orc.time_step(6.5, t, wl.t_its, wl.t_ite, it, c, a, s, wl.u12, wl.v12, wl.w12, wl.k1,
+                      wl.k2, wl.k3, vs, f)
+        t += 6.5
+    t0 = time.perf_counter()
+    for it in range(args.steps):
+        orc.time_step(6.5, t, wl.t_its, wl.t_ite, args.warmup + it, c, a, s, wl.u12, wl.v12,
+                      wl.w12, wl.k1, wl.k2, wl.k3, vs, f)
+        t += 6.5
+    el = time.perf_counter() - t0
+    cbs = g.nx * g.ny * g.nz * wl.nbins
+    v = cbs * args.steps / el
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "c2: 400x300x60 grid, 20 bins, 2 Suzuki sources",
+                       "parallelism": "cpu-openmp"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full steps of the 400x300x60x20 case"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c2"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    res = run_c2(args, ws, rank, local, pg)
+    wl = res.pop("workload")
+    if rank == 0:
+        g = wl.grid
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"c2: {g.nx}x{g.ny}x{g.nz} grid, {wl.nbins} bins, FP32 precision "
+                                   "form (FP64 deposit/flux sums), one domain per GPU",
+                       "parallelism": f"replicas x{ws}",
+                       "l2": f"inputs larger than L2: c is {g.nx*g.ny*g.nz*wl.nbins*4/2**20:.0f} MiB "
+                             f"vs {L2_BYTES/2**20:.0f} MiB L2"},
+            "fp64_plain_value": res["fp64_value"],
+            "fp64_ms_per_step": res["fp64_ms_per_step"],
+            "speedup_vs_fp64": res["value"] / res["fp64_value"],
+            "gpu_launches": res["launches"],
+            "clocks": res["clocks"],
+            "roofline": res["roofline"],
+            "e2e": res["e2e"],
+        }
+        for k in ("fp32_rel_l2_vs_fp64", "fp32_rel_l2_vs_fp64_worst_bin"):
+            if k in res:
+                line[k] = res[k]
+        if ws == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_c2(wl)
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

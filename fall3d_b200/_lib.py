@@ -44,6 +44,7 @@ SIGNATURES = {
     "f3d_ads_get_stream": [_vp, C.POINTER(_vp)],
     "f3d_ads_set_profiling": [_vp, C.c_int],
     "f3d_ads_get_profile": [_vp, _dp, _ip],
+    "f3d_ads_launch_count": [_vp, C.POINTER(C.c_longlong)],
     "f3d_ads_update_vcomps": [_vp, C.c_double],
     "f3d_ads_solve_along_x": [_vp, C.c_double, _dp, _dp],
     "f3d_ads_solve_along_y": [_vp, C.c_double, _dp, _dp],

@@ -138,6 +138,11 @@ class Domain:
         check(lib().f3d_ads_get_profile(self._h, _p(ms), C.byref(n)), "f3d_ads_get_profile")
         return ms, n.value
 
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        check(lib().f3d_ads_launch_count(self._h, C.byref(n)), "f3d_ads_launch_count")
+        return n.value
+
     def ADS_update_horizontal_vcomps(self, stime):
         check(lib().f3d_ads_update_vcomps(self._h, float(stime)), "f3d_ads_update_vcomps")
 

@@ -113,6 +113,7 @@ struct f3d_ctx {
   cudaEvent_t ev[8] = {};
   double prof_ms[6] = {0, 0, 0, 0, 0, 0};
   int prof_steps = 0;
+  long long launches = 0;  // kernels launched by this context
 };
 
 template <class T>
@@ -536,6 +537,7 @@ extern "C" int f3d_ads_download_state(f3d_ctx* c, double* my_c, double* my_acum)
 
 // ---- step ---------------------------------------------------------------
 static int enqueue_sweep(f3d_ctx* c, int dir) {
+  c->launches += 1;
   if (c->prec == F3D_PREC_FP64)
     launch_sweep64(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
   else
@@ -545,6 +547,7 @@ static int enqueue_sweep(f3d_ctx* c, int dir) {
 }
 
 static int enqueue_prep(f3d_ctx* c, int mask) {
+  if (c->prec == F3D_PREC_FP64) c->launches += 1;  // the FP32 form interpolates inside the sweeps
   if (c->prec == F3D_PREC_FP64)
     launch_prep64(c->dm, c->dprep_member, c->dprep_first, c->nprep, mask, c->st);
   else
@@ -555,6 +558,7 @@ static int enqueue_prep(f3d_ctx* c, int mask) {
 
 static int enqueue_source(f3d_ctx* c) {
   if (c->hm.nsrc <= 0) return 0;
+  c->launches += 1;
   if (c->prec == F3D_PREC_FP64) launch_source64(c->dm, 1, c->st);
   else launch_source32(c->dm, 1, c->st);
   CKL();
@@ -573,6 +577,7 @@ static int enqueue_step(f3d_ctx* c, double dt, double time, int iiter) {
   auto rec = [&](int k) { if (c->prof) cudaEventRecord(c->ev[k], c->st); };
   rec(0);
   launch_set_step(c->dm, 0, dt, time, iiter, c->st);
+  c->launches += 1;
   CKL();
   if (enqueue_prep(c, 7) || enqueue_source(c)) return 1;
   rec(1);
@@ -584,6 +589,7 @@ static int enqueue_step(f3d_ctx* c, double dt, double time, int iiter) {
   if (enqueue_sweep(c, DIR_Z)) return 1;
   rec(4);
   launch_flux_reduce(c->dm, 1, 7, c->st);
+  c->launches += 1;
   CKL();
   rec(5);
   if (c->prof) {
@@ -611,6 +617,12 @@ extern "C" int f3d_ads_set_profiling(f3d_ctx* c, int on) {
   c->prof = on != 0;
   for (double& x : c->prof_ms) x = 0.0;
   c->prof_steps = 0;
+  return 0;
+}
+
+extern "C" int f3d_ads_launch_count(f3d_ctx* c, long long* count) {
+  if (!c || !count) return set_err("f3d_ads_launch_count: null argument");
+  *count = c->launches;
   return 0;
 }
 

@@ -133,6 +133,9 @@ int f3d_ads_get_stream(f3d_ctx *ctx, void **stream);
 int f3d_ads_set_profiling(f3d_ctx *ctx, int on);
 int f3d_ads_get_profile(f3d_ctx *ctx, double ms[6], int *nsteps);
 
+/* Number of CUDA kernels this context has launched since creation. */
+int f3d_ads_launch_count(f3d_ctx *ctx, long long *count);
+
 /* The pieces of the step, for unit parity with the ADS_* routines. */
 /* ADS_update_horizontal_vcomps(u1,u2,v1,v2,stime)  mod_ADS.F90:187 */
 int f3d_ads_update_vcomps(f3d_ctx *ctx, double stime);
