@@ -53,6 +53,8 @@ SIGNATURES = {
     "f3d_ads_get_time_step": [_vp, C.c_double, C.c_int, C.c_double, C.c_double, _dp, _dp],
     "f3d_ads_mass_volume": [_vp, _dp, _dp],
     "f3d_ads_mass_boundaries": [_dp, _dp, _dp],
+    "f3d_mass_volume_noalloc": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
+                                _vp],
     "f3d_vset_points": [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip],
     "f3d_ads_compute_vset": [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_double, _dp],
     "f3d_host_alloc": [C.c_size_t, C.POINTER(_vp)],

@@ -24,6 +24,7 @@ SOURCES = [
     ("ads_fp32.cu", []),
     ("ens.cu", []),
     ("mlp.cu", []),
+    ("noalloc.cu", ["--fmad=false"]),
     ("f3d_capi.cu", ["-Xcompiler", "-ffp-contract=off"]),
 ]
 

@@ -64,6 +64,19 @@ static int set_err(const char* fmt, ...) {
   return 1;
 }
 
+namespace f3d {
+// Error reporting shared with the other translation units of the library.
+int set_error_msg(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return 1;
+}
+}  // namespace f3d
+
 #define CK(call)                                                                        \
   do {                                                                                  \
     cudaError_t e_ = (call);                                                            \
