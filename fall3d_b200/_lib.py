@@ -23,8 +23,7 @@ class F3DDims(C.Structure):
 
 
 class F3DEnsMember(C.Structure):
-    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("grid_class", C.c_int),
-                ("wind_factor", C.c_double)]
+    _fields_ = [("grid_class", C.c_int), ("wind_factor", C.c_double)]
 
 
 SIGNATURES = {
@@ -57,6 +56,28 @@ SIGNATURES = {
                                 _vp],
     "f3d_vset_points": [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip],
     "f3d_ads_compute_vset": [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_double, _dp],
+    "f3d_ens_create": [C.c_int, C.POINTER(F3DDims), C.c_int, _vp, C.c_int, C.c_int, C.c_int,
+                       C.c_int, C.POINTER(_vp)],
+    "f3d_ens_destroy": [_vp],
+    "f3d_ens_set_class_grid": [_vp, C.c_int] + [_dp] * 9,
+    "f3d_ens_set_class_meteo": [_vp, C.c_int] + [_dp] * 7 + [C.c_double, C.c_double],
+    "f3d_ens_compute_class_vset": [_vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
+                                   C.c_double],
+    "f3d_ens_set_member_source": [_vp, C.c_int, C.c_int, _ip, _dp],
+    "f3d_ens_upload_member_state": [_vp, C.c_int, _dp, _dp],
+    "f3d_ens_download_member_state": [_vp, C.c_int, _dp, _dp],
+    "f3d_ens_compute_time_steps": [_vp, C.c_double, C.c_int, C.c_double, C.c_double, _dp],
+    "f3d_ens_set_clock": [_vp, _dp, C.c_int],
+    "f3d_ens_get_clock": [_vp, _dp, _ip],
+    "f3d_ens_set_tuning": [_vp, C.c_int, C.c_int, C.c_int],
+    "f3d_ens_run": [_vp, C.c_int],
+    "f3d_ens_step": [_vp, _dp, _dp, C.c_int, _dp],
+    "f3d_ens_get_fluxes": [_vp, _dp],
+    "f3d_ens_mass_volume": [_vp, C.c_int, _dp],
+    "f3d_ens_synchronize": [_vp],
+    "f3d_ens_get_stream": [_vp, C.POINTER(_vp)],
+    "f3d_ens_launch_count": [_vp, C.POINTER(C.c_longlong)],
+    "f3d_ens_status": [_vp, _ip],
     "f3d_host_alloc": [C.c_size_t, C.POINTER(_vp)],
     "f3d_host_free": [_vp],
 }

@@ -15,6 +15,7 @@
 
 #include "f3d_common.cuh"
 #include "march.cuh"
+#include "step_dev.cuh"
 
 namespace f3d {
 
@@ -132,15 +133,15 @@ __device__ __forceinline__ void block_reduce2_f64(double a, double b, double* ou
   }
 }
 
+// One work item (32 pencils x bpb bins of one member) of a sweep; called by
+// the per-sweep kernels and by the persistent fused step kernel.
 template <int DIR, int LIM, int TM>
-__global__ void __launch_bounds__(128) k_sweep32(const MemberDev* __restrict__ members,
-                                                 const WorkItem* __restrict__ work, int bpb) {
-  const WorkItem w = work[blockIdx.x];
+__device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ members,
+                                             const WorkItem w, int bpb, unsigned char* f3d_smem) {
   const MemberDev& m = members[w.member];
   const int nx = m.nx, ny = m.ny, nz = m.nz;
   const long long nsp = (DIR == DIR_X) ? (long long)ny * nz
                         : (DIR == DIR_Y) ? (long long)nx * nz : (long long)nx * ny;
-  extern __shared__ __align__(16) unsigned char f3d_smem[];
   const int warp = threadIdx.x >> 5;
   const long long pen_raw = (long long)w.pen0 + 32 * (warp / bpb) + (threadIdx.x & 31);
   const long long pen0w = (long long)w.pen0 + 32 * (warp / bpb);
@@ -218,6 +219,13 @@ __global__ void __launch_bounds__(128) k_sweep32(const MemberDev* __restrict__ m
     }
   }
   block_reduce2_f64(clo, chi, m.flux_part + 2 * (long long)w.slot);
+}
+
+template <int DIR, int LIM, int TM>
+__global__ void __launch_bounds__(128) k_sweep32(const MemberDev* __restrict__ members,
+                                                 const WorkItem* __restrict__ work, int bpb) {
+  extern __shared__ __align__(16) unsigned char f3d_smem[];
+  sweep32_item<DIR, LIM, TM>(members, work[blockIdx.x], bpb, f3d_smem);
 }
 
 template <int DIR>
@@ -335,6 +343,79 @@ __global__ void k_fp32_fields(MemberDev* members, int mi) {
 
 void launch_fp32_fields(MemberDev* members, int mi, cudaStream_t st) {
   k_fp32_fields<<<2048, 256, 0, st>>>(members, mi);
+}
+
+}  // namespace f3d
+
+namespace f3d {
+
+// Source term of every member, grid-stride over (member, cell, bin).
+__device__ __forceinline__ void source32_all(MemberDev* members, int nmembers) {
+  for (int mi = 0; mi < nmembers; ++mi) {
+    const MemberDev& m = members[mi];
+    const long long tot = (long long)m.nsrc * m.nb;
+    const long long ncell = (long long)m.nx * m.ny * m.nz;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+      int q = (int)(e / m.nb), b = (int)(e % m.nb);
+      float* cc = m.c32 + (long long)b * ncell + m.src_cell[q];
+      *cc = (float)((double)*cc + m.dt * m.src_s[(long long)q * m.nb + b] / m.src_vol[q]);
+    }
+  }
+}
+
+// Out-of-line sweep items for the persistent kernel: each direction keeps its
+// own register allocation instead of one inlined union of all three.
+template <int DIR, int LIM, int TM>
+__device__ __noinline__ void sweep32_item_call(MemberDev* members, WorkItem w, int bpb,
+                                               unsigned char* smem) {
+  sweep32_item<DIR, LIM, TM>(members, w, bpb, smem);
+}
+
+// One whole time step of every member in one persistent kernel: source,
+// the two horizontal sweeps (order by iiter parity, mod_F3D.F90:1477-1487),
+// the z sweep, boundary-flux reduction and the device clock.  Blocks pull
+// work items from per-phase atomic counters (members of uneven size balance
+// themselves) and meet at bounded grid barriers between phases.  Launched
+// cooperatively so that every block is resident.
+template <int LIM, int TM>
+__global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
+  extern __shared__ __align__(16) unsigned char f3d_smem[];
+  __shared__ int slot;
+  __shared__ double sa[128], sb[128];
+  source32_all(a.members, a.nmembers);
+  grid_barrier(a.counters + 6, a.err);
+  const bool xfirst = (a.members[0].iiter % 2) == 0;
+  for (int ph = 0; ph < 3; ++ph) {
+    const int dir = (ph == 2) ? 2 : (((ph == 0) == xfirst) ? 0 : 1);
+    for (;;) {
+      const int it = grab_item(a.counters + ph, &slot);
+      if (it >= a.nwork[dir]) break;
+      const WorkItem w = a.work[dir][it];
+      if (dir == 0) sweep32_item_call<0, LIM, TM>(a.members, w, a.bpb, f3d_smem);
+      else if (dir == 1) sweep32_item_call<1, LIM, TM>(a.members, w, a.bpb, f3d_smem);
+      else sweep32_item_call<2, LIM, TM>(a.members, w, a.bpb, f3d_smem);
+    }
+    grid_barrier(a.counters + 6, a.err);
+  }
+  for (int mi = blockIdx.x; mi < a.nmembers; mi += gridDim.x) {
+    member_flux_reduce(a.members[mi], 7, sa, sb);
+    if (threadIdx.x == 0) member_advance(a.members[mi]);
+    __syncthreads();
+  }
+}
+
+int fused32_smem() { return 4 * XTile<float>::BYTES; }
+
+const void* fused32_func(int lim, int tm) {
+  if (tm == 1) {
+    if (lim == 1) return (const void*)k_fused32<1, 1>;
+    if (lim == 2) return (const void*)k_fused32<2, 1>;
+    return (const void*)k_fused32<3, 1>;
+  }
+  if (lim == 1) return (const void*)k_fused32<1, 2>;
+  if (lim == 2) return (const void*)k_fused32<2, 2>;
+  return (const void*)k_fused32<3, 2>;
 }
 
 }  // namespace f3d

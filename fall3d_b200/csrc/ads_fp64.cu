@@ -14,6 +14,7 @@
 
 #include "f3d_common.cuh"
 #include "march.cuh"
+#include "step_dev.cuh"
 
 namespace f3d {
 
@@ -136,15 +137,14 @@ __device__ __forceinline__ void block_reduce2(double a, double b, double* out) {
   }
 }
 
+// One work item of a sweep (per-sweep kernels and the persistent step kernel).
 template <int DIR, int LIM, int TM>
-__global__ void __launch_bounds__(128) k_sweep64(const MemberDev* __restrict__ members,
-                                                 const WorkItem* __restrict__ work, int bpb) {
-  const WorkItem w = work[blockIdx.x];
+__device__ __forceinline__ void sweep64_item(const MemberDev* __restrict__ members,
+                                             const WorkItem w, int bpb, unsigned char* f3d_smem) {
   const MemberDev& m = members[w.member];
   const int nx = m.nx, ny = m.ny, nz = m.nz;
   const long long nsp = (DIR == DIR_X) ? (long long)ny * nz
                         : (DIR == DIR_Y) ? (long long)nx * nz : (long long)nx * ny;
-  extern __shared__ __align__(16) unsigned char f3d_smem[];
   const int warp = threadIdx.x >> 5;
   const long long pen_raw = (long long)w.pen0 + 32 * (warp / bpb) + (threadIdx.x & 31);
   const long long pen0w = (long long)w.pen0 + 32 * (warp / bpb);
@@ -216,6 +216,13 @@ __global__ void __launch_bounds__(128) k_sweep64(const MemberDev* __restrict__ m
   block_reduce2(clo, chi, m.flux_part + 2 * (long long)w.slot);
 }
 
+template <int DIR, int LIM, int TM>
+__global__ void __launch_bounds__(128) k_sweep64(const MemberDev* __restrict__ members,
+                                                 const WorkItem* __restrict__ work, int bpb) {
+  extern __shared__ __align__(16) unsigned char f3d_smem[];
+  sweep64_item<DIR, LIM, TM>(members, work[blockIdx.x], bpb, f3d_smem);
+}
+
 // Host launchers -------------------------------------------------------------
 template <int DIR>
 static void launch_dir64(int lim, int tm, const MemberDev* members,
@@ -252,26 +259,37 @@ void launch_sweep64(int dir, int lim, int tm, const MemberDev* members,
 // Per-step preparation: current winds u,v,w = (1-s) x1 + s x2
 // (mod_F3D.F90:1437-1439, mod_ADS.F90:667), then the sparse source term
 // c += dt*s/vol (mod_F3D.F90:1456-1473).
-__global__ void k_prep64(const MemberDev* __restrict__ members, const int* __restrict__ blk_member,
-                         const int* __restrict__ blk_first, int mask) {
-  const int mi = blk_member[blockIdx.x];
-  const MemberDev& m = members[mi];
+// Current winds of one member: u = (1-s) f u1 + s f u2 with the member's
+// wind factor f applied to the snapshots first (the ensemble perturbs the
+// meteo winds, task_Fall3d.F90:194-198; f = 1 for a single run leaves the
+// values unchanged), w = (1-s) w1 + s w2.  Elements [q0, q0+cnt) of the
+// member's concatenated (u, v, w) face list.
+__device__ __forceinline__ void prep64_range(const MemberDev& m, long long q0, long long cnt,
+                                             int mask) {
   const long long nu = (long long)(m.nx + 1) * m.ny * m.nz;
   const long long nv = (long long)(m.ny + 1) * m.nx * m.nz;
   const long long nw = (long long)(m.nz + 1) * m.nx * m.ny;
-  const double s = m.stime;
-  long long q = (long long)(blockIdx.x - blk_first[mi]) * blockDim.x + threadIdx.x;
-  if (q < nu) {
-    if (mask & 1) m.ucur[q] = (1.0 - s) * m.ux[0][q] + s * m.ux[1][q];
-    return;
+  const double s = m.stime, f = m.wfacd;
+  for (long long e = threadIdx.x; e < cnt; e += blockDim.x) {
+    long long q = q0 + e;
+    if (q < nu) {
+      if (mask & 1) m.ucur[q] = (1.0 - s) * (f * m.ux[0][q]) + s * (f * m.ux[1][q]);
+      continue;
+    }
+    q -= nu;
+    if (q < nv) {
+      if (mask & 2) m.vcur[q] = (1.0 - s) * (f * m.vy[0][q]) + s * (f * m.vy[1][q]);
+      continue;
+    }
+    q -= nv;
+    if (q < nw && (mask & 4)) m.wcur[q] = (1.0 - s) * m.wz[0][q] + s * m.wz[1][q];
   }
-  q -= nu;
-  if (q < nv) {
-    if (mask & 2) m.vcur[q] = (1.0 - s) * m.vy[0][q] + s * m.vy[1][q];
-    return;
-  }
-  q -= nv;
-  if (q < nw && (mask & 4)) m.wcur[q] = (1.0 - s) * m.wz[0][q] + s * m.wz[1][q];
+}
+
+__global__ void k_prep64(const MemberDev* __restrict__ members, const int* __restrict__ blk_member,
+                         const int* __restrict__ blk_first, int mask) {
+  const int mi = blk_member[blockIdx.x];
+  prep64_range(members[mi], (long long)(blockIdx.x - blk_first[mi]) * 256, 256, mask);
 }
 
 __global__ void k_source64(const MemberDev* __restrict__ members, int nmembers) {
@@ -296,6 +314,78 @@ void launch_prep64(const MemberDev* members, const int* blk_member, const int* b
 void launch_source64(const MemberDev* members, int nmembers, cudaStream_t st) {
   dim3 g(8, nmembers < 65535 ? nmembers : 65535);
   k_source64<<<g, 128, 0, st>>>(members, nmembers);
+}
+
+}  // namespace f3d
+
+namespace f3d {
+
+__device__ __forceinline__ void source64_all(MemberDev* members, int nmembers) {
+  for (int mi = 0; mi < nmembers; ++mi) {
+    const MemberDev& m = members[mi];
+    const long long tot = (long long)m.nsrc * m.nb;
+    const long long ncell = (long long)m.nx * m.ny * m.nz;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+      int q = (int)(e / m.nb), b = (int)(e % m.nb);
+      double* cc = m.c64 + (long long)b * ncell + m.src_cell[q];
+      *cc = *cc + m.dt * m.src_s[(long long)q * m.nb + b] / m.src_vol[q];
+    }
+  }
+}
+
+template <int DIR, int LIM, int TM>
+__device__ __noinline__ void sweep64_item_call(MemberDev* members, WorkItem w, int bpb,
+                                               unsigned char* smem) {
+  sweep64_item<DIR, LIM, TM>(members, w, bpb, smem);
+}
+
+// FP64 form of the persistent step kernel (see k_fused32); the first phase
+// also builds each member's current winds.
+template <int LIM, int TM>
+__global__ void __launch_bounds__(128) k_fused64(FusedArgs a) {
+  extern __shared__ __align__(16) unsigned char f3d_smem[];
+  __shared__ int slot;
+  __shared__ double sa[128], sb[128];
+  for (;;) {
+    const int it = grab_item(a.counters + 3, &slot);
+    if (it >= a.nprep) break;
+    const int mi = a.prep_member[it];
+    prep64_range(a.members[mi], (long long)(it - a.prep_first[mi]) * 256, 256, 7);
+  }
+  source64_all(a.members, a.nmembers);
+  grid_barrier(a.counters + 6, a.err);
+  const bool xfirst = (a.members[0].iiter % 2) == 0;
+  for (int ph = 0; ph < 3; ++ph) {
+    const int dir = (ph == 2) ? 2 : (((ph == 0) == xfirst) ? 0 : 1);
+    for (;;) {
+      const int it = grab_item(a.counters + ph, &slot);
+      if (it >= a.nwork[dir]) break;
+      const WorkItem w = a.work[dir][it];
+      if (dir == 0) sweep64_item_call<0, LIM, TM>(a.members, w, a.bpb, f3d_smem);
+      else if (dir == 1) sweep64_item_call<1, LIM, TM>(a.members, w, a.bpb, f3d_smem);
+      else sweep64_item_call<2, LIM, TM>(a.members, w, a.bpb, f3d_smem);
+    }
+    grid_barrier(a.counters + 6, a.err);
+  }
+  for (int mi = blockIdx.x; mi < a.nmembers; mi += gridDim.x) {
+    member_flux_reduce(a.members[mi], 7, sa, sb);
+    if (threadIdx.x == 0) member_advance(a.members[mi]);
+    __syncthreads();
+  }
+}
+
+int fused64_smem() { return 4 * XTile<double>::BYTES; }
+
+const void* fused64_func(int lim, int tm) {
+  if (tm == 1) {
+    if (lim == 1) return (const void*)k_fused64<1, 1>;
+    if (lim == 2) return (const void*)k_fused64<2, 1>;
+    return (const void*)k_fused64<3, 1>;
+  }
+  if (lim == 1) return (const void*)k_fused64<1, 2>;
+  if (lim == 2) return (const void*)k_fused64<2, 2>;
+  return (const void*)k_fused64<3, 2>;
 }
 
 }  // namespace f3d

@@ -7,6 +7,7 @@
 #include <cstdint>
 
 #include "f3d_common.cuh"
+#include "step_dev.cuh"
 
 namespace f3d {
 
@@ -224,6 +225,64 @@ __global__ void k_set_dt_stime(MemberDev* members, int mi, double dt, double sti
   members[mi].dt = dt;
   members[mi].stime = stime;
 }
+// Per-member step parameters for up to 64 members per launch (arguments are
+// copied at launch, so the host arrays may change right after).
+struct StepChunk {
+  int first, count, iiter;
+  double dt[64];
+  double time[64];
+};
+__global__ void k_set_steps(MemberDev* members, StepChunk c) {
+  const int q = threadIdx.x;
+  if (q < c.count) {
+    MemberDev& m = members[c.first + q];
+    m.dt = c.dt[q];
+    m.time = c.time[q];
+    m.iiter = c.iiter;
+    m.stime = (c.time[q] - m.t_its) / (m.t_ite - m.t_its);
+  }
+}
+void launch_set_steps(MemberDev* members, int n, const double* dt, const double* time, int iiter,
+                      cudaStream_t st) {
+  for (int f = 0; f < n; f += 64) {
+    StepChunk c;
+    c.first = f;
+    c.count = (n - f < 64) ? n - f : 64;
+    c.iiter = iiter;
+    for (int q = 0; q < c.count; ++q) {
+      c.dt[q] = dt[f + q];
+      c.time[q] = time[f + q];
+    }
+    k_set_steps<<<1, 64, 0, st>>>(members, c);
+  }
+}
+
+// Device clock of every member (graph replays need no host input).
+__global__ void k_advance_clock(MemberDev* members, int n) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) member_advance(members[q]);
+}
+void launch_advance_clock(MemberDev* members, int n, cudaStream_t st) {
+  k_advance_clock<<<(n + 63) / 64, 64, 0, st>>>(members, n);
+}
+
+// dt of each member from its CFL maxima (mod_Grid.F90:1125-1138), in place.
+__global__ void k_finalize_dt(MemberDev* members, int n, const double* red, double cfl,
+                              double run_end) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) {
+    double mx = fmax(fmax(red[3 * q], red[3 * q + 1]), red[3 * q + 2]);
+    if (mx > 0.0) mx = 1.0 / mx;
+    mx = cfl * mx;
+    MemberDev& m = members[q];
+    m.dt = fmin(mx, run_end);
+  }
+}
+void launch_finalize_dt(MemberDev* members, int n, const double* red, double cfl, double run_end,
+                        cudaStream_t st) {
+  k_finalize_dt<<<(n + 63) / 64, 64, 0, st>>>(members, n, red, cfl, run_end);
+}
+
 void launch_set_step(MemberDev* members, int mi, double dt, double time, int iiter,
                      cudaStream_t st) {
   k_set_step<<<1, 1, 0, st>>>(members, mi, dt, time, iiter);
@@ -237,46 +296,8 @@ void launch_set_dt_stime(MemberDev* members, int mi, double dt, double stime, cu
 // to flux_step {W,E,S,N,U,D} and are added to the running totals with a
 // Kahan-compensated update.
 __global__ void k_flux_reduce(const MemberDev* __restrict__ members, int dirmask) {
-  const MemberDev& m = members[blockIdx.x];
   __shared__ double sa[256], sb[256];
-  double res[6] = {0, 0, 0, 0, 0, 0};
-  for (int d = 0; d < 3; ++d) {
-    if (!(dirmask & (1 << d))) continue;
-    double a = 0.0, b = 0.0;
-    const double* p = m.flux_part + 2LL * m.part_base[d];
-    // strided first pass: thread t sums slots t, t+256, ... in order
-    for (int s = threadIdx.x; s < m.part_count[d]; s += blockDim.x) {
-      a = a + p[2 * s];
-      b = b + p[2 * s + 1];
-    }
-    sa[threadIdx.x] = a;
-    sb[threadIdx.x] = b;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-      if (threadIdx.x < s) {
-        sa[threadIdx.x] = sa[threadIdx.x] + sa[threadIdx.x + s];
-        sb[threadIdx.x] = sb[threadIdx.x] + sb[threadIdx.x + s];
-      }
-      __syncthreads();
-    }
-    // x -> (W,E) = 0,1 ; y -> (S,N) = 2,3 ; z -> (D,U) = 5,4
-    if (d == 0) { res[0] = sa[0]; res[1] = sb[0]; }
-    if (d == 1) { res[2] = sa[0]; res[3] = sb[0]; }
-    if (d == 2) { res[5] = sa[0]; res[4] = sb[0]; }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < 6; ++q) {
-      bool on = (q < 2) ? (dirmask & 1) : (q < 4) ? (dirmask & 2) : (dirmask & 4);
-      if (!on) continue;
-      m.flux_step[q] = res[q];
-      // Kahan: tot[q] + comp[q]
-      double y = res[q] - m.flux_tot[6 + q];
-      double t = m.flux_tot[q] + y;
-      m.flux_tot[6 + q] = (t - m.flux_tot[q]) - y;
-      m.flux_tot[q] = t;
-    }
-  }
+  member_flux_reduce(members[blockIdx.x], dirmask, sa, sb);
 }
 __global__ void k_zero_step(const MemberDev* __restrict__ members) {
   const MemberDev& m = members[blockIdx.x];
@@ -310,8 +331,9 @@ __global__ void k_cfl(const MemberDev* __restrict__ members, int mi, double s, i
     long long iu = ((long long)k * (nx + 1) + i) * ny + j;
     long long iv = ((long long)k * (ny + 1) + j) * nx + i;
     long long iw = ((long long)k * ny + j) * nx + i;
-    double u = (1.0 - s) * m.ux[0][iu] + s * m.ux[1][iu];
-    double v = (1.0 - s) * m.vy[0][iv] + s * m.vy[1][iv];
+    const double f = m.wfacd;
+    double u = (1.0 - s) * (f * m.ux[0][iu]) + s * (f * m.ux[1][iu]);
+    double v = (1.0 - s) * (f * m.vy[0][iv]) + s * (f * m.vy[1][iv]);
     double w = (1.0 - s) * m.wz[0][iw] + s * m.wz[1][iw];
     double k1 = m.k1x[((long long)k * (nx + 2) + (i + 1)) * ny + j];
     double k2 = m.k2y[((long long)k * (ny + 2) + (j + 1)) * nx + i];

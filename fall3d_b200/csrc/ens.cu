@@ -1,0 +1,917 @@
+// ens.cu -- host side of the batched ensemble (f3d_ens_* in fall3d_ads.h).
+//
+// All members of an ensemble live on one GPU in one member table.  Members of
+// a grid class point at the class's grid, meteo and settling-velocity arrays;
+// each member owns its concentration, deposit, source, fluxes and clock.  A
+// step is either a short sequence of kernels (source, sweeps, flux
+// reduction, clock) replayed from CUDA graphs, or one persistent cooperative
+// kernel that runs the whole step with bounded grid barriers between phases.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/fall3d_ads.h"
+#include "f3d_common.cuh"
+#include "step_dev.cuh"
+
+namespace f3d {
+int set_error_msg(const char* fmt, ...);
+void launch_sweep64(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
+                    int nblocks, int bpb, cudaStream_t st);
+void launch_sweep32(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
+                    int nblocks, int bpb, cudaStream_t st);
+void launch_prep64(const MemberDev* members, const int* blk_member, const int* blk_first,
+                   int nblocks, int mask, cudaStream_t st);
+void launch_source64(const MemberDev* members, int nmembers, cudaStream_t st);
+void launch_source32(const MemberDev* members, int nmembers, cudaStream_t st);
+void launch_conv(int which, const double* in, double* out, int nx, int ny, int nz, int nb,
+                 cudaStream_t st);
+void launch_flux_reduce(const MemberDev* members, int nmembers, int dirmask, cudaStream_t st);
+void launch_cfl(const MemberDev* members, int mi, double s, int criterion, double* out3,
+                cudaStream_t st);
+void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* partials, int nblk,
+                 double* out, cudaStream_t st);
+void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc,
+                       const double* tc, const double* bin_par, const int* bin_flags,
+                       double vset_fac, int* nfail, cudaStream_t st);
+void launch_face_kk(MemberDev* members, int mi, cudaStream_t st);
+void launch_fp32_fields(MemberDev* members, int mi, cudaStream_t st);
+void launch_set_steps(MemberDev* members, int n, const double* dt, const double* time, int iiter,
+                      cudaStream_t st);
+void launch_advance_clock(MemberDev* members, int n, cudaStream_t st);
+void launch_finalize_dt(MemberDev* members, int n, const double* red, double cfl, double run_end,
+                        cudaStream_t st);
+int fused32_smem();
+int fused64_smem();
+const void* fused32_func(int lim, int tm);
+const void* fused64_func(int lim, int tm);
+}  // namespace f3d
+
+using namespace f3d;
+
+#define ECK(call)                                                                       \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return set_error_msg("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),      \
+                           __FILE__, __LINE__);                                         \
+  } while (0)
+#define ECKL()                                                                          \
+  do {                                                                                  \
+    cudaError_t e_ = cudaGetLastError();                                                \
+    if (e_ != cudaSuccess)                                                              \
+      return set_error_msg("kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_),  \
+                           __FILE__, __LINE__);                                         \
+  } while (0)
+
+namespace {
+
+struct EnsClass {
+  int nx = 0, ny = 0, nz = 0;
+  int rep = -1;  // a member of the class, used to address class arrays in kernels
+  double* ux = nullptr;  // [2][k][f][j]
+  double* vy = nullptr;
+  double* wz = nullptr;
+  double* k1x = nullptr;
+  double* k2y = nullptr;
+  double* k3z = nullptr;
+  double* vs = nullptr;
+  double* kkf[3] = {nullptr, nullptr, nullptr};
+  double4* geo[3] = {nullptr, nullptr, nullptr};
+  float* ux32 = nullptr;
+  float* vy32 = nullptr;
+  float* wz32 = nullptr;
+  float* kf[3] = {nullptr, nullptr, nullptr};
+  float* vs32 = nullptr;
+  float* rdx[3] = {nullptr, nullptr, nullptr};
+  double* dx[6] = {};   // dx1p dx1b dx2p dx2b dx3p dx3b
+  double* hm[3] = {};   // hm1 hm2 hm3
+  std::vector<double> dX1_p, dX2_p, dX3_p, Hm1_p, Hm2_p, Hm3_p;
+  double t_its = 0.0, t_ite = 1.0;
+  bool grid_set = false, meteo_set = false;
+};
+
+}  // namespace
+
+struct f3d_ens {
+  int ncls = 0, nm = 0, nb = 0, lim = 2, tm = 2, prec = 0, device = 0;
+  int mode = F3D_ENS_MODE_KERNELS, bpb = 4, ctas_per_sm = 0;
+  cudaStream_t st = nullptr;
+  std::vector<EnsClass> cls;
+  std::vector<int> member_class;
+  std::vector<MemberDev> hm;
+  MemberDev* dm = nullptr;
+  std::vector<void*> allocs;
+  WorkItem* dwork[3] = {nullptr, nullptr, nullptr};
+  int nwork[3] = {0, 0, 0};
+  int* dprep_member = nullptr;
+  int* dprep_first = nullptr;
+  int nprep = 0;
+  double* flux_part = nullptr;
+  double* flux_tot = nullptr;   // [12 * nm]
+  double* flux_step = nullptr;  // [6 * nm]
+  double* d_red = nullptr;      // CFL maxima [3 * nm] and mass partials
+  int mass_nblk = 296;
+  unsigned int* counters = nullptr;  // persistent kernel: 6 phase counters + barrier
+  int* d_err = nullptr;
+  int* d_nfail = nullptr;
+  double* staging = nullptr;
+  size_t staging_elems = 0;
+  double* h_pin = nullptr;
+  size_t h_pin_elems = 0;
+  int iiter = 0;
+  bool dm_valid = false;  // the device member table has been written once
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool graph_ok = false;
+  int fused_grid = 0;
+  long long launches = 0;
+  std::vector<void*> work_allocs;  // rebuilt with the tuning
+};
+
+namespace {
+
+template <class T>
+int ealloc(f3d_ens* e, T** p, size_t n) {
+  void* q = nullptr;
+  if (n == 0) n = 1;
+  ECK(cudaMalloc(&q, n * sizeof(T)));
+  e->allocs.push_back(q);
+  *p = reinterpret_cast<T*>(q);
+  return 0;
+}
+
+void drop_graphs(f3d_ens* e) {
+  for (auto& g : e->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  e->graph_ok = false;
+}
+
+// The device owns dt, time, stime and iiter once steps have run (device clock,
+// CFL on the device): refresh them in the host mirror before re-uploading it.
+int pull_dynamic(f3d_ens* e) {
+  if (!e->dm || !e->dm_valid) return 0;
+  std::vector<MemberDev> dev(e->nm);
+  ECK(cudaStreamSynchronize(e->st));
+  ECK(cudaMemcpy(dev.data(), e->dm, sizeof(MemberDev) * e->nm, cudaMemcpyDeviceToHost));
+  for (int m = 0; m < e->nm; ++m) {
+    e->hm[m].dt = dev[m].dt;
+    e->hm[m].time = dev[m].time;
+    e->hm[m].stime = dev[m].stime;
+    e->hm[m].iiter = dev[m].iiter;
+  }
+  return 0;
+}
+
+int upload_members(f3d_ens* e) {
+  if (pull_dynamic(e)) return 1;
+  ECK(cudaMemcpyAsync(e->dm, e->hm.data(), sizeof(MemberDev) * e->nm, cudaMemcpyHostToDevice,
+                      e->st));
+  e->dm_valid = true;
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+// Work lists of the three sweeps.  Items of one class are ordered spatial
+// tile -> member -> bin group, so the blocks that read the same class face
+// fields at the same place run back to back.  Flux slots stay contiguous
+// per member.
+int build_work(f3d_ens* e) {
+  for (void* p : e->work_allocs) cudaFree(p);
+  e->work_allocs.clear();
+  const int bpb = e->bpb;
+  const int span = 32 * (4 / bpb);
+  const int nbg = (e->nb + bpb - 1) / bpb;
+  int slot = 0;
+  std::vector<std::vector<WorkItem>> lists(3);
+  for (int d = 0; d < 3; ++d) {
+    for (int mi = 0; mi < e->nm; ++mi) {
+      const EnsClass& c = e->cls[e->member_class[mi]];
+      long long nsp = d == 0 ? (long long)c.ny * c.nz : d == 1 ? (long long)c.nx * c.nz
+                                                               : (long long)c.nx * c.ny;
+      const int ng = (int)((nsp + span - 1) / span);
+      e->hm[mi].part_base[d] = slot;
+      e->hm[mi].part_count[d] = ng * nbg;
+      slot += ng * nbg;
+    }
+    for (int ci = 0; ci < e->ncls; ++ci) {
+      const EnsClass& c = e->cls[ci];
+      long long nsp = d == 0 ? (long long)c.ny * c.nz : d == 1 ? (long long)c.nx * c.nz
+                                                               : (long long)c.nx * c.ny;
+      const int ng = (int)((nsp + span - 1) / span);
+      for (int g = 0; g < ng; ++g)
+        for (int mi = 0; mi < e->nm; ++mi) {
+          if (e->member_class[mi] != ci) continue;
+          for (int bg = 0; bg < nbg; ++bg)
+            lists[d].push_back(WorkItem{mi, span * g, bg * bpb, e->hm[mi].part_base[d] + g * nbg + bg});
+        }
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    void* p = nullptr;
+    ECK(cudaMalloc(&p, std::max<size_t>(1, lists[d].size()) * sizeof(WorkItem)));
+    e->work_allocs.push_back(p);
+    e->dwork[d] = static_cast<WorkItem*>(p);
+    ECK(cudaMemcpy(p, lists[d].data(), lists[d].size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+    e->nwork[d] = (int)lists[d].size();
+  }
+  void* fp = nullptr;
+  ECK(cudaMalloc(&fp, 2 * (size_t)std::max(1, slot) * sizeof(double)));
+  e->work_allocs.push_back(fp);
+  e->flux_part = static_cast<double*>(fp);
+  for (int mi = 0; mi < e->nm; ++mi) e->hm[mi].flux_part = e->flux_part;
+  // FP64 prep blocks (256 faces each) per member
+  std::vector<int> pm, pf(e->nm);
+  for (int mi = 0; mi < e->nm; ++mi) {
+    const EnsClass& c = e->cls[e->member_class[mi]];
+    long long nf = (long long)(c.nx + 1) * c.ny * c.nz + (long long)(c.ny + 1) * c.nx * c.nz +
+                   (long long)(c.nz + 1) * c.nx * c.ny;
+    pf[mi] = (int)pm.size();
+    for (long long q = 0; q < (nf + 255) / 256; ++q) pm.push_back(mi);
+  }
+  void *a = nullptr, *b = nullptr;
+  ECK(cudaMalloc(&a, std::max<size_t>(1, pm.size()) * sizeof(int)));
+  ECK(cudaMalloc(&b, std::max<size_t>(1, pf.size()) * sizeof(int)));
+  e->work_allocs.push_back(a);
+  e->work_allocs.push_back(b);
+  ECK(cudaMemcpy(a, pm.data(), pm.size() * sizeof(int), cudaMemcpyHostToDevice));
+  ECK(cudaMemcpy(b, pf.data(), pf.size() * sizeof(int), cudaMemcpyHostToDevice));
+  e->dprep_member = static_cast<int*>(a);
+  e->dprep_first = static_cast<int*>(b);
+  e->nprep = (int)pm.size();
+  return upload_members(e);
+}
+
+}  // namespace
+
+extern "C" int f3d_ens_destroy(f3d_ens* e) {
+  if (!e) return 0;
+  cudaSetDevice(e->device);
+  if (e->st) cudaStreamSynchronize(e->st);
+  drop_graphs(e);
+  for (void* p : e->work_allocs) cudaFree(p);
+  for (void* p : e->allocs) cudaFree(p);
+  if (e->h_pin) cudaFreeHost(e->h_pin);
+  if (e->st) cudaStreamDestroy(e->st);
+  delete e;
+  return 0;
+}
+
+extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
+                              const f3d_ens_member* members, int limiter, int time_marching,
+                              int precision, int device, f3d_ens** out) {
+  if (!out || !dims || !members || nclasses < 1 || nmembers < 1)
+    return set_error_msg("f3d_ens_create: bad arguments");
+  if (limiter < 1 || limiter > 3) return set_error_msg("f3d_ens_create: limiter %d not in 1..3", limiter);
+  if (time_marching < 1 || time_marching > 2)
+    return set_error_msg("f3d_ens_create: time_marching %d not in 1..2", time_marching);
+  if (precision != F3D_PREC_FP64 && precision != F3D_PREC_FP32)
+    return set_error_msg("f3d_ens_create: precision %d unknown", precision);
+  const int nb = dims[0].nbins;
+  for (int c = 0; c < nclasses; ++c)
+    if (dims[c].nx < 1 || dims[c].ny < 1 || dims[c].nz < 1 || dims[c].nbins != nb)
+      return set_error_msg("f3d_ens_create: class %d dims invalid or bins differ", c);
+  for (int m = 0; m < nmembers; ++m)
+    if (members[m].grid_class < 0 || members[m].grid_class >= nclasses)
+      return set_error_msg("f3d_ens_create: member %d class %d out of range", m, members[m].grid_class);
+  *out = nullptr;
+  ECK(cudaSetDevice(device));
+  f3d_ens* e = new f3d_ens();
+  e->ncls = nclasses;
+  e->nm = nmembers;
+  e->nb = nb;
+  e->lim = limiter;
+  e->tm = time_marching;
+  e->prec = precision;
+  e->device = device;
+  e->cls.resize(nclasses);
+  e->member_class.resize(nmembers);
+  e->hm.resize(nmembers);
+  int rc = 0;
+  if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete e;
+    return set_error_msg("f3d_ens_create: stream creation failed");
+  }
+  const bool f32 = precision == F3D_PREC_FP32;
+  size_t stage = 0;
+  for (int c = 0; c < nclasses && !rc; ++c) {
+    EnsClass& k = e->cls[c];
+    k.nx = dims[c].nx;
+    k.ny = dims[c].ny;
+    k.nz = dims[c].nz;
+    const size_t nx = k.nx, ny = k.ny, nz = k.nz;
+    const size_t fu = (nx + 1) * ny * nz, fv = (ny + 1) * nx * nz, fw = (nz + 1) * nx * ny;
+    rc |= ealloc(e, &k.ux, 2 * fu);
+    rc |= ealloc(e, &k.vy, 2 * fv);
+    rc |= ealloc(e, &k.wz, 2 * fw);
+    rc |= ealloc(e, &k.k1x, (nx + 2) * ny * nz);
+    rc |= ealloc(e, &k.k2y, (ny + 2) * nx * nz);
+    rc |= ealloc(e, &k.k3z, (nz + 2) * nx * ny);
+    rc |= ealloc(e, &k.vs, nb * fw);
+    if (!f32) {
+      rc |= ealloc(e, &k.kkf[0], fu);
+      rc |= ealloc(e, &k.kkf[1], fv);
+      rc |= ealloc(e, &k.kkf[2], fw);
+      rc |= ealloc(e, &k.geo[0], nx + 1);
+      rc |= ealloc(e, &k.geo[1], ny + 1);
+      rc |= ealloc(e, &k.geo[2], nz + 1);
+    } else {
+      rc |= ealloc(e, &k.ux32, 2 * fu);
+      rc |= ealloc(e, &k.vy32, 2 * fv);
+      rc |= ealloc(e, &k.wz32, 2 * fw);
+      rc |= ealloc(e, &k.kf[0], fu);
+      rc |= ealloc(e, &k.kf[1], fv);
+      rc |= ealloc(e, &k.kf[2], fw);
+      rc |= ealloc(e, &k.vs32, nb * fw);
+      rc |= ealloc(e, &k.rdx[0], nx);
+      rc |= ealloc(e, &k.rdx[1], ny);
+      rc |= ealloc(e, &k.rdx[2], nz);
+    }
+    const size_t dn[6] = {nx + 4, nx + 3, ny + 4, ny + 3, nz + 4, nz + 3};
+    for (int q = 0; q < 6; ++q) rc |= ealloc(e, &k.dx[q], dn[q]);
+    rc |= ealloc(e, &k.hm[0], ny);
+    rc |= ealloc(e, &k.hm[1], ny + 4);
+    rc |= ealloc(e, &k.hm[2], nx * ny);
+    stage = std::max({stage, (nx + 4) * (ny + 4) * (nz + 4) * nb, nx * ny * (nz + 3) * nb,
+                      2 * (nx + 3) * ny * nz, 2 * (ny + 3) * nx * nz, 2 * (nz + 3) * nx * ny,
+                      (nx + 4) * ny * nz, (ny + 4) * nx * nz, (nz + 4) * nx * ny,
+                      2 * (nx + 1) * (ny + 1) * (nz + 1)});
+  }
+  rc |= ealloc(e, &e->flux_tot, 12 * (size_t)nmembers);
+  rc |= ealloc(e, &e->flux_step, 6 * (size_t)nmembers);
+  rc |= ealloc(e, &e->d_red, std::max<size_t>(3 * (size_t)nmembers, (size_t)e->mass_nblk * nb + 64));
+  rc |= ealloc(e, &e->counters, 16);
+  rc |= ealloc(e, &e->d_err, 1);
+  rc |= ealloc(e, &e->d_nfail, 4);
+  rc |= ealloc(e, &e->staging, stage + 4 * (size_t)nb);
+  e->staging_elems = stage;
+  for (int m = 0; m < nmembers && !rc; ++m) {
+    const int c = members[m].grid_class;
+    e->member_class[m] = c;
+    EnsClass& k = e->cls[c];
+    if (k.rep < 0) k.rep = m;
+    MemberDev& d = e->hm[m];
+    memset(&d, 0, sizeof(MemberDev));
+    d.nx = k.nx;
+    d.ny = k.ny;
+    d.nz = k.nz;
+    d.nb = nb;
+    d.wfac = (float)members[m].wind_factor;
+    d.wfacd = members[m].wind_factor;
+    const size_t nx = k.nx, ny = k.ny, nz = k.nz, ncell = nx * ny * nz;
+    const size_t fu = (nx + 1) * ny * nz, fv = (ny + 1) * nx * nz, fw = (nz + 1) * nx * ny;
+    if (f32) rc |= ealloc(e, &d.c32, ncell * nb);
+    else rc |= ealloc(e, &d.c64, ncell * nb);
+    rc |= ealloc(e, &d.acum, nx * ny * nb);
+    d.ux[0] = k.ux; d.ux[1] = k.ux + fu;
+    d.vy[0] = k.vy; d.vy[1] = k.vy + fv;
+    d.wz[0] = k.wz; d.wz[1] = k.wz + fw;
+    d.k1x = k.k1x; d.k2y = k.k2y; d.k3z = k.k3z; d.vs = k.vs;
+    if (!f32) {
+      rc |= ealloc(e, &d.ucur, fu);
+      rc |= ealloc(e, &d.vcur, fv);
+      rc |= ealloc(e, &d.wcur, fw);
+      for (int q = 0; q < 3; ++q) { d.kkf[q] = k.kkf[q]; d.geo[q] = k.geo[q]; }
+    } else {
+      d.ux32[0] = k.ux32; d.ux32[1] = k.ux32 + fu;
+      d.vy32[0] = k.vy32; d.vy32[1] = k.vy32 + fv;
+      d.wz32[0] = k.wz32; d.wz32[1] = k.wz32 + fw;
+      d.kfx = k.kf[0]; d.kfy = k.kf[1]; d.kfz = k.kf[2];
+      d.vs32 = k.vs32;
+      d.rdx1b32 = k.rdx[0]; d.rdx2b32 = k.rdx[1]; d.rdx3b32 = k.rdx[2];
+    }
+    d.dx1p = k.dx[0]; d.dx1b = k.dx[1]; d.dx2p = k.dx[2];
+    d.dx2b = k.dx[3]; d.dx3p = k.dx[4]; d.dx3b = k.dx[5];
+    d.hm1 = k.hm[0]; d.hm2 = k.hm[1]; d.hm3 = k.hm[2];
+    d.flux_tot = e->flux_tot + 12 * (size_t)m;
+    d.flux_step = e->flux_step + 6 * (size_t)m;
+    d.t_ite = 1.0;
+    if (!rc) {
+      if (f32) rc |= cudaMemsetAsync(d.c32, 0, ncell * nb * 4, e->st) != cudaSuccess;
+      else rc |= cudaMemsetAsync(d.c64, 0, ncell * nb * 8, e->st) != cudaSuccess;
+      rc |= cudaMemsetAsync(d.acum, 0, nx * ny * nb * 8, e->st) != cudaSuccess;
+    }
+  }
+  if (!rc) {
+    rc |= cudaMemsetAsync(e->flux_tot, 0, 12 * (size_t)nmembers * 8, e->st) != cudaSuccess;
+    rc |= cudaMemsetAsync(e->flux_step, 0, 6 * (size_t)nmembers * 8, e->st) != cudaSuccess;
+    rc |= cudaMemsetAsync(e->d_err, 0, 4, e->st) != cudaSuccess;
+    e->h_pin_elems = 16 * (size_t)nmembers + 64;
+    rc |= cudaMallocHost(&e->h_pin, e->h_pin_elems * 8) != cudaSuccess;
+  }
+  if (!rc) rc |= ealloc(e, &e->dm, (size_t)nmembers);
+  if (!rc) rc |= build_work(e);
+  if (rc) {
+    f3d_ens_destroy(e);
+    return set_error_msg("f3d_ens_create: device allocation failed (out of memory?)");
+  }
+  *out = e;
+  return 0;
+}
+
+extern "C" int f3d_ens_set_class_grid(f3d_ens* e, int ci, const double* dX1_p, const double* dX1_b,
+                                      const double* dX2_p, const double* dX2_b,
+                                      const double* dX3_p, const double* dX3_b,
+                                      const double* Hm1_p, const double* Hm2_p,
+                                      const double* Hm3_p) {
+  if (!e || ci < 0 || ci >= e->ncls) return set_error_msg("f3d_ens_set_class_grid: bad class");
+  if (!dX1_p || !dX1_b || !dX2_p || !dX2_b || !dX3_p || !dX3_b || !Hm1_p || !Hm2_p || !Hm3_p)
+    return set_error_msg("f3d_ens_set_class_grid: null array");
+  ECK(cudaSetDevice(e->device));
+  EnsClass& k = e->cls[ci];
+  const size_t nx = k.nx, ny = k.ny, nz = k.nz;
+  const double* src[6] = {dX1_p, dX1_b, dX2_p, dX2_b, dX3_p, dX3_b};
+  const size_t dn[6] = {nx + 4, nx + 3, ny + 4, ny + 3, nz + 4, nz + 3};
+  for (int q = 0; q < 6; ++q) ECK(cudaMemcpy(k.dx[q], src[q], dn[q] * 8, cudaMemcpyHostToDevice));
+  ECK(cudaMemcpy(k.hm[0], Hm1_p, ny * 8, cudaMemcpyHostToDevice));
+  ECK(cudaMemcpy(k.hm[1], Hm2_p, (ny + 4) * 8, cudaMemcpyHostToDevice));
+  ECK(cudaMemcpy(k.hm[2], Hm3_p, nx * ny * 8, cudaMemcpyHostToDevice));
+  k.dX1_p.assign(dX1_p, dX1_p + nx + 4);
+  k.dX2_p.assign(dX2_p, dX2_p + ny + 4);
+  k.dX3_p.assign(dX3_p, dX3_p + nz + 4);
+  k.Hm1_p.assign(Hm1_p, Hm1_p + ny);
+  k.Hm2_p.assign(Hm2_p, Hm2_p + ny + 4);
+  k.Hm3_p.assign(Hm3_p, Hm3_p + nx * ny);
+  const double* dp[3] = {dX1_p, dX2_p, dX3_p};
+  const double* db[3] = {dX1_b, dX2_b, dX3_b};
+  const size_t nn[3] = {nx, ny, nz};
+  for (int d = 0; d < 3; ++d) {
+    if (e->prec == F3D_PREC_FP64) {
+      std::vector<double4> g(nn[d] + 1);
+      for (size_t q = 0; q <= nn[d]; ++q) {
+        double a = dp[d][q + 1], b = db[d][q];
+        if (!(std::fabs(a) >= 0x1p-100 && std::fabs(a) <= 0x1p100 && std::fabs(b) >= 0x1p-100 &&
+              std::fabs(b) <= 0x1p100))
+          return set_error_msg("f3d_ens_set_class_grid: spacing outside [2^-100, 2^100]");
+        g[q] = make_double4(a, 1.0 / a, b, 1.0 / b);
+      }
+      ECK(cudaMemcpy(k.geo[d], g.data(), g.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> r(nn[d]);
+      for (size_t q = 0; q < nn[d]; ++q) r[q] = (float)(1.0 / db[d][q + 1]);
+      ECK(cudaMemcpy(k.rdx[d], r.data(), nn[d] * 4, cudaMemcpyHostToDevice));
+    }
+  }
+  k.grid_set = true;
+  return 0;
+}
+
+static int ens_upload_conv(f3d_ens* e, const EnsClass& k, int which, const double* host,
+                           size_t elems, double* dst) {
+  if (elems > e->staging_elems) return set_error_msg("ensemble staging too small");
+  ECK(cudaMemcpyAsync(e->staging, host, elems * 8, cudaMemcpyHostToDevice, e->st));
+  launch_conv(which, e->staging, dst, k.nx, k.ny, k.nz, e->nb, e->st);
+  e->launches += 1;
+  ECKL();
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+static int class_derived_fields(f3d_ens* e, int ci) {
+  EnsClass& k = e->cls[ci];
+  if (k.rep < 0 || !k.meteo_set) return 0;
+  if (e->prec == F3D_PREC_FP32) launch_fp32_fields(e->dm, k.rep, e->st);
+  else launch_face_kk(e->dm, k.rep, e->st);
+  e->launches += 1;
+  ECKL();
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+extern "C" int f3d_ens_set_class_meteo(f3d_ens* e, int ci, const double* u, const double* v,
+                                       const double* w, const double* k1, const double* k2,
+                                       const double* k3, const double* vs, double t_its,
+                                       double t_ite) {
+  if (!e || ci < 0 || ci >= e->ncls) return set_error_msg("f3d_ens_set_class_meteo: bad class");
+  if (!u || !v || !w || !k1 || !k2 || !k3) return set_error_msg("f3d_ens_set_class_meteo: null array");
+  if (!(t_ite != t_its)) return set_error_msg("f3d_ens_set_class_meteo: t_ite == t_its");
+  ECK(cudaSetDevice(e->device));
+  EnsClass& k = e->cls[ci];
+  const size_t nx = k.nx, ny = k.ny, nz = k.nz, nb = e->nb;
+  if (ens_upload_conv(e, k, 0, u, 2 * (nx + 3) * ny * nz, k.ux) ||
+      ens_upload_conv(e, k, 1, v, 2 * (ny + 3) * nx * nz, k.vy) ||
+      ens_upload_conv(e, k, 2, w, 2 * (nz + 3) * nx * ny, k.wz) ||
+      ens_upload_conv(e, k, 3, k1, (nx + 4) * ny * nz, k.k1x) ||
+      ens_upload_conv(e, k, 4, k2, (ny + 4) * nx * nz, k.k2y) ||
+      ens_upload_conv(e, k, 5, k3, (nz + 4) * nx * ny, k.k3z))
+    return 1;
+  if (vs && ens_upload_conv(e, k, 6, vs, nx * ny * (nz + 3) * nb, k.vs)) return 1;
+  k.t_its = t_its;
+  k.t_ite = t_ite;
+  for (int m = 0; m < e->nm; ++m)
+    if (e->member_class[m] == ci) {
+      e->hm[m].t_its = t_its;
+      e->hm[m].t_ite = t_ite;
+    }
+  if (upload_members(e)) return 1;
+  k.meteo_set = true;
+  return class_derived_fields(e, ci);
+}
+
+extern "C" int f3d_ens_compute_class_vset(f3d_ens* e, int ci, int model, const double* rhoc,
+                                          const double* tc, const double* diam,
+                                          const double* rhop, const double* psi,
+                                          const int* bin_cat, const int* is_aggregate,
+                                          double vset_fac) {
+  if (!e || ci < 0 || ci >= e->ncls) return set_error_msg("f3d_ens_compute_class_vset: bad class");
+  if (!rhoc || !tc || !diam || !rhop || !psi || !bin_cat)
+    return set_error_msg("f3d_ens_compute_class_vset: null array");
+  if (model < 1 || model > 7) return set_error_msg("setling velocity model not found");
+  EnsClass& k = e->cls[ci];
+  if (k.rep < 0) return 0;
+  if (!k.grid_set) return set_error_msg("f3d_ens_compute_class_vset: grid not set");
+  ECK(cudaSetDevice(e->device));
+  const size_t ncor = (size_t)(k.nx + 1) * (k.ny + 1) * (k.nz + 1);
+  if (2 * ncor + 4 * (size_t)e->nb > e->staging_elems + 4 * (size_t)e->nb)
+    return set_error_msg("ensemble staging too small for corner fields");
+  double* drho = e->staging;
+  double* dtc = drho + ncor;
+  double* dpar = dtc + ncor;
+  int* dflags = reinterpret_cast<int*>(dpar + 3 * e->nb);
+  std::vector<double> par(3 * e->nb);
+  std::vector<int> fl(e->nb);
+  for (int b = 0; b < e->nb; ++b) {
+    par[3 * b] = diam[b];
+    par[3 * b + 1] = rhop[b];
+    par[3 * b + 2] = psi[b];
+    fl[b] = bin_cat[b] | ((is_aggregate && is_aggregate[b]) ? (1 << 8) : 0);
+  }
+  ECK(cudaMemcpyAsync(drho, rhoc, ncor * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(dtc, tc, ncor * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(dpar, par.data(), par.size() * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(dflags, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemsetAsync(e->d_nfail, 0, 4, e->st));
+  launch_vset_field(e->dm, k.rep, model, drho, dtc, dpar, dflags, vset_fac, e->d_nfail, e->st);
+  e->launches += 1;
+  ECKL();
+  int nfail = 0;
+  ECK(cudaMemcpyAsync(e->h_pin, e->d_nfail, 4, cudaMemcpyDeviceToHost, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  memcpy(&nfail, e->h_pin, 4);
+  if (class_derived_fields(e, ci)) return 1;
+  if (nfail) {
+    set_error_msg("no convergence in vset (%d points)", nfail);
+    return 2;
+  }
+  return 0;
+}
+
+extern "C" int f3d_ens_set_member_source(f3d_ens* e, int mi, int n, const int* ijk,
+                                         const double* s) {
+  if (!e || mi < 0 || mi >= e->nm) return set_error_msg("f3d_ens_set_member_source: bad member");
+  if (n < 0 || (n > 0 && (!ijk || !s))) return set_error_msg("f3d_ens_set_member_source: bad arguments");
+  const EnsClass& k = e->cls[e->member_class[mi]];
+  if (!k.grid_set) return set_error_msg("f3d_ens_set_member_source: grid not set");
+  ECK(cudaSetDevice(e->device));
+  MemberDev& m = e->hm[mi];
+  std::vector<int> cell(n);
+  std::vector<double> vol(n);
+  for (int q = 0; q < n; ++q) {
+    int i = ijk[3 * q] - 1, j = ijk[3 * q + 1] - 1, kk = ijk[3 * q + 2] - 1;
+    if (i < 0 || i >= k.nx || j < 0 || j >= k.ny || kk < 0 || kk >= k.nz)
+      return set_error_msg("f3d_ens_set_member_source: cell %d outside the domain", q);
+    cell[q] = i + k.nx * (j + k.ny * kk);
+    volatile double a = k.dX1_p[i + 2] * k.dX2_p[j + 2];
+    volatile double b = a * k.dX3_p[kk + 2];
+    volatile double h = k.Hm1_p[j] * k.Hm2_p[j + 2];
+    volatile double h3 = h * k.Hm3_p[i + (size_t)k.nx * j];
+    vol[q] = b * h3;
+  }
+  if (n > 0) {
+    int* dc;
+    double *ds, *dv;
+    if (ealloc(e, &dc, (size_t)n) || ealloc(e, &ds, (size_t)n * e->nb) || ealloc(e, &dv, (size_t)n))
+      return 1;
+    ECK(cudaMemcpy(dc, cell.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    ECK(cudaMemcpy(ds, s, sizeof(double) * n * e->nb, cudaMemcpyHostToDevice));
+    ECK(cudaMemcpy(dv, vol.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    m.src_cell = dc;
+    m.src_s = ds;
+    m.src_vol = dv;
+  }
+  m.nsrc = n;
+  return upload_members(e);
+}
+
+extern "C" int f3d_ens_upload_member_state(f3d_ens* e, int mi, const double* my_c,
+                                           const double* my_acum) {
+  if (!e || mi < 0 || mi >= e->nm) return set_error_msg("f3d_ens_upload_member_state: bad member");
+  ECK(cudaSetDevice(e->device));
+  const EnsClass& k = e->cls[e->member_class[mi]];
+  MemberDev& m = e->hm[mi];
+  const size_t nx = k.nx, ny = k.ny, nz = k.nz, nb = e->nb;
+  if (my_c) {
+    if (e->prec == F3D_PREC_FP64) {
+      if (ens_upload_conv(e, k, 7, my_c, (nx + 4) * (ny + 4) * (nz + 4) * nb, m.c64)) return 1;
+    } else {
+      std::vector<float> tmp(nx * ny * nz * nb);
+      for (size_t b = 0; b < nb; ++b)
+        for (size_t kk = 0; kk < nz; ++kk)
+          for (size_t j = 0; j < ny; ++j)
+            for (size_t i = 0; i < nx; ++i)
+              tmp[((b * nz + kk) * ny + j) * nx + i] = (float)my_c[(i + 2) + (nx + 4) *
+                  ((j + 2) + (ny + 4) * ((kk + 2) + (nz + 4) * b))];
+      ECK(cudaMemcpy(m.c32, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice));
+    }
+  }
+  if (my_acum && ens_upload_conv(e, k, 8, my_acum, (nx + 4) * (ny + 4) * nb, m.acum)) return 1;
+  return 0;
+}
+
+extern "C" int f3d_ens_download_member_state(f3d_ens* e, int mi, double* my_c, double* my_acum) {
+  if (!e || mi < 0 || mi >= e->nm) return set_error_msg("f3d_ens_download_member_state: bad member");
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaStreamSynchronize(e->st));
+  const EnsClass& k = e->cls[e->member_class[mi]];
+  const MemberDev& m = e->hm[mi];
+  const size_t nx = k.nx, ny = k.ny, nz = k.nz, nb = e->nb;
+  if (my_c) {
+    std::vector<double> tmp(nx * ny * nz * nb);
+    if (e->prec == F3D_PREC_FP64) {
+      ECK(cudaMemcpy(tmp.data(), m.c64, tmp.size() * 8, cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> t32(tmp.size());
+      ECK(cudaMemcpy(t32.data(), m.c32, t32.size() * 4, cudaMemcpyDeviceToHost));
+      for (size_t q = 0; q < t32.size(); ++q) tmp[q] = t32[q];
+    }
+    for (size_t b = 0; b < nb; ++b)
+      for (size_t kk = 0; kk < nz; ++kk)
+        for (size_t j = 0; j < ny; ++j)
+          memcpy(&my_c[2 + (nx + 4) * ((j + 2) + (ny + 4) * ((kk + 2) + (nz + 4) * b))],
+                 &tmp[((b * nz + kk) * ny + j) * nx], nx * 8);
+  }
+  if (my_acum) {
+    std::vector<double> tmp(nx * ny * nb);
+    ECK(cudaMemcpy(tmp.data(), m.acum, tmp.size() * 8, cudaMemcpyDeviceToHost));
+    for (size_t b = 0; b < nb; ++b)
+      for (size_t j = 0; j < ny; ++j)
+        memcpy(&my_acum[2 + (nx + 4) * ((j + 2) + (ny + 4) * b)], &tmp[(b * ny + j) * nx], nx * 8);
+  }
+  return 0;
+}
+
+// ---- time step, clock and execution ----------------------------------------
+extern "C" int f3d_ens_compute_time_steps(f3d_ens* e, double stime, int criterion, double cfl,
+                                          double run_end, double* dt) {
+  if (!e) return set_error_msg("f3d_ens_compute_time_steps: null ensemble");
+  if (criterion != 1 && criterion != 2)
+    return set_error_msg("f3d_ens_compute_time_steps: criterion %d not in 1..2", criterion);
+  for (const EnsClass& k : e->cls)
+    if (k.rep >= 0 && !k.meteo_set) return set_error_msg("f3d_ens_compute_time_steps: meteo not set");
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaMemsetAsync(e->d_red, 0, 3 * (size_t)e->nm * sizeof(double), e->st));
+  for (int m = 0; m < e->nm; ++m) {
+    launch_cfl(e->dm, m, stime, criterion, e->d_red + 3 * (size_t)m, e->st);
+    e->launches += 1;
+  }
+  launch_finalize_dt(e->dm, e->nm, e->d_red, cfl, run_end, e->st);
+  e->launches += 1;
+  ECKL();
+  if (pull_dynamic(e)) return 1;
+  if (dt)
+    for (int m = 0; m < e->nm; ++m) dt[m] = e->hm[m].dt;
+  return 0;
+}
+
+extern "C" int f3d_ens_set_clock(f3d_ens* e, const double* time, int iiter) {
+  if (!e || !time) return set_error_msg("f3d_ens_set_clock: null argument");
+  ECK(cudaSetDevice(e->device));
+  if (pull_dynamic(e)) return 1;
+  for (int m = 0; m < e->nm; ++m) {
+    MemberDev& d = e->hm[m];
+    d.time = time[m];
+    d.iiter = iiter;
+    d.stime = (time[m] - d.t_its) / (d.t_ite - d.t_its);
+  }
+  e->iiter = iiter;
+  ECK(cudaMemcpyAsync(e->dm, e->hm.data(), sizeof(MemberDev) * e->nm, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+extern "C" int f3d_ens_get_clock(f3d_ens* e, double* time, int* iiter) {
+  if (!e) return set_error_msg("f3d_ens_get_clock: null ensemble");
+  ECK(cudaSetDevice(e->device));
+  if (pull_dynamic(e)) return 1;
+  if (time)
+    for (int m = 0; m < e->nm; ++m) time[m] = e->hm[m].time;
+  if (iiter) *iiter = e->hm[0].iiter;
+  return 0;
+}
+
+extern "C" int f3d_ens_set_tuning(f3d_ens* e, int mode, int bins_per_block, int ctas_per_sm) {
+  if (!e) return set_error_msg("f3d_ens_set_tuning: null ensemble");
+  if (mode != F3D_ENS_MODE_KERNELS && mode != F3D_ENS_MODE_PERSISTENT)
+    return set_error_msg("f3d_ens_set_tuning: mode %d unknown", mode);
+  if (bins_per_block != 1 && bins_per_block != 2 && bins_per_block != 4)
+    return set_error_msg("f3d_ens_set_tuning: bins_per_block %d not 1, 2 or 4", bins_per_block);
+  if (ctas_per_sm < 0 || ctas_per_sm > 16)
+    return set_error_msg("f3d_ens_set_tuning: ctas_per_sm %d out of range", ctas_per_sm);
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaStreamSynchronize(e->st));
+  drop_graphs(e);
+  e->mode = mode;
+  e->ctas_per_sm = ctas_per_sm;
+  if (bins_per_block != e->bpb) {
+    if (pull_dynamic(e)) return 1;
+    e->bpb = bins_per_block;
+    if (build_work(e)) return 1;
+  }
+  return 0;
+}
+
+namespace {
+
+int fused_setup(f3d_ens* e, const void** func, int* smem) {
+  const bool f32 = e->prec == F3D_PREC_FP32;
+  *func = f32 ? fused32_func(e->lim, e->tm) : fused64_func(e->lim, e->tm);
+  *smem = f32 ? fused32_smem() : fused64_smem();
+  ECK(cudaFuncSetAttribute(*func, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
+  int per_sm = 0;
+  ECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, *func, 128, *smem));
+  if (per_sm < 1) return set_error_msg("persistent step kernel does not fit on an SM");
+  if (e->ctas_per_sm > 0) per_sm = std::min(per_sm, e->ctas_per_sm);
+  int nsm = 0;
+  ECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device));
+  e->fused_grid = per_sm * nsm;
+  return 0;
+}
+
+// Enqueue one step.  set_host: dt/time come from the host arrays.
+int enqueue_step(f3d_ens* e, bool xfirst, bool advance) {
+  if (e->mode == F3D_ENS_MODE_PERSISTENT) {
+    const void* func;
+    int smem;
+    if (fused_setup(e, &func, &smem)) return 1;
+    ECK(cudaMemsetAsync(e->counters, 0, 16 * sizeof(unsigned int), e->st));
+    FusedArgs a;
+    a.members = e->dm;
+    a.nmembers = e->nm;
+    for (int d = 0; d < 3; ++d) {
+      a.work[d] = e->dwork[d];
+      a.nwork[d] = e->nwork[d];
+    }
+    a.prep_member = e->dprep_member;
+    a.prep_first = e->dprep_first;
+    a.nprep = e->prec == F3D_PREC_FP64 ? e->nprep : 0;
+    a.counters = e->counters;
+    a.err = e->d_err;
+    a.bpb = e->bpb;
+    void* args[] = {&a};
+    ECK(cudaLaunchCooperativeKernel(func, dim3(e->fused_grid), dim3(128), args, (size_t)smem, e->st));
+    e->launches += 1;
+    return 0;
+  }
+  if (e->prec == F3D_PREC_FP64) {
+    launch_prep64(e->dm, e->dprep_member, e->dprep_first, e->nprep, 7, e->st);
+    launch_source64(e->dm, e->nm, e->st);
+  } else {
+    launch_source32(e->dm, e->nm, e->st);
+  }
+  e->launches += (e->prec == F3D_PREC_FP64) ? 2 : 1;
+  const int order[3] = {xfirst ? DIR_X : DIR_Y, xfirst ? DIR_Y : DIR_X, DIR_Z};
+  for (int q = 0; q < 3; ++q) {
+    const int d = order[q];
+    if (e->prec == F3D_PREC_FP64)
+      launch_sweep64(d, e->lim, e->tm, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
+    else
+      launch_sweep32(d, e->lim, e->tm, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
+    e->launches += 1;
+  }
+  launch_flux_reduce(e->dm, e->nm, 7, e->st);
+  e->launches += 1;
+  if (advance) {
+    launch_advance_clock(e->dm, e->nm, e->st);
+    e->launches += 1;
+  }
+  ECKL();
+  return 0;
+}
+
+int build_graphs(f3d_ens* e) {
+  drop_graphs(e);
+  const int ng = (e->mode == F3D_ENS_MODE_PERSISTENT) ? 1 : 2;
+  for (int q = 0; q < ng; ++q) {
+    cudaGraph_t g = nullptr;
+    ECK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    long long keep = e->launches;
+    int rc = enqueue_step(e, q == 0, true);
+    cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+    e->launches = keep;
+    if (rc || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return set_error_msg("step graph capture failed: %s", cudaGetErrorString(ce));
+    }
+    cudaError_t ie = cudaGraphInstantiate(&e->graph[q], g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return set_error_msg("graph instantiation failed: %s", cudaGetErrorString(ie));
+  }
+  if (ng == 1) e->graph[1] = nullptr;
+  e->graph_ok = true;
+  return 0;
+}
+
+int kernels_per_step(const f3d_ens* e) {
+  if (e->mode == F3D_ENS_MODE_PERSISTENT) return 1;
+  return (e->prec == F3D_PREC_FP64 ? 2 : 1) + 3 + 1 + 1;
+}
+
+}  // namespace
+
+extern "C" int f3d_ens_run(f3d_ens* e, int nsteps) {
+  if (!e || nsteps < 0) return set_error_msg("f3d_ens_run: bad arguments");
+  for (const EnsClass& k : e->cls)
+    if (k.rep >= 0 && (!k.meteo_set || !k.grid_set)) return set_error_msg("f3d_ens_run: class not ready");
+  ECK(cudaSetDevice(e->device));
+  if (!e->graph_ok && build_graphs(e)) return 1;
+  for (int s = 0; s < nsteps; ++s) {
+    cudaGraphExec_t g = (e->mode == F3D_ENS_MODE_PERSISTENT) ? e->graph[0] : e->graph[e->iiter & 1];
+    ECK(cudaGraphLaunch(g, e->st));
+    e->launches += kernels_per_step(e);
+    e->iiter += 1;
+  }
+  return 0;
+}
+
+extern "C" int f3d_ens_step(f3d_ens* e, const double* dt, const double* time, int iiter,
+                            double* fluxes) {
+  if (!e || !dt || !time) return set_error_msg("f3d_ens_step: null argument");
+  for (const EnsClass& k : e->cls)
+    if (k.rep >= 0 && (!k.meteo_set || !k.grid_set)) return set_error_msg("f3d_ens_step: class not ready");
+  ECK(cudaSetDevice(e->device));
+  launch_set_steps(e->dm, e->nm, dt, time, iiter, e->st);
+  e->launches += (e->nm + 63) / 64;
+  ECKL();
+  if (enqueue_step(e, iiter % 2 == 0, false)) return 1;
+  e->iiter = iiter + 1;
+  if (fluxes) {
+    ECK(cudaMemcpyAsync(e->h_pin, e->flux_step, 6 * (size_t)e->nm * 8, cudaMemcpyDeviceToHost, e->st));
+    ECK(cudaStreamSynchronize(e->st));
+    for (int q = 0; q < 6 * e->nm; ++q) fluxes[q] = fluxes[q] + e->h_pin[q];
+  }
+  return 0;
+}
+
+extern "C" int f3d_ens_get_fluxes(f3d_ens* e, double* fluxes) {
+  if (!e || !fluxes) return set_error_msg("f3d_ens_get_fluxes: null argument");
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaMemcpyAsync(e->h_pin, e->flux_tot, 12 * (size_t)e->nm * 8, cudaMemcpyDeviceToHost, e->st));
+  ECK(cudaMemsetAsync(e->flux_tot, 0, 12 * (size_t)e->nm * 8, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  for (int m = 0; m < e->nm; ++m)
+    for (int q = 0; q < 6; ++q)
+      fluxes[6 * m + q] = fluxes[6 * m + q] + (e->h_pin[12 * m + q] - e->h_pin[12 * m + 6 + q]);
+  return 0;
+}
+
+extern "C" int f3d_ens_mass_volume(f3d_ens* e, int mi, double* mass) {
+  if (!e || !mass || mi < 0 || mi >= e->nm) return set_error_msg("f3d_ens_mass_volume: bad arguments");
+  if (e->nb > 64) return set_error_msg("f3d_ens_mass_volume: more than 64 bins");
+  ECK(cudaSetDevice(e->device));
+  double* out = e->d_red + (size_t)e->mass_nblk * e->nb;
+  launch_mass(e->dm, mi, e->nb, e->prec == F3D_PREC_FP32, e->d_red, e->mass_nblk, out, e->st);
+  e->launches += 2;
+  ECKL();
+  ECK(cudaMemcpyAsync(e->h_pin, out, e->nb * 8, cudaMemcpyDeviceToHost, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  double tot = 0.0, comp = 0.0;
+  for (int b = 0; b < e->nb; ++b) {
+    double x = e->h_pin[b], t = tot + x;
+    comp += (std::fabs(tot) >= std::fabs(x)) ? (tot - t) + x : (x - t) + tot;
+    tot = t;
+  }
+  *mass = tot + comp;
+  return 0;
+}
+
+extern "C" int f3d_ens_synchronize(f3d_ens* e) {
+  if (!e) return set_error_msg("f3d_ens_synchronize: null ensemble");
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+extern "C" int f3d_ens_get_stream(f3d_ens* e, void** stream) {
+  if (!e || !stream) return set_error_msg("f3d_ens_get_stream: null argument");
+  *stream = (void*)e->st;
+  return 0;
+}
+
+extern "C" int f3d_ens_launch_count(f3d_ens* e, long long* count) {
+  if (!e || !count) return set_error_msg("f3d_ens_launch_count: null argument");
+  *count = e->launches;
+  return 0;
+}
+
+extern "C" int f3d_ens_status(f3d_ens* e, int* device_error) {
+  if (!e || !device_error) return set_error_msg("f3d_ens_status: null argument");
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaMemcpy(device_error, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  return 0;
+}

@@ -211,6 +211,7 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
   MemberDev& m = c->hm;
   m.nx = c->nx; m.ny = c->ny; m.nz = c->nz; m.nb = c->nb;
   m.wfac = 1.0f;
+  m.wfacd = 1.0;
   const size_t nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb;
   const size_t ncell = nx * ny * nz;
   int rc = 0;

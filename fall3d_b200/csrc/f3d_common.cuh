@@ -62,7 +62,8 @@ struct MemberDev {
   float* ucur32;
   float* vcur32;
   float* wcur32;
-  float wfac;       // per-member multiplicative factor on u,v (ensemble)
+  float wfac;       // per-member multiplicative factor on u,v (ensemble), FP32 form
+  double wfacd;     // the same factor for the FP64 form and the CFL reduction
   // grid metrics (reference arrays with their halos)
   const double* dx1p;  // (nx+4)   ips-2..ipe+2
   const double* dx1b;  // (nx+3)   ibs-1..ibe+1

@@ -1,0 +1,313 @@
+"""Batched ensemble on one GPU (f3d_ens_* of the C ABI) and its workloads.
+
+FALL3D builds an ensemble by perturbing inputs of each member
+(ensemble_perturbate_variable, mod_Ensemble.F90:888-935) and runs members as
+separate jobs.  Here all members advance together on one GPU: members are
+grouped into grid classes that share grid, meteo and settling velocity; each
+member has its own wind factor, source, concentration, time step and clock.
+
+  Ensemble            the C-ABI object (step, run on the device clock, tuning)
+  ensemble_workload   members on uneven grids with perturbed wind, source
+                      height and mass rate (seeded)
+  autotune            picks execution mode and bins per block by timing a
+                      few steps, cached per (class shapes, bins, precision)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import workloads as W
+from ._lib import F3DDims, F3DEnsMember, F3DError, check, lib
+from .source import (ID_COLUMN_HEIGHT, ID_U_WIND, PERTURBATION_TYPE_ABSOLUTE,
+                     PERTURBATION_TYPE_RELATIVE, perturbate, place_source, suzuki)
+
+MODE_KERNELS, MODE_PERSISTENT = 0, 1
+_dp = C.POINTER(C.c_double)
+
+
+def _p(a):
+    if a is None:
+        return None
+    if not (a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim <= 1)):
+        raise F3DError("arrays must be Fortran-contiguous float64")
+    return a.ctypes.data_as(_dp)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class Ensemble:
+    """An f3d_ens: members of several grid classes stepped together."""
+
+    def __init__(self, class_grids, nbins, member_classes, wind_factors, limiter=2,
+                 time_marching=2, precision=1, device=0):
+        self.grids = list(class_grids)
+        self.nbins = nbins
+        self.member_classes = list(member_classes)
+        self.nm = len(member_classes)
+        dims = (F3DDims * len(self.grids))(*[F3DDims(g.nx, g.ny, g.nz, nbins) for g in self.grids])
+        mem = (F3DEnsMember * self.nm)(*[F3DEnsMember(int(c), float(f))
+                                         for c, f in zip(member_classes, wind_factors)])
+        h = C.c_void_p()
+        check(lib().f3d_ens_create(len(self.grids), dims, self.nm, C.cast(mem, C.c_void_p),
+                                   limiter, time_marching, precision, device, C.byref(h)),
+              "f3d_ens_create")
+        self._h = h
+        self.precision = precision
+        self._keep = []
+        for ci, g in enumerate(self.grids):
+            arrs = [np.ascontiguousarray(getattr(g, n), dtype=np.float64) for n in
+                    ("dX1_p", "dX1_b", "dX2_p", "dX2_b", "dX3_p", "dX3_b", "Hm1_p", "Hm2_p")]
+            arrs.append(np.asfortranarray(g.Hm3_p, dtype=np.float64))
+            self._keep.append(arrs)
+            check(lib().f3d_ens_set_class_grid(self._h, ci, *[_p(a) for a in arrs]),
+                  "f3d_ens_set_class_grid")
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().f3d_ens_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_class_meteo(self, ci, u12, v12, w12, k1, k2, k3, vs, t_its, t_ite):
+        check(lib().f3d_ens_set_class_meteo(self._h, ci, _p(u12), _p(v12), _p(w12), _p(k1), _p(k2),
+                                            _p(k3), _p(vs), float(t_its), float(t_ite)),
+              "f3d_ens_set_class_meteo")
+
+    def compute_class_vset(self, ci, model, rhoc, tc, diam, rhop, psi, bin_cat):
+        cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
+        check(lib().f3d_ens_compute_class_vset(
+            self._h, ci, int(model), _p(np.asfortranarray(rhoc, dtype=np.float64)),
+            _p(np.asfortranarray(tc, dtype=np.float64)), _p(np.ascontiguousarray(diam, np.float64)),
+            _p(np.ascontiguousarray(rhop, np.float64)), _p(np.ascontiguousarray(psi, np.float64)),
+            _ip(cat), None, 1.0), "f3d_ens_compute_class_vset")
+
+    def set_member_source(self, m, ijk, vals):
+        ijk = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
+        vals = np.ascontiguousarray(vals, dtype=np.float64).reshape(-1, self.nbins)
+        check(lib().f3d_ens_set_member_source(self._h, m, len(ijk), _ip(ijk), vals.ctypes.data_as(_dp)),
+              "f3d_ens_set_member_source")
+
+    def upload_member_state(self, m, my_c=None, my_acum=None):
+        check(lib().f3d_ens_upload_member_state(self._h, m, _p(my_c), _p(my_acum)),
+              "f3d_ens_upload_member_state")
+
+    def download_member_state(self, m):
+        g = self.grids[self.member_classes[m]]
+        c = np.zeros((g.nx + 4, g.ny + 4, g.nz + 4, self.nbins), order="F")
+        a = np.zeros((g.nx + 4, g.ny + 4, self.nbins), order="F")
+        check(lib().f3d_ens_download_member_state(self._h, m, _p(c), _p(a)),
+              "f3d_ens_download_member_state")
+        return c, a
+
+    def compute_time_steps(self, stime=0.5, criterion=2, cfl=0.9, run_end=1e30):
+        dt = np.zeros(self.nm)
+        check(lib().f3d_ens_compute_time_steps(self._h, float(stime), int(criterion), float(cfl),
+                                               float(run_end), _p(dt)), "f3d_ens_compute_time_steps")
+        return dt
+
+    def set_clock(self, times, iiter=0):
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(times, dtype=np.float64), (self.nm,)))
+        check(lib().f3d_ens_set_clock(self._h, _p(t), int(iiter)), "f3d_ens_set_clock")
+
+    def get_clock(self):
+        t = np.zeros(self.nm)
+        it = C.c_int()
+        check(lib().f3d_ens_get_clock(self._h, _p(t), C.byref(it)), "f3d_ens_get_clock")
+        return t, it.value
+
+    def set_tuning(self, mode=MODE_KERNELS, bins_per_block=4, ctas_per_sm=0):
+        check(lib().f3d_ens_set_tuning(self._h, int(mode), int(bins_per_block), int(ctas_per_sm)),
+              "f3d_ens_set_tuning")
+        self.tuning = (mode, bins_per_block, ctas_per_sm)
+
+    def run(self, nsteps):
+        check(lib().f3d_ens_run(self._h, int(nsteps)), "f3d_ens_run")
+
+    def step(self, dt, times, iiter, fluxes=None):
+        dt = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (self.nm,)))
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(times, dtype=np.float64), (self.nm,)))
+        check(lib().f3d_ens_step(self._h, _p(dt), _p(t), int(iiter), _p(fluxes)), "f3d_ens_step")
+        return fluxes
+
+    def get_fluxes(self):
+        f = np.zeros(6 * self.nm)
+        check(lib().f3d_ens_get_fluxes(self._h, _p(f)), "f3d_ens_get_fluxes")
+        return f.reshape(self.nm, 6)
+
+    def mass_volume(self, m):
+        x = C.c_double()
+        check(lib().f3d_ens_mass_volume(self._h, m, C.byref(x)), "f3d_ens_mass_volume")
+        return x.value
+
+    def synchronize(self):
+        check(lib().f3d_ens_synchronize(self._h), "f3d_ens_synchronize")
+
+    @property
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        check(lib().f3d_ens_get_stream(self._h, C.byref(s)), "f3d_ens_get_stream")
+        return s.value or 0
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        check(lib().f3d_ens_launch_count(self._h, C.byref(n)), "f3d_ens_launch_count")
+        return n.value
+
+    def status(self) -> int:
+        e = C.c_int()
+        check(lib().f3d_ens_status(self._h, C.byref(e)), "f3d_ens_status")
+        return e.value
+
+
+# ---------------------------------------------------------------------------
+@dataclass
+class EnsembleWorkload:
+    """Grid classes (with their meteo) and perturbed members."""
+    classes: list                      # Workload per grid class (meteo, bins, air)
+    member_class: list
+    wind_factor: list
+    src: list                          # (ijk, vals) per member
+    mass_rate: list
+    heights: list = field(default_factory=list)
+
+    @property
+    def nbins(self):
+        return self.classes[0].nbins
+
+    def cell_bins(self, m=None):
+        def cb(c):
+            g = self.classes[c].grid
+            return g.nx * g.ny * g.nz * self.nbins
+        if m is not None:
+            return cb(self.member_class[m])
+        return sum(cb(c) for c in self.member_class)
+
+
+def ensemble_workload(class_shapes=((200, 150, 40), (400, 300, 60), (600, 450, 80)),
+                      class_members=(16, 32, 16), nbins=12, seed=0, height=8000.0,
+                      mfr=1e6, wind_range=20.0, height_range=2000.0):
+    """Members on uneven grids: u, v x (1 + r wind_range/100) with r uniform in
+    [-1, 1] (RELATIVE), column height + r height_range (ABSOLUTE), mass flow
+    rate x 2^s with s uniform in [-1, 1] (log-uniform in [0.5, 2]; the
+    reference has no log-uniform PDF, mod_Ensemble.F90:39-40).  Member 0 of
+    every class is unperturbed, like the reference's first member
+    (mod_Ensemble.F90:775-776)."""
+    rng = np.random.default_rng(seed)
+    classes = []
+    for ci, (nx, ny, nz) in enumerate(class_shapes):
+        wl = W.random_c2(nx, ny, nz, nbins, hours=1.0, seed=seed * 100 + ci, src_heights=(height,),
+                         mass_rates=(mfr,))
+        classes.append(wl)
+    member_class, wind, src, rates, heights = [], [], [], [], []
+    for ci, nmem in enumerate(class_members):
+        g = classes[ci].grid
+        for q in range(nmem):
+            r = np.zeros(3) if q == 0 else rng.uniform(-1.0, 1.0, 3)
+            f = float(perturbate(ID_U_WIND, PERTURBATION_TYPE_RELATIVE, 1.0, r[0], wind_range))
+            H = float(perturbate(ID_COLUMN_HEIGHT, PERTURBATION_TYPE_ABSOLUTE, height, r[1],
+                                 height_range))
+            H = min(H, 0.95 * g.X3max)
+            M0 = mfr * 2.0 ** r[2]
+            zs, M = suzuki(100, M0, H, 4.0, 5.0, 0.0, classes[ci].bin_fc)
+            lon = g.lon_p[int(0.35 * g.nx)]
+            lat = g.lat_p[int(0.4 * g.ny)]
+            ijk, vals = place_source(g, np.full(100, lon), np.full(100, lat), zs, M)
+            member_class.append(ci)
+            wind.append(f)
+            src.append((ijk, vals))
+            rates.append(float(M.sum()))
+            heights.append(H)
+    return EnsembleWorkload(classes, member_class, wind, src, rates, heights)
+
+
+def build_ensemble(ew: EnsembleWorkload, precision=1, device=0, vset="iterative", vs_classes=None,
+                   limiter=2, time_marching=2):
+    """Create the device ensemble and load meteo, settling velocity, sources.
+    vset: "iterative" (phys_get_vset on the device), "given" (vs_classes)."""
+    ens = Ensemble([c.grid for c in ew.classes], ew.nbins, ew.member_class, ew.wind_factor,
+                   limiter, time_marching, precision, device)
+    for ci, wl in enumerate(ew.classes):
+        vs = None if vs_classes is None else vs_classes[ci]
+        ens.set_class_meteo(ci, wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3, vs, wl.t_its, wl.t_ite)
+        if vs is None and vset == "iterative":
+            ens.compute_class_vset(ci, wl.vset_model, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi,
+                                   wl.bin_cat)
+    for m, (ijk, vals) in enumerate(ew.src):
+        ens.set_member_source(m, ijk, vals)
+    return ens
+
+
+# ---------------------------------------------------------------------------
+def _cache_path():
+    d = os.environ.get("F3D_AUTOTUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache",
+                                                              "fall3d_b200")
+    return os.path.join(d, "autotune.json")
+
+
+def autotune(ens: Ensemble, key: str, steps=2, candidates=None, use_cache=True):
+    """Time each (mode, bins per block, blocks per SM) for a few steps on the
+    device clock and keep the fastest; the result is cached under `key`
+    (class shapes, bins, precision).  Member state advances during tuning,
+    so callers reset the clock/state afterwards if they need to."""
+    path = _cache_path()
+    cache = {}
+    if use_cache and os.path.exists(path):
+        try:
+            with open(path) as f:
+                cache = json.load(f)
+        except (OSError, ValueError):
+            cache = {}
+    if use_cache and key in cache:
+        best = cache[key]
+        ens.set_tuning(*best["tuning"])
+        return best
+    import torch
+    if candidates is None:
+        candidates = [(MODE_KERNELS, b, 0) for b in (4, 2, 1)] + \
+                     [(MODE_PERSISTENT, b, 0) for b in (4, 2)]
+    s = torch.cuda.ExternalStream(ens.stream_ptr)
+    results = []
+    for cand in candidates:
+        try:
+            ens.set_tuning(*cand)
+            ens.run(1)  # warm-up (graph build)
+            ens.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            ens.run(steps)
+            e1.record(s)
+            ens.synchronize()
+            if ens.status() != 0:
+                raise F3DError("device barrier timeout")
+            results.append({"tuning": list(cand), "ms_per_step": e0.elapsed_time(e1) / steps})
+        except F3DError as exc:
+            results.append({"tuning": list(cand), "error": str(exc)[:200]})
+    ok = [r for r in results if "ms_per_step" in r]
+    if not ok:
+        raise F3DError(f"autotune: no configuration ran: {results}")
+    best = min(ok, key=lambda r: r["ms_per_step"])
+    best = {"tuning": best["tuning"], "ms_per_step": best["ms_per_step"], "all": results,
+            "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+    ens.set_tuning(*best["tuning"])
+    if use_cache:
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            cache[key] = best
+            with open(path, "w") as f:
+                json.dump(cache, f, indent=1)
+        except OSError:
+            pass
+    return best

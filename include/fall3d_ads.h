@@ -211,6 +211,78 @@ int f3d_ads_compute_vset(f3d_ctx *ctx, int model, const double *rhoc,
                          const int *bin_cat, const int *is_aggregate,
                          double vset_fac, double *vs_out);
 
+/* ---- batched ensemble -------------------------------------------------------
+ * Ensemble members of FALL3D run as independent jobs in separate MPI
+ * communicators (mod_Parallel.F90:188-217, task_SetEns.F90).  Here every
+ * member of an ensemble lives on one GPU and all members advance together,
+ * one batched step per call.  Members are grouped into grid classes: the
+ * members of a class share the grid, the meteo term and the settling
+ * velocity (the ensemble perturbs the winds by one factor per member,
+ * task_Fall3d.F90:194-198, applied on the device), and own their
+ * concentration, deposit, source, time step and clock. */
+typedef struct f3d_ens f3d_ens;
+
+typedef struct {
+  int grid_class;     /* 0 .. nclasses-1 */
+  double wind_factor; /* multiplier of u and v: 1 + r range/100 (RELATIVE perturbation) */
+} f3d_ens_member;
+
+#define F3D_ENS_MODE_KERNELS 0    /* one kernel per phase, replayed from CUDA graphs */
+#define F3D_ENS_MODE_PERSISTENT 1 /* one persistent cooperative kernel per step */
+
+int f3d_ens_create(int nclasses, const f3d_dims *class_dims, int nmembers,
+                   const f3d_ens_member *members, int limiter, int time_marching,
+                   int precision, int device, f3d_ens **out);
+int f3d_ens_destroy(f3d_ens *ens);
+/* Same arrays and layouts as f3d_ads_set_grid / f3d_ads_set_meteo, per class. */
+int f3d_ens_set_class_grid(f3d_ens *ens, int cls, const double *dX1_p,
+                           const double *dX1_b, const double *dX2_p,
+                           const double *dX2_b, const double *dX3_p,
+                           const double *dX3_b, const double *Hm1_p,
+                           const double *Hm2_p, const double *Hm3_p);
+int f3d_ens_set_class_meteo(f3d_ens *ens, int cls, const double *u,
+                            const double *v, const double *w, const double *k1,
+                            const double *k2, const double *k3, const double *vs,
+                            double t_its, double t_ite);
+/* phys_get_vset + vs/Hm3 of a class on the device (see f3d_ads_compute_vset). */
+int f3d_ens_compute_class_vset(f3d_ens *ens, int cls, int model,
+                               const double *rhoc, const double *tc,
+                               const double *diam, const double *rhop,
+                               const double *psi, const int *bin_cat,
+                               const int *is_aggregate, double vset_fac);
+int f3d_ens_set_member_source(f3d_ens *ens, int member, int n, const int *ijk,
+                              const double *s);
+int f3d_ens_upload_member_state(f3d_ens *ens, int member, const double *my_c,
+                                const double *my_acum);
+int f3d_ens_download_member_state(f3d_ens *ens, int member, double *my_c,
+                                  double *my_acum);
+/* grid_get_time_step for every member at stime (each with its own winds);
+ * the members' dt are set on the device and copied to dt[nmembers] if given. */
+int f3d_ens_compute_time_steps(f3d_ens *ens, double stime, int criterion,
+                               double cfl, double run_end, double *dt);
+/* Model clock of every member (time[nmembers]) and the common iteration. */
+int f3d_ens_set_clock(f3d_ens *ens, const double *time, int iiter);
+int f3d_ens_get_clock(f3d_ens *ens, double *time, int *iiter);
+/* Execution shape: mode, bins per sweep block (1, 2, 4) and, for the
+ * persistent mode, resident blocks per SM (0 = as many as fit). */
+int f3d_ens_set_tuning(f3d_ens *ens, int mode, int bins_per_block,
+                       int ctas_per_sm);
+/* Advance every member nsteps times with its own dt on the device clock
+ * (time += dt, iiter += 1 after each step); enqueued, not waited for. */
+int f3d_ens_run(f3d_ens *ens, int nsteps);
+/* One step with host-given dt[m], time[m]; fluxes[6*m..] INOUT {W,E,S,N,U,D}
+ * (may be NULL: increments stay on the device).  Blocks when fluxes given. */
+int f3d_ens_step(f3d_ens *ens, const double *dt, const double *time, int iiter,
+                 double *fluxes);
+/* Adds the device-accumulated flux totals to fluxes[6*nmembers], zeroes them. */
+int f3d_ens_get_fluxes(f3d_ens *ens, double *fluxes);
+int f3d_ens_mass_volume(f3d_ens *ens, int member, double *mass);
+int f3d_ens_synchronize(f3d_ens *ens);
+int f3d_ens_get_stream(f3d_ens *ens, void **stream);
+int f3d_ens_launch_count(f3d_ens *ens, long long *count);
+/* Device error status: 1 after a bounded grid-barrier wait gave up. */
+int f3d_ens_status(f3d_ens *ens, int *device_error);
+
 /* ---- pinned host memory for fast transfers --------------------------------- */
 int f3d_host_alloc(size_t bytes, void **ptr);
 int f3d_host_free(void *ptr);

@@ -1,0 +1,165 @@
+"""Batched ensemble (f3d_ens_*) on the GPU against the CPU oracle.
+
+Every member of an FP64 ensemble must be bit-identical to the oracle run on
+that member alone with its perturbed winds (u, v times the member factor);
+the persistent fused step kernel must give the same bits as the per-phase
+kernels; the device clock must reproduce host-driven steps.
+"""
+import numpy as np
+import pytest
+
+from fall3d_b200 import workloads as W
+from fall3d_b200.ads import Domain
+from fall3d_b200.ensemble import MODE_KERNELS, MODE_PERSISTENT, Ensemble, autotune
+from fall3d_b200.source import dense_source
+from tests.helpers import acum_interior, interior, oracle_vs
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(20, 16, 10), (26, 14, 8), (12, 9, 6)]
+FACTORS = [1.0, 0.87, 1.13, 1.0, 1.19]
+CLASSES = [0, 0, 1, 2, 1]
+NB = 3
+
+
+def _classes(oracle_mod):
+    cls = []
+    for ci, (nx, ny, nz) in enumerate(SHAPES):
+        wl = W.small_case(nx, ny, nz, NB, seed=50 + ci)
+        wl.vs = oracle_vs(oracle_mod, wl)
+        cls.append(wl)
+    return cls
+
+
+def _build(cls, precision, mode=MODE_KERNELS, bpb=4):
+    ens = Ensemble([c.grid for c in cls], NB, CLASSES, FACTORS, 2, 2, precision)
+    for ci, wl in enumerate(cls):
+        ens.set_class_meteo(ci, wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3, wl.vs, wl.t_its, wl.t_ite)
+    for m, ci in enumerate(CLASSES):
+        wl = cls[ci]
+        ens.set_member_source(m, wl.src_ijk, wl.src_vals * (1.0 + 0.1 * m))
+        c0, a0 = W.random_state(wl, seed=70 + m)
+        ens.upload_member_state(m, c0, a0)
+    ens.set_tuning(mode, bpb, 0)
+    return ens
+
+
+def _oracle_member(oracle_mod, wl, f, m, dts, t0s, nsteps):
+    g = wl.grid
+    orc = oracle_mod.Oracle(g, NB, wl.limiter, wl.time_marching)
+    c, a = W.random_state(wl, seed=70 + m)
+    s = dense_source(g, wl.src_ijk, wl.src_vals * (1.0 + 0.1 * m), NB)
+    u12 = np.asfortranarray(f * wl.u12)
+    v12 = np.asfortranarray(f * wl.v12)
+    fl = np.zeros(6)
+    t = t0s[m]
+    for it in range(nsteps):
+        orc.time_step(dts[m], t, wl.t_its, wl.t_ite, it, c, a, s, u12, v12, wl.w12, wl.k1, wl.k2,
+                      wl.k3, wl.vs, fl)
+        t = t + dts[m]
+    return c, a, fl
+
+
+@pytest.mark.parametrize("mode", [MODE_KERNELS, MODE_PERSISTENT])
+def test_fp64_members_bitexact_to_oracle(oracle_mod, built_lib, mode):
+    cls = _classes(oracle_mod)
+    ens = _build(cls, 0, mode)
+    dts = np.array([5.0, 6.5, 4.25, 3.0, 7.0])
+    t0s = np.array([0.0, 100.0, 37.5, 1200.0, 10.0])
+    fl = np.zeros(6 * len(CLASSES))
+    times = t0s.copy()
+    for it in range(3):
+        ens.step(dts, times, it, fl)
+        times = times + dts
+    assert ens.status() == 0
+    for m, ci in enumerate(CLASSES):
+        c_o, a_o, f_o = _oracle_member(oracle_mod, cls[ci], FACTORS[m], m, dts, t0s, 3)
+        c_g, a_g = ens.download_member_state(m)
+        assert np.array_equal(interior(c_o), interior(c_g)), f"member {m}"
+        assert np.array_equal(acum_interior(a_o), acum_interior(a_g)), f"member {m}"
+        scale = max(np.abs(f_o).max(), 1e-300)
+        assert np.all(np.abs(fl[6 * m:6 * m + 6] - f_o) <= 1e-11 * scale), (m, f_o, fl[6 * m:6 * m + 6])
+    ens.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_persistent_equals_kernels_and_device_clock(oracle_mod, built_lib, precision):
+    cls = _classes(oracle_mod)
+    outs = []
+    for mode in (MODE_KERNELS, MODE_PERSISTENT):
+        for bpb in ((4, 1) if mode == MODE_KERNELS else (2,)):
+            ens = _build(cls, precision, mode, bpb)
+            dt = ens.compute_time_steps(0.5, 2, 0.9, 1e30)
+            ens.set_clock(np.zeros(len(CLASSES)), 0)
+            ens.run(4)
+            t, it = ens.get_clock()
+            assert it == 4 and np.allclose(t, 4 * dt, rtol=1e-15)
+            assert ens.status() == 0
+            outs.append([interior(ens.download_member_state(m)[0]) for m in range(len(CLASSES))])
+            outs[-1].append(ens.get_fluxes())
+            ens.close()
+    for o in outs[1:]:
+        for m in range(len(CLASSES)):
+            assert np.array_equal(outs[0][m], o[m]), m
+        assert np.allclose(outs[0][-1], o[-1], rtol=1e-12, atol=0)
+
+
+def test_device_clock_equals_host_steps(oracle_mod, built_lib):
+    cls = _classes(oracle_mod)
+    a = _build(cls, 0)
+    dt = a.compute_time_steps(0.5, 2, 0.9, 1e30)
+    a.set_clock(np.full(len(CLASSES), 30.0), 0)
+    a.run(3)
+    b = _build(cls, 0)
+    t = np.full(len(CLASSES), 30.0)
+    for it in range(3):
+        b.step(dt, t, it)
+        t = t + dt
+    for m in range(len(CLASSES)):
+        assert np.array_equal(interior(a.download_member_state(m)[0]),
+                              interior(b.download_member_state(m)[0]))
+    a.close()
+    b.close()
+
+
+def test_member_cfl_matches_single_domain(oracle_mod, built_lib):
+    cls = _classes(oracle_mod)
+    ens = _build(cls, 0)
+    dts = ens.compute_time_steps(0.5, 2, 0.9, 1e30)
+    for m, ci in enumerate(CLASSES):
+        wl = cls[ci]
+        dom = Domain(wl.grid, NB)
+        dom.set_meteo(np.asfortranarray(FACTORS[m] * wl.u12), np.asfortranarray(FACTORS[m] * wl.v12),
+                      wl.w12, wl.k1, wl.k2, wl.k3, wl.vs, wl.t_its, wl.t_ite)
+        assert dom.grid_get_time_step(0.5, 2, 0.9, 1e30)[1] == dts[m]
+        dom.close()
+    ens.close()
+
+
+def test_fp32_ensemble_error_vs_fp64(oracle_mod, built_lib):
+    cls = _classes(oracle_mod)
+    res = []
+    for prec in (0, 1):
+        ens = _build(cls, prec)
+        ens.compute_time_steps(0.5, 2, 0.9, 1e30)
+        ens.set_clock(np.zeros(len(CLASSES)), 0)
+        ens.run(5)
+        res.append([interior(ens.download_member_state(m)[0]) for m in range(len(CLASSES))])
+        ens.close()
+    for m in range(len(CLASSES)):
+        a, b = res[0][m], res[1][m]
+        assert np.linalg.norm(b - a) <= 1e-5 * np.linalg.norm(a), m
+
+
+def test_autotune_picks_a_working_shape(oracle_mod, built_lib, tmp_path, monkeypatch):
+    monkeypatch.setenv("F3D_AUTOTUNE_CACHE", str(tmp_path))
+    cls = _classes(oracle_mod)
+    ens = _build(cls, 1)
+    ens.compute_time_steps(0.5, 2, 0.9, 1e30)
+    ens.set_clock(np.zeros(len(CLASSES)), 0)
+    best = autotune(ens, "test-key", steps=2)
+    assert best["ms_per_step"] > 0 and len(best["all"]) >= 3
+    assert (tmp_path / "autotune.json").exists()
+    again = autotune(ens, "test-key")
+    assert again["tuning"] == best["tuning"]
+    ens.close()
