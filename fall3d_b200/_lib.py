@@ -15,6 +15,7 @@ LIB_PATH = os.environ.get("F3D_LIB_PATH") or os.path.join(HERE, "libfall3d_ads.s
 # Every function the header declares, with its ctypes signature.
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
+_fp = C.POINTER(C.c_float)
 _vp = C.c_void_p
 
 
@@ -56,6 +57,8 @@ SIGNATURES = {
                                 _vp],
     "f3d_vset_points": [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip],
     "f3d_ads_compute_vset": [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_double, _dp],
+    "f3d_ads_compute_vset_mlp": [_vp, _vp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_double, C.c_int,
+                                 C.POINTER(C.c_longlong), _dp],
     "f3d_ens_create": [C.c_int, C.POINTER(F3DDims), C.c_int, _vp, C.c_int, C.c_int, C.c_int,
                        C.c_int, C.POINTER(_vp)],
     "f3d_ens_destroy": [_vp],
@@ -63,6 +66,9 @@ SIGNATURES = {
     "f3d_ens_set_class_meteo": [_vp, C.c_int] + [_dp] * 7 + [C.c_double, C.c_double],
     "f3d_ens_compute_class_vset": [_vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
                                    C.c_double],
+    "f3d_ens_compute_class_vset_mlp": [_vp, C.c_int, _vp, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
+                                       C.c_double, C.c_int, C.POINTER(C.c_longlong)],
+    "f3d_ens_vset_ms": [_vp, C.POINTER(C.c_float)],
     "f3d_ens_set_member_source": [_vp, C.c_int, C.c_int, _ip, _dp],
     "f3d_ens_upload_member_state": [_vp, C.c_int, _dp, _dp],
     "f3d_ens_download_member_state": [_vp, C.c_int, _dp, _dp],
@@ -78,6 +84,17 @@ SIGNATURES = {
     "f3d_ens_get_stream": [_vp, C.POINTER(_vp)],
     "f3d_ens_launch_count": [_vp, C.POINTER(C.c_longlong)],
     "f3d_ens_status": [_vp, _ip],
+    "f3d_mlp_create": [C.c_int, _dp, C.c_double, C.c_ulonglong, C.c_int, C.POINTER(_vp)],
+    "f3d_mlp_destroy": [_vp],
+    "f3d_mlp_generate": [_vp, C.c_longlong, C.c_ulonglong, C.POINTER(C.c_longlong)],
+    "f3d_mlp_get_samples": [_vp, C.c_longlong, C.c_longlong, _dp, _fp],
+    "f3d_mlp_train": [_vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_ulonglong, _fp, _fp],
+    "f3d_mlp_gradient": [_vp, C.c_longlong, _fp, _fp, _fp, _fp],
+    "f3d_mlp_get_params": [_vp, _fp],
+    "f3d_mlp_set_params": [_vp, _fp],
+    "f3d_mlp_get_norm": [_vp, _dp],
+    "f3d_mlp_predict": [_vp, C.c_longlong, _dp, _dp, _dp, _dp, _dp, C.c_int, _dp, _ip],
+    "f3d_mlp_last_ms": [_vp, C.POINTER(C.c_float)],
     "f3d_host_alloc": [C.c_size_t, C.POINTER(_vp)],
     "f3d_host_free": [_vp],
 }

@@ -195,6 +195,24 @@ class Domain:
         check(rc, "f3d_ads_compute_vset")
         return vs
 
+    def phys_get_vset_mlp(self, surrogate, rhoc, tc, diam, rhop, psi, bin_cat, is_aggregate=None,
+                          vset_fac=1.0, refine=0, want_host=False):
+        """phys_get_vset with the learned surrogate in place of the drag-law
+        iteration (the iteration answers outside the surrogate's envelope).
+        Returns (vs or None, number of w-faces that took the iteration)."""
+        g = self.grid
+        vs = np.zeros((g.nx, g.ny, g.nz + 3, self.nbins), order="F") if want_host else None
+        cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
+        agg = None if is_aggregate is None else np.ascontiguousarray(is_aggregate, dtype=np.int32)
+        nfb = C.c_longlong(0)
+        rc = lib().f3d_ads_compute_vset_mlp(
+            self._h, surrogate.handle, _p(np.asfortranarray(rhoc, dtype=np.float64)),
+            _p(np.asfortranarray(tc, dtype=np.float64)), _p(np.ascontiguousarray(diam, np.float64)),
+            _p(np.ascontiguousarray(rhop, np.float64)), _p(np.ascontiguousarray(psi, np.float64)),
+            _ip(cat), _ip(agg), float(vset_fac), int(refine), C.byref(nfb), _p(vs))
+        check(rc, "f3d_ads_compute_vset_mlp")
+        return vs, nfb.value
+
 
 def grid_get_mass_boundaries(fluxes):
     g, l = C.c_double(), C.c_double()

@@ -23,7 +23,7 @@ SOURCES = [
     ("aux_fp64.cu", ["--fmad=false"]),
     ("ads_fp32.cu", []),
     ("ens.cu", []),
-    ("mlp.cu", []),
+    ("mlp.cu", ["--fmad=false"]),
     ("noalloc.cu", ["--fmad=false"]),
     ("f3d_capi.cu", ["-Xcompiler", "-ffp-contract=off"]),
 ]

@@ -37,6 +37,10 @@ void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* par
 void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc,
                        const double* tc, const double* bin_par, const int* bin_flags,
                        double vset_fac, int* nfail, cudaStream_t st);
+int mlp_vset_field(f3d_mlp* h, const MemberDev* dm, int mi, int nx, int ny, int nz, int nb,
+                   const double* drhoc, const double* dtc, const double* diam, const double* rhop,
+                   const double* psi, const int* bin_cat, const int* is_aggregate, double vset_fac,
+                   int refine, cudaStream_t st, long long* nfallback, int* nfail);
 void launch_face_kk(MemberDev* members, int mi, cudaStream_t st);
 void launch_fp32_fields(MemberDev* members, int mi, cudaStream_t st);
 void launch_set_steps(MemberDev* members, int n, const double* dt, const double* time, int iiter,
@@ -129,6 +133,8 @@ struct f3d_ens {
   int fused_grid = 0;
   long long launches = 0;
   std::vector<void*> work_allocs;  // rebuilt with the tuning
+  cudaEvent_t vev[2] = {nullptr, nullptr};  // around the last class vset kernel
+  float vset_ms = 0.0f;
 };
 
 namespace {
@@ -257,6 +263,8 @@ extern "C" int f3d_ens_destroy(f3d_ens* e) {
   for (void* p : e->work_allocs) cudaFree(p);
   for (void* p : e->allocs) cudaFree(p);
   if (e->h_pin) cudaFreeHost(e->h_pin);
+  for (auto& ev : e->vev)
+    if (ev) cudaEventDestroy(ev);
   if (e->st) cudaStreamDestroy(e->st);
   delete e;
   return 0;
@@ -513,26 +521,19 @@ extern "C" int f3d_ens_set_class_meteo(f3d_ens* e, int ci, const double* u, cons
   return class_derived_fields(e, ci);
 }
 
-extern "C" int f3d_ens_compute_class_vset(f3d_ens* e, int ci, int model, const double* rhoc,
-                                          const double* tc, const double* diam,
-                                          const double* rhop, const double* psi,
-                                          const int* bin_cat, const int* is_aggregate,
-                                          double vset_fac) {
-  if (!e || ci < 0 || ci >= e->ncls) return set_error_msg("f3d_ens_compute_class_vset: bad class");
-  if (!rhoc || !tc || !diam || !rhop || !psi || !bin_cat)
-    return set_error_msg("f3d_ens_compute_class_vset: null array");
-  if (model < 1 || model > 7) return set_error_msg("setling velocity model not found");
+// Stage a class's corner air density/temperature and bin table on the device.
+static int ens_stage_vset(f3d_ens* e, int ci, const double* rhoc, const double* tc, const double* diam,
+                          const double* rhop, const double* psi, const int* bin_cat, const int* is_aggregate,
+                          double** drho, double** dtc, double** dpar, int** dflags) {
   EnsClass& k = e->cls[ci];
-  if (k.rep < 0) return 0;
-  if (!k.grid_set) return set_error_msg("f3d_ens_compute_class_vset: grid not set");
   ECK(cudaSetDevice(e->device));
   const size_t ncor = (size_t)(k.nx + 1) * (k.ny + 1) * (k.nz + 1);
   if (2 * ncor + 4 * (size_t)e->nb > e->staging_elems + 4 * (size_t)e->nb)
     return set_error_msg("ensemble staging too small for corner fields");
-  double* drho = e->staging;
-  double* dtc = drho + ncor;
-  double* dpar = dtc + ncor;
-  int* dflags = reinterpret_cast<int*>(dpar + 3 * e->nb);
+  *drho = e->staging;
+  *dtc = *drho + ncor;
+  *dpar = *dtc + ncor;
+  *dflags = reinterpret_cast<int*>(*dpar + 3 * e->nb);
   std::vector<double> par(3 * e->nb);
   std::vector<int> fl(e->nb);
   for (int b = 0; b < e->nb; ++b) {
@@ -541,23 +542,90 @@ extern "C" int f3d_ens_compute_class_vset(f3d_ens* e, int ci, int model, const d
     par[3 * b + 2] = psi[b];
     fl[b] = bin_cat[b] | ((is_aggregate && is_aggregate[b]) ? (1 << 8) : 0);
   }
-  ECK(cudaMemcpyAsync(drho, rhoc, ncor * 8, cudaMemcpyHostToDevice, e->st));
-  ECK(cudaMemcpyAsync(dtc, tc, ncor * 8, cudaMemcpyHostToDevice, e->st));
-  ECK(cudaMemcpyAsync(dpar, par.data(), par.size() * 8, cudaMemcpyHostToDevice, e->st));
-  ECK(cudaMemcpyAsync(dflags, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(*drho, rhoc, ncor * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(*dtc, tc, ncor * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(*dpar, par.data(), par.size() * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(*dflags, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  if (!e->vev[0]) {
+    ECK(cudaEventCreate(&e->vev[0]));
+    ECK(cudaEventCreate(&e->vev[1]));
+  }
+  return 0;
+}
+
+static int ens_check_vset_args(f3d_ens* e, int ci, const double* rhoc, const double* tc, const double* diam,
+                               const double* rhop, const double* psi, const int* bin_cat) {
+  if (!e || ci < 0 || ci >= e->ncls) return set_error_msg("f3d_ens_compute_class_vset: bad class");
+  if (!rhoc || !tc || !diam || !rhop || !psi || !bin_cat)
+    return set_error_msg("f3d_ens_compute_class_vset: null array");
+  if (e->cls[ci].rep >= 0 && !e->cls[ci].grid_set)
+    return set_error_msg("f3d_ens_compute_class_vset: grid not set");
+  return 0;
+}
+
+extern "C" int f3d_ens_compute_class_vset(f3d_ens* e, int ci, int model, const double* rhoc,
+                                          const double* tc, const double* diam,
+                                          const double* rhop, const double* psi,
+                                          const int* bin_cat, const int* is_aggregate,
+                                          double vset_fac) {
+  if (ens_check_vset_args(e, ci, rhoc, tc, diam, rhop, psi, bin_cat)) return 1;
+  if (model < 1 || model > 7) return set_error_msg("setling velocity model not found");
+  EnsClass& k = e->cls[ci];
+  if (k.rep < 0) return 0;
+  double *drho, *dtc, *dpar;
+  int* dflags;
+  if (ens_stage_vset(e, ci, rhoc, tc, diam, rhop, psi, bin_cat, is_aggregate, &drho, &dtc, &dpar, &dflags))
+    return 1;
   ECK(cudaMemsetAsync(e->d_nfail, 0, 4, e->st));
+  ECK(cudaEventRecord(e->vev[0], e->st));
   launch_vset_field(e->dm, k.rep, model, drho, dtc, dpar, dflags, vset_fac, e->d_nfail, e->st);
-  e->launches += 1;
   ECKL();
+  ECK(cudaEventRecord(e->vev[1], e->st));
+  e->launches += 1;
   int nfail = 0;
   ECK(cudaMemcpyAsync(e->h_pin, e->d_nfail, 4, cudaMemcpyDeviceToHost, e->st));
   ECK(cudaStreamSynchronize(e->st));
   memcpy(&nfail, e->h_pin, 4);
+  cudaEventElapsedTime(&e->vset_ms, e->vev[0], e->vev[1]);
   if (class_derived_fields(e, ci)) return 1;
   if (nfail) {
     set_error_msg("no convergence in vset (%d points)", nfail);
     return 2;
   }
+  return 0;
+}
+
+extern "C" int f3d_ens_compute_class_vset_mlp(f3d_ens* e, int ci, f3d_mlp* h, const double* rhoc,
+                                              const double* tc, const double* diam,
+                                              const double* rhop, const double* psi,
+                                              const int* bin_cat, const int* is_aggregate,
+                                              double vset_fac, int refine, long long* nfallback) {
+  if (ens_check_vset_args(e, ci, rhoc, tc, diam, rhop, psi, bin_cat)) return 1;
+  if (!h) return set_error_msg("f3d_ens_compute_class_vset_mlp: null surrogate");
+  EnsClass& k = e->cls[ci];
+  if (k.rep < 0) return 0;
+  double *drho, *dtc, *dpar;
+  int* dflags;
+  if (ens_stage_vset(e, ci, rhoc, tc, diam, rhop, psi, bin_cat, is_aggregate, &drho, &dtc, &dpar, &dflags))
+    return 1;
+  int nfail = 0;
+  if (mlp_vset_field(h, e->dm, k.rep, k.nx, k.ny, k.nz, e->nb, drho, dtc, diam, rhop, psi, bin_cat,
+                     is_aggregate, vset_fac, refine, e->st, nfallback, &nfail))
+    return 1;
+  e->launches += 1;
+  f3d_mlp_last_ms(h, &e->vset_ms);  // the inference kernel alone
+  if (class_derived_fields(e, ci)) return 1;
+  if (nfail) {
+    set_error_msg("no convergence in vset (%d points)", nfail);
+    return 2;
+  }
+  return 0;
+}
+
+extern "C" int f3d_ens_vset_ms(f3d_ens* e, float* ms) {
+  if (!e || !ms) return set_error_msg("f3d_ens_vset_ms: bad arguments");
+  *ms = e->vset_ms;
   return 0;
 }
 

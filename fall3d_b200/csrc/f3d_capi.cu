@@ -36,6 +36,10 @@ void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* par
 void launch_vset_points(int model, int n, const double* diam, const double* rhop,
                         const double* psi, const double* rhoa, const double* visc, double* vset,
                         int* flags, int* iters, int* nfail, cudaStream_t st);
+int mlp_vset_field(f3d_mlp* h, const MemberDev* dm, int mi, int nx, int ny, int nz, int nb,
+                   const double* drhoc, const double* dtc, const double* diam, const double* rhop,
+                   const double* psi, const int* bin_cat, const int* is_aggregate, double vset_fac,
+                   int refine, cudaStream_t st, long long* nfallback, int* nfail);
 void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc,
                        const double* tc, const double* bin_par, const int* bin_flags,
                        double vset_fac, int* nfail, cudaStream_t st);
@@ -840,6 +844,61 @@ extern "C" int f3d_vset_points(int model, int n, const double* diam, const doubl
   return 0;
 }
 
+// Stage corner air density/temperature and the bin table on the device.
+static int stage_vset_inputs(f3d_ctx* c, const double* rhoc, const double* tc, const double* diam,
+                             const double* rhop, const double* psi, const int* bin_cat,
+                             const int* is_aggregate, double** drho, double** dt, double** dpar,
+                             int** dflags) {
+  const size_t ncor = (size_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+  size_t need = 2 * ncor + 3 * (size_t)c->nb + (size_t)c->nb;
+  if (need > c->rhoc_cap) {
+    if (c->d_rhoc_tc) cudaFree(c->d_rhoc_tc);
+    c->d_rhoc_tc = nullptr;
+    c->rhoc_cap = 0;
+    CK(cudaMalloc(&c->d_rhoc_tc, need * 8));
+    c->rhoc_cap = need;
+  }
+  *drho = c->d_rhoc_tc;
+  *dt = *drho + ncor;
+  *dpar = *dt + ncor;
+  *dflags = reinterpret_cast<int*>(*dpar + 3 * c->nb);
+  std::vector<double> par(3 * c->nb);
+  std::vector<int> fl(c->nb);
+  for (int b = 0; b < c->nb; ++b) {
+    par[3 * b] = diam[b];
+    par[3 * b + 1] = rhop[b];
+    par[3 * b + 2] = psi[b];
+    fl[b] = bin_cat[b] | ((is_aggregate && is_aggregate[b]) ? (1 << 8) : 0);
+  }
+  CK(cudaMemcpyAsync(*drho, rhoc, ncor * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(*dt, tc, ncor * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(*dpar, par.data(), par.size() * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(*dflags, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// After a new vs field: FP32 copies, optional download, non-convergence status.
+static int finish_vset(f3d_ctx* c, int nfail, double* vs_out) {
+  if (c->prec == F3D_PREC_FP32 && c->meteo_set) {
+    launch_fp32_fields(c->dm, 0, c->st);
+    CKL();
+  }
+  if (vs_out) {
+    size_t n = (size_t)c->nx * c->ny * (c->nz + 3) * c->nb;
+    if (n > c->staging_elems) return set_err("staging too small");
+    launch_conv(9, c->hm.vs, c->staging, c->nx, c->ny, c->nz, c->nb, c->st);
+    CKL();
+    CK(cudaMemcpyAsync(vs_out, c->staging, n * 8, cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  if (nfail) {
+    set_err("no convergence in vset (%d points)", nfail);
+    return 2;
+  }
+  return 0;
+}
+
 extern "C" int f3d_ads_compute_vset(f3d_ctx* c, int model, const double* rhoc, const double* tc,
                                     const double* diam, const double* rhop, const double* psi,
                                     const int* bin_cat, const int* is_aggregate, double vset_fac,
@@ -850,53 +909,39 @@ extern "C" int f3d_ads_compute_vset(f3d_ctx* c, int model, const double* rhoc, c
     return set_err("f3d_ads_compute_vset: null array");
   if (model < 1 || model > 7) return set_err("setling velocity model not found");
   CK(cudaSetDevice(c->device));
-  const size_t ncor = (size_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
-  size_t need = 2 * ncor + 3 * (size_t)c->nb + (size_t)c->nb;
-  if (need > c->rhoc_cap) {
-    if (c->d_rhoc_tc) cudaFree(c->d_rhoc_tc);
-    CK(cudaMalloc(&c->d_rhoc_tc, need * 8));
-    c->rhoc_cap = need;
-  }
-  double* drho = c->d_rhoc_tc;
-  double* dt = drho + ncor;
-  double* dpar = dt + ncor;
-  int* dflags = reinterpret_cast<int*>(dpar + 3 * c->nb);
-  std::vector<double> par(3 * c->nb);
-  std::vector<int> fl(c->nb);
-  for (int b = 0; b < c->nb; ++b) {
-    par[3 * b] = diam[b];
-    par[3 * b + 1] = rhop[b];
-    par[3 * b + 2] = psi[b];
-    fl[b] = bin_cat[b] | ((is_aggregate && is_aggregate[b]) ? (1 << 8) : 0);
-  }
-  CK(cudaMemcpyAsync(drho, rhoc, ncor * 8, cudaMemcpyHostToDevice, c->st));
-  CK(cudaMemcpyAsync(dt, tc, ncor * 8, cudaMemcpyHostToDevice, c->st));
-  CK(cudaMemcpyAsync(dpar, par.data(), par.size() * 8, cudaMemcpyHostToDevice, c->st));
-  CK(cudaMemcpyAsync(dflags, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, c->st));
+  double *drho, *dt, *dpar;
+  int* dflags;
+  if (stage_vset_inputs(c, rhoc, tc, diam, rhop, psi, bin_cat, is_aggregate, &drho, &dt, &dpar, &dflags))
+    return 1;
   CK(cudaMemsetAsync(c->d_nfail, 0, 4, c->st));
   launch_vset_field(c->dm, 0, model, drho, dt, dpar, dflags, vset_fac, c->d_nfail, c->st);
   CKL();
-  if (c->prec == F3D_PREC_FP32 && c->meteo_set) {
-    launch_fp32_fields(c->dm, 0, c->st);
-    CKL();
-  }
   int nfail = 0;
   CK(cudaMemcpyAsync(c->h_pin, c->d_nfail, 4, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   memcpy(&nfail, c->h_pin, 4);
-  if (vs_out) {
-    size_t n = (size_t)c->nx * c->ny * (c->nz + 3) * c->nb;
-    if (n > c->staging_elems) return set_err("staging too small");
-    launch_conv(9, c->hm.vs, c->staging, c->nx, c->ny, c->nz, c->nb, c->st);
-    CKL();
-    CK(cudaMemcpyAsync(vs_out, c->staging, n * 8, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-  }
-  if (nfail) {
-    set_err("no convergence in vset (%d points)", nfail);
-    return 2;
-  }
-  return 0;
+  return finish_vset(c, nfail, vs_out);
+}
+
+extern "C" int f3d_ads_compute_vset_mlp(f3d_ctx* c, f3d_mlp* h, const double* rhoc, const double* tc,
+                                        const double* diam, const double* rhop, const double* psi,
+                                        const int* bin_cat, const int* is_aggregate, double vset_fac,
+                                        int refine, long long* nfallback, double* vs_out) {
+  if (!c || !h) return set_err("f3d_ads_compute_vset_mlp: null handle");
+  if (!c->grid_set) return set_err("f3d_ads_compute_vset_mlp: grid not set");
+  if (!rhoc || !tc || !diam || !rhop || !psi || !bin_cat)
+    return set_err("f3d_ads_compute_vset_mlp: null array");
+  CK(cudaSetDevice(c->device));
+  double *drho, *dt, *dpar;
+  int* dflags;
+  if (stage_vset_inputs(c, rhoc, tc, diam, rhop, psi, bin_cat, is_aggregate, &drho, &dt, &dpar, &dflags))
+    return 1;
+  int nfail = 0;
+  if (mlp_vset_field(h, c->dm, 0, c->nx, c->ny, c->nz, c->nb, drho, dt, diam, rhop, psi, bin_cat,
+                     is_aggregate, vset_fac, refine, c->st, nfallback, &nfail))
+    return 1;
+  c->launches += 1;
+  return finish_vset(c, nfail, vs_out);
 }
 
 extern "C" int f3d_host_alloc(size_t bytes, void** ptr) {

@@ -94,6 +94,24 @@ class Ensemble:
             _p(np.ascontiguousarray(rhop, np.float64)), _p(np.ascontiguousarray(psi, np.float64)),
             _ip(cat), None, 1.0), "f3d_ens_compute_class_vset")
 
+    def compute_class_vset_mlp(self, ci, surrogate, rhoc, tc, diam, rhop, psi, bin_cat, refine=0):
+        """Class settling velocity with the learned surrogate; returns the
+        number of w-faces that took the iteration (outside the envelope)."""
+        cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
+        nfb = C.c_longlong(0)
+        check(lib().f3d_ens_compute_class_vset_mlp(
+            self._h, ci, surrogate.handle, _p(np.asfortranarray(rhoc, dtype=np.float64)),
+            _p(np.asfortranarray(tc, dtype=np.float64)), _p(np.ascontiguousarray(diam, np.float64)),
+            _p(np.ascontiguousarray(rhop, np.float64)), _p(np.ascontiguousarray(psi, np.float64)),
+            _ip(cat), None, 1.0, int(refine), C.byref(nfb)), "f3d_ens_compute_class_vset_mlp")
+        return nfb.value
+
+    def vset_ms(self) -> float:
+        """Device time of the last class settling-velocity kernel."""
+        ms = C.c_float(0.0)
+        check(lib().f3d_ens_vset_ms(self._h, C.byref(ms)), "f3d_ens_vset_ms")
+        return ms.value
+
     def set_member_source(self, m, ijk, vals):
         ijk = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
         vals = np.ascontiguousarray(vals, dtype=np.float64).reshape(-1, self.nbins)
@@ -234,9 +252,10 @@ def ensemble_workload(class_shapes=((200, 150, 40), (400, 300, 60), (600, 450, 8
 
 
 def build_ensemble(ew: EnsembleWorkload, precision=1, device=0, vset="iterative", vs_classes=None,
-                   limiter=2, time_marching=2):
+                   limiter=2, time_marching=2, surrogate=None, refine=0):
     """Create the device ensemble and load meteo, settling velocity, sources.
-    vset: "iterative" (phys_get_vset on the device), "given" (vs_classes)."""
+    vset: "iterative" (phys_get_vset on the device), "mlp" (the learned
+    surrogate, iteration outside its envelope) or "given" (vs_classes)."""
     ens = Ensemble([c.grid for c in ew.classes], ew.nbins, ew.member_class, ew.wind_factor,
                    limiter, time_marching, precision, device)
     for ci, wl in enumerate(ew.classes):
@@ -245,6 +264,9 @@ def build_ensemble(ew: EnsembleWorkload, precision=1, device=0, vset="iterative"
         if vs is None and vset == "iterative":
             ens.compute_class_vset(ci, wl.vset_model, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi,
                                    wl.bin_cat)
+        elif vs is None and vset == "mlp":
+            ens.compute_class_vset_mlp(ci, surrogate, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi,
+                                       wl.bin_cat, refine)
     for m, (ijk, vals) in enumerate(ew.src):
         ens.set_member_source(m, ijk, vals)
     return ens

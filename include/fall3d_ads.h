@@ -25,6 +25,7 @@ extern "C" {
 #endif
 
 typedef struct f3d_ctx f3d_ctx;
+typedef struct f3d_mlp f3d_mlp;
 
 /* Interior mass points of the domain (my_ipe-my_ips+1, ...) and bins. */
 typedef struct {
@@ -211,6 +212,20 @@ int f3d_ads_compute_vset(f3d_ctx *ctx, int model, const double *rhoc,
                          const int *bin_cat, const int *is_aggregate,
                          double vset_fac, double *vs_out);
 
+/* Same as f3d_ads_compute_vset, with the learned surrogate (see f3d_mlp_*)
+ * in place of the drag-law iteration; w-faces outside the surrogate's
+ * envelope (and every face of a bin outside it) take the iteration.
+ * refine = 1 adds one Steffensen correction (two drag-law evaluations) to the
+ * surrogate value.  nfallback (may be NULL) = faces that took the iteration.
+ * No reference counterpart: replaces the phys_get_vset_point call inside
+ * phys_get_vset (mod_Phys.F90:717-718). */
+int f3d_ads_compute_vset_mlp(f3d_ctx *ctx, f3d_mlp *mlp, const double *rhoc,
+                             const double *tc, const double *diam,
+                             const double *rhop, const double *psi,
+                             const int *bin_cat, const int *is_aggregate,
+                             double vset_fac, int refine, long long *nfallback,
+                             double *vs_out);
+
 /* ---- batched ensemble -------------------------------------------------------
  * Ensemble members of FALL3D run as independent jobs in separate MPI
  * communicators (mod_Parallel.F90:188-217, task_SetEns.F90).  Here every
@@ -250,6 +265,15 @@ int f3d_ens_compute_class_vset(f3d_ens *ens, int cls, int model,
                                const double *diam, const double *rhop,
                                const double *psi, const int *bin_cat,
                                const int *is_aggregate, double vset_fac);
+/* The same with the learned surrogate (see f3d_ads_compute_vset_mlp). */
+int f3d_ens_compute_class_vset_mlp(f3d_ens *ens, int cls, f3d_mlp *mlp,
+                                   const double *rhoc, const double *tc,
+                                   const double *diam, const double *rhop,
+                                   const double *psi, const int *bin_cat,
+                                   const int *is_aggregate, double vset_fac,
+                                   int refine, long long *nfallback);
+/* Device time (ms) of the last class settling-velocity kernel. */
+int f3d_ens_vset_ms(f3d_ens *ens, float *ms);
 int f3d_ens_set_member_source(f3d_ens *ens, int member, int n, const int *ijk,
                               const double *s);
 int f3d_ens_upload_member_state(f3d_ens *ens, int member, const double *my_c,
@@ -282,6 +306,57 @@ int f3d_ens_get_stream(f3d_ens *ens, void **stream);
 int f3d_ens_launch_count(f3d_ens *ens, long long *count);
 /* Device error status: 1 after a bounded grid-barrier wait gave up. */
 int f3d_ens_status(f3d_ens *ens, int *device_error);
+
+/* ---- learned settling velocity ----------------------------------------------
+ * A 5 -> 64 -> 64 -> 1 tanh network standing in for the fixed-point drag-law
+ * solve of phys_get_vset_point (mod_Phys.F90:757-954); no reference
+ * counterpart.  Inputs (diameter, particle density, sphericity, air density,
+ * air viscosity) enter as normalised log features; the output is the log
+ * ratio of the particle Reynolds number to its Stokes value.  Training data
+ * are generated and labelled on the device by the model's own iteration;
+ * training (forward, backward, Adam) runs in the library's own kernels;
+ * inference runs layer 2 on the tensor cores (tcgen05, split BF16 operands,
+ * FP32 accumulate).  Parameter vector (F3D_MLP_NPARAMS floats): W1[64][5],
+ * b1[64], W2[64][64], b2[64], W3[64], b3 (row-major, out x in). */
+#define F3D_MLP_NPARAMS 4609
+
+/* envelope[10] = {d_lo, d_hi, rhop_lo, rhop_hi, psi_lo, psi_hi, rhoa_lo,
+ * rhoa_hi, visc_lo, visc_hi} (SI units).  Training samples are drawn from the
+ * envelope widened by margin (diameter by exp(+-3 margin), the others by
+ * (1 -+ margin), sphericity capped at 1).  model: 1,2,3,5,6,7 (the iterative
+ * models of phys_get_vset_point).  seed: parameter initialisation. */
+int f3d_mlp_create(int model, const double *envelope, double margin,
+                   unsigned long long seed, int device, f3d_mlp **out);
+int f3d_mlp_destroy(f3d_mlp *mlp);
+/* nsamples uniform draws over the training box, labelled by the iteration;
+ * nfail (may be NULL) = draws whose iteration did not converge (unused). */
+int f3d_mlp_generate(f3d_mlp *mlp, long long nsamples, unsigned long long seed,
+                     long long *nfail);
+/* raw[5 n] = (d, rhop, psi, rhoa, visc) per sample; rec[8 n] = (5 features,
+ * target, 0, 0) per sample.  Either may be NULL. */
+int f3d_mlp_get_samples(f3d_mlp *mlp, long long first, long long n,
+                        double *raw, float *rec);
+/* Adam over steps minibatches of batch samples (a multiple of 128), cosine
+ * learning rate lr_max -> lr_min.  loss_hist[steps] and train_ms may be NULL. */
+int f3d_mlp_train(f3d_mlp *mlp, int steps, int batch, double lr_max,
+                  double lr_min, unsigned long long seed, float *loss_hist,
+                  float *train_ms);
+/* Gradient (F3D_MLP_NPARAMS) and value of the mean squared error over n
+ * given samples (features[5 n], targets[n]) at the current parameters. */
+int f3d_mlp_gradient(f3d_mlp *mlp, long long n, const float *features,
+                     const float *targets, float *grad, float *loss);
+int f3d_mlp_get_params(f3d_mlp *mlp, float *params);
+int f3d_mlp_set_params(f3d_mlp *mlp, const float *params);
+/* out[19]: lar_c, lar_sinv, sg_scale, psi_lo, psi_sinv, lnd_lo, lnd_sinv,
+ * lnmu_lo, lnmu_sinv, then the training box (lo, hi) per coordinate. */
+int f3d_mlp_get_norm(f3d_mlp *mlp, double *out);
+/* Settling velocity of n points; used[n] (may be NULL) = 1 where the
+ * surrogate answered, 0 where the point was outside the envelope. */
+int f3d_mlp_predict(f3d_mlp *mlp, long long n, const double *diam,
+                    const double *rhop, const double *psi, const double *rhoa,
+                    const double *visc, int refine, double *vset, int *used);
+/* Device time (ms) of the last inference kernel. */
+int f3d_mlp_last_ms(f3d_mlp *mlp, float *ms);
 
 /* ---- pinned host memory for fast transfers --------------------------------- */
 int f3d_host_alloc(size_t bytes, void **ptr);
