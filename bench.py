@@ -9,12 +9,15 @@ collective ("scaling": "weak"); torch.distributed only provides the barrier
 around the timed region and the max-over-ranks of the device time.
 
 Workloads (seeded synthetic inputs standing in for a meteo database):
+  ensemble  (default, the headline) the 64-member ensemble on uneven grids,
+            12 bins (fall3d_b200.ensemble): FP32 + batched ensemble + learned
+            settling velocity timed; the plain FP64 form (one domain per
+            member, iterative settling velocity) timed on the first member of
+            each grid class and weighted by the class member counts; errors
+            of those members against their FP64 runs after the same steps
   c2        400x300x60 grid, 20 bins, random-phase winds, log-normal K, two
             Suzuki sources (one domain per GPU), FP32 precision form timed,
             FP64 form timed on the same inputs for the ratio
-  ensemble  the 64-member ensemble on uneven grids, 12 bins (see
-            fall3d_b200.ensemble); FP32 + learned settling velocity timed,
-            plain FP64 timed on the same members
 """
 from __future__ import annotations
 
@@ -340,9 +343,8 @@ def column_vset(O, wl):
     return vs
 
 
-def run_reference(args, ws, rank):
-    """Reference arm: the CPU restatement of the reference path (the Fortran
-    reference cannot be built here) on the host cores, same metric/config."""
+def run_reference_c2(args, ws, rank):
+    """Reference arm on the single-domain c2 workload."""
     if rank != 0:
         return
     from fall3d_b200 import workloads as W
@@ -382,19 +384,379 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# The 64-member ensemble: FP32 + batched ensemble + learned settling velocity
+# against the plain FP64 form (one domain per member, iterative settling
+# velocity) on the same members.
+ENS_CONFIG = ("64 members on uneven grids: 16x(200x150x40) + 32x(400x300x60) + 16x(600x450x80), "
+              "12 bins (phi -2..6), winds x(1+-20%), source height +-2 km, mass rate x[0.5,2] "
+              "log-uniform")
+METEO_INTERVAL_S = 3600.0   # meteo coupling interval: settling velocity recomputed once per hour
+
+
+def class_reps(ew):
+    """First member (unperturbed winds) of every grid class."""
+    return [ew.member_class.index(c) for c in range(len(ew.classes))]
+
+
+def fp64_member_domain(ew, m, device):
+    """The plain FP64 form of member m: its own domain, iterative settling
+    velocity, the member's perturbed winds and source."""
+    from fall3d_b200.ads import PREC_FP64, Domain
+    wl = ew.classes[ew.member_class[m]]
+    f = ew.wind_factor[m]
+    dom = Domain(wl.grid, wl.nbins, wl.limiter, wl.time_marching, PREC_FP64, device=device)
+    dom.set_meteo(np.asfortranarray(f * wl.u12), np.asfortranarray(f * wl.v12), wl.w12, wl.k1, wl.k2,
+                  wl.k3, None, wl.t_its, wl.t_ite)
+    dom.phys_get_vset(wl.vset_model, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi, wl.bin_cat)
+    ijk, vals = ew.src[m]
+    dom.set_source(ijk, vals)
+    return dom
+
+
+def deposit_mass(g, acum):
+    area = g.dX1_p[2:-2][:, None] * (g.Hm1_p * g.dX2_p[2:-2])[None, :]
+    return float((acum[2:-2, 2:-2, :] * area[:, :, None]).sum())
+
+
+def run_ensemble(args, ws, rank, local, pg):
+    import torch
+    from fall3d_b200.ensemble import Ensemble, autotune, ensemble_workload
+    from fall3d_b200.mlp import trained_surrogate
+    torch.cuda.set_device(local)
+    K, Wu = args.steps, args.warmup
+    ew = ensemble_workload(seed=rank)
+    nm, nb = len(ew.member_class), ew.nbins
+    cbs = float(ew.cell_bins())
+    out = {"workload": ew}
+    # ---- learned settling velocity (trained once, outside the timed region)
+    t0 = time.perf_counter()
+    sur = trained_surrogate(device=local)
+    out["mlp_train_s"] = round(time.perf_counter() - t0, 2)
+    out["mlp_train_ms_device"] = round(sur.train_ms, 1)
+    # ---- FP32 batched ensemble; class settling velocity by the iteration
+    # (timed, for the plain arm) and then by the surrogate (kept)
+    ens = Ensemble([c.grid for c in ew.classes], nb, ew.member_class, ew.wind_factor, 2, 2, 1, local)
+    vinfo = {"iter_ms": [], "mlp_ms": [], "fallback_faces": [], "faces": []}
+    for ci, wl in enumerate(ew.classes):
+        ens.set_class_meteo(ci, wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3, None, wl.t_its, wl.t_ite)
+        for rep in range(2):  # second pass timed (warm)
+            ens.compute_class_vset(ci, wl.vset_model, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi, wl.bin_cat)
+            it_ms = ens.vset_ms()
+            nfb = ens.compute_class_vset_mlp(ci, sur, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi, wl.bin_cat, 1)
+            ml_ms = ens.vset_ms()
+        vinfo["iter_ms"].append(round(it_ms, 3))
+        vinfo["mlp_ms"].append(round(ml_ms, 3))
+        vinfo["fallback_faces"].append(int(nfb))
+        vinfo["faces"].append(int((wl.grid.nz + 1) * wl.grid.ny * wl.grid.nx * nb))
+    for m, (ijk, vals) in enumerate(ew.src):
+        ens.set_member_source(m, ijk, vals)
+    run_end = ew.classes[0].run_end
+    dts = ens.compute_time_steps(0.5, 2, 0.9, run_end)
+    reps = class_reps(ew)
+    steps_per_meteo = [max(1.0, METEO_INTERVAL_S / dts[m]) for m in reps]
+    # ---- autotune (tile shapes / mode), then a fresh start
+    key = f"ens64-{nb}-fp32-{torch.cuda.get_device_name(local)}"
+    tune = autotune(ens, key, steps=2)
+    out["tuning"] = {"mode": ["kernels+graphs", "persistent"][tune["tuning"][0]],
+                     "bins_per_block": tune["tuning"][1], "ctas_per_sm": tune["tuning"][2],
+                     "candidates": [{"tuning": r["tuning"], "ms_per_step": round(r.get("ms_per_step", -1), 3)}
+                                    for r in tune.get("all", [])]}
+    ens.reset_state()
+    ens.set_clock(np.zeros(nm), 0)
+    ens.run(Wu)
+    ens.synchronize()
+    s = torch.cuda.ExternalStream(ens.stream_ptr, device=torch.device("cuda", local))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    n0 = ens.launch_count()
+    with ClockSampler(local) as clk:
+        e0.record(s)
+        ens.run(K)
+        e1.record(s)
+        ens.synchronize()
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    ms_steps = max_over_ranks(pg, e0.elapsed_time(e1))
+    if ens.status() != 0:
+        raise RuntimeError("device barrier timeout in the timed region")
+    # settling velocity once per meteo interval, per class, amortised per step
+    vset_amort = sum(vinfo["mlp_ms"][c] / steps_per_meteo[c] for c in range(len(ew.classes)))
+    ms_tot = ms_steps + K * vset_amort
+    out.update(value=ws * cbs * K / (ms_tot / 1e3), ms_per_step=ms_tot / K,
+               steps_only_value=ws * cbs * K / (ms_steps / 1e3), launches=ens.launch_count() - n0,
+               clocks=clk.summary(), vset=vinfo, vset_amortised_ms_per_step=round(vset_amort, 4),
+               steps_per_meteo_interval=[round(x, 1) for x in steps_per_meteo])
+    # ---- plain FP64 arm: each class's first member as its own domain, the
+    # same W + K steps with the same dt; error of the FP32+MLP members
+    fp64_ms = []
+    errs = []
+    iter_amort = 0.0
+    for ci, m in enumerate(reps):
+        dom = fp64_member_domain(ew, m, local)
+        g = ew.classes[ci].grid
+        ms64, _, _ = time_steps(dom, float(dts[m]), K, Wu, local, pg)
+        fp64_ms.append(max_over_ranks(pg, ms64))
+        c64, a64 = dom.download_state()
+        mv64 = dom.grid_get_mass_volume()
+        dom.close()
+        c32, a32 = ens.download_member_state(m)
+        mv32 = ens.mass_volume(m)
+        i64, i32 = c64[2:-2, 2:-2, 2:-2, :], c32[2:-2, 2:-2, 2:-2, :]
+        d64, d32 = deposit_mass(g, a64), deposit_mass(g, a32)
+        errs.append({"member": m, "grid": f"{g.nx}x{g.ny}x{g.nz}",
+                     "conc_rel_l2": float(np.linalg.norm(i32 - i64) / np.linalg.norm(i64)),
+                     "conc_rel_l2_worst_bin": float(max(np.linalg.norm(i32[..., q] - i64[..., q]) /
+                                                        max(np.linalg.norm(i64[..., q]), 1e-300)
+                                                        for q in range(nb))),
+                     "deposit_rel": abs(d32 / d64 - 1.0) if d64 else 0.0,
+                     "mass_rel": abs((mv32 + d32) / (mv64 + d64) - 1.0)})
+        del c64, a64, c32, a32, i64, i32
+        n_c = ew.member_class.count(ci)
+        # every plain member job recomputes its own settling velocity by the iteration
+        iter_amort += sum(vinfo["iter_ms"][ci] / max(1.0, METEO_INTERVAL_S / dts[q])
+                          for q in range(nm) if ew.member_class[q] == ci)
+    fp64_step_ms = sum(ew.member_class.count(ci) * fp64_ms[ci] / K for ci in range(len(reps)))
+    fp64_tot = fp64_step_ms + iter_amort
+    out.update(fp64_value=ws * cbs / (fp64_tot / 1e3), fp64_ms_per_step=fp64_tot,
+               fp64_class_ms_per_step=[round(x / K, 3) for x in fp64_ms], errors=errs)
+    out["ens"], out["sur"], out["dts"], out["reps"] = ens, sur, dts, reps
+    out["steps_per_meteo"] = steps_per_meteo
+    return out
+
+
+def ens_roofline(r, K):
+    """Dominant kernel of the ensemble step, from event-timed profiled steps
+    in the tuned mode; algorithmic bytes: every member's concentration read
+    and written once per sweep, the class fields (shared by the members of a
+    class) once."""
+    ens, ew = r["ens"], r["workload"]
+    ens.set_profiling(True)
+    ens.run(3)
+    ens.synchronize()
+    ms, n = ens.get_profile()
+    ens.set_profiling(False)
+    per = ms / max(n, 1)
+    nb = ew.nbins
+
+    def bytes_dir(d):
+        tot = 0.0
+        for ci, wl in enumerate(ew.classes):
+            g = wl.grid
+            nmem = ew.member_class.count(ci)
+            cells = g.nx * g.ny * g.nz
+            tot += nmem * 2.0 * 4 * cells * nb                 # c read + write, FP32
+            tot += sweep_bytes(wl, 4, d) - 2.0 * 4 * cells * nb  # class fields once
+        return tot
+
+    peak, kind = hbm_peak()
+    if r["tuning"]["mode"] == "persistent":
+        byts = sum(bytes_dir(d) for d in "xyz")
+        t = per[1]
+        name = "k_fused32 (persistent step: x, y, z sweeps of all 64 members)"
+        tkey = "fused32"
+    else:
+        sw = {"x": per[1], "y": per[2], "z": per[3]}
+        dk = max(sw, key=sw.get)
+        byts = bytes_dir(dk)
+        t = sw[dk]
+        name = f"k_sweep32<{'xyz'.index(dk)},2,2> ({dk} sweep of all 64 members)"
+        tkey = f"sweep32_{dk}"
+    achieved = byts / (t / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": kind,
+            "traffic": load_traffic(tkey, "ensemble"), "algorithmic_bytes": byts,
+            "launch_ms": round(t, 3),
+            "phase_ms": {k: round(float(v), 3) for k, v in zip(("prep", "x", "y", "z", "flux"), per)}}
+
+
+def pinned_copy(a):
+    """A Fortran-ordered copy of a in page-locked host memory (f3d_host_alloc)."""
+    import ctypes as C
+    from fall3d_b200._lib import check, lib
+    p = C.c_void_p()
+    check(lib().f3d_host_alloc(max(a.nbytes, 1), C.byref(p)), "f3d_host_alloc")
+    buf = (C.c_char * a.nbytes).from_address(p.value)
+    arr = np.ndarray(a.shape, a.dtype, buffer=buf, order="F")
+    arr[...] = a
+    return arr, p
+
+
+def e2e_ensemble(r, K, pg, ws):
+    """The same metric through the public API with host buffers: every step is
+    f3d_ens_step with host dt/time arrays and the boundary fluxes of all
+    members read back; the meteo term (from pinned host memory) and the
+    surrogate settling velocity (corner air fields uploaded) are charged per
+    step at the meteo coupling interval of the most frequently updated class."""
+    from fall3d_b200._lib import lib
+    ens, ew, sur, dts = r["ens"], r["workload"], r["sur"], r["dts"]
+    nm = len(ew.member_class)
+    cbs = float(ew.cell_bins())
+    held = []
+    pin = []
+    for wl in ew.classes:
+        arrs = []
+        for a in (wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3, wl.rhoc, wl.tc):
+            x, h = pinned_copy(np.asfortranarray(a))
+            arrs.append(x)
+            held.append(h)
+        pin.append(arrs)
+    meteo_bytes = sum(x.nbytes for arrs in pin for x in arrs)
+    ens.reset_state()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for ci, wl in enumerate(ew.classes):
+        u, v, w, k1, k2, k3, rc, tc = pin[ci]
+        ens.set_class_meteo(ci, u, v, w, k1, k2, k3, None, wl.t_its, wl.t_ite)
+        ens.compute_class_vset_mlp(ci, sur, rc, tc, wl.diam, wl.rhop, wl.psi, wl.bin_cat, 1)
+    t1 = time.perf_counter()
+    fl = np.zeros(6 * nm)
+    times = np.zeros(nm)
+    for it in range(K):
+        ens.step(dts, times, it, fl)
+        times = times + dts
+    t2 = time.perf_counter()
+    for h in held:
+        lib().f3d_host_free(h)
+    spm = min(r["steps_per_meteo"])
+    t_tot = max_over_ranks(pg, (t2 - t1) + (t1 - t0) * K / spm)
+    return {"value": ws * cbs * K / t_tot, "unit": UNIT,
+            "h2d_bytes_per_step": int(meteo_bytes / spm + 16 * nm + 8),
+            "d2h_bytes_per_step": 48 * nm,
+            "meteo_and_vset_upload_s": round(t1 - t0, 3), "steps_per_meteo_interval": round(spm, 1)}
+
+
+def oracle_member_steps(O, ew, m, dt, steps, threads, warm=0):
+    """Seconds for `steps` FP64 oracle steps of member m (after `warm`)."""
+    from fall3d_b200.source import dense_source
+    wl = ew.classes[ew.member_class[m]]
+    g = wl.grid
+    orc = O.Oracle(g, wl.nbins, wl.limiter, wl.time_marching, threads=threads)
+    vs = column_vset(O, wl)
+    f = ew.wind_factor[m]
+    u12, v12 = np.asfortranarray(f * wl.u12), np.asfortranarray(f * wl.v12)
+    c = np.zeros((g.nx + 4, g.ny + 4, g.nz + 4, wl.nbins), order="F")
+    a = np.zeros((g.nx + 4, g.ny + 4, wl.nbins), order="F")
+    ijk, vals = ew.src[m]
+    src = dense_source(g, ijk, vals, wl.nbins)
+    fl = np.zeros(6)
+    t = 0.0
+    for it in range(warm):
+        orc.time_step(dt, t, wl.t_its, wl.t_ite, it, c, a, src, u12, v12, wl.w12, wl.k1, wl.k2, wl.k3, vs, fl)
+        t += dt
+    t0 = time.perf_counter()
+    for it in range(warm, warm + steps):
+        orc.time_step(dt, t, wl.t_its, wl.t_ite, it, c, a, src, u12, v12, wl.w12, wl.k1, wl.k2, wl.k3, vs, fl)
+        t += dt
+    return time.perf_counter() - t0
+
+
+def cpu_baseline_ensemble(ew, dts, steps=1, warm=0):
+    """The CPU FP64 oracle (restatement of the reference path), all host
+    threads, on a bounded sample: `steps` steps of the first member of each
+    grid class, weighted by the number of members of the class."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    reps = class_reps(ew)
+    secs = [oracle_member_steps(O, ew, m, float(dts[m]), steps, threads, warm) for m in reps]
+    tot = sum(ew.member_class.count(ci) * secs[ci] for ci in range(len(reps)))
+    return {"value": float(ew.cell_bins()) * steps / tot, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} step(s) of the first member of each grid class (200x150x40, 400x300x60, "
+                      f"600x450x80; 12 bins), FP64 oracle with OpenMP over pencils, weighted by the "
+                      f"class member counts (16, 32, 16)",
+            "class_seconds": [round(x, 3) for x in secs]}
+
+
+def run_reference_ensemble(args, ws, rank):
+    """Reference arm: the CPU restatement of the reference path (the Fortran
+    reference cannot be built here) on the host cores, on the same ensemble
+    workload and metric.  Each step = one time step of the first member of
+    each grid class, weighted by the class member counts."""
+    if rank != 0:
+        return
+    from fall3d_b200.ensemble import ensemble_workload
+    ew = ensemble_workload(seed=0)
+    dts = [6.0] * len(ew.member_class)
+    base = cpu_baseline_ensemble(ew, dts, steps=args.steps, warm=args.warmup)
+    v = base["value"]
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * float(ew.cell_bins()) / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "ensemble: " + ENS_CONFIG, "parallelism": "cpu-openmp"},
+            "cpu_baseline": dict(base, sample=base["sample"].replace("1 step(s)", f"{args.steps} step(s)")),
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def line_ensemble(args, ws, res):
+    ew = res["workload"]
+    e = res["errors"]
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "ensemble: " + ENS_CONFIG,
+                   "form": "FP32 state and stencils (FP64 deposit, flux sums, CFL), batched "
+                           "ensemble step, learned settling velocity (surrogate + one Steffensen "
+                           "correction; iteration outside the envelope), once per 1 h meteo interval",
+                   "parallelism": f"replicas x{ws} (one 64-member ensemble per GPU)",
+                   "l2": f"inputs larger than L2: member concentrations total "
+                         f"{ew.cell_bins() * 4 / 2**30:.1f} GiB vs {L2_BYTES / 2**20:.0f} MiB L2"},
+        "fp64_plain_value": res["fp64_value"],
+        "fp64_ms_per_step": res["fp64_ms_per_step"],
+        "speedup_vs_fp64_plain": res["value"] / res["fp64_value"],
+        "steps_only_value": res["steps_only_value"],
+        "gpu_launches": res["launches"],
+        "clocks": res["clocks"],
+        "roofline": res["roofline"],
+        "e2e": res["e2e"],
+        "errors_vs_fp64": {
+            "conc_rel_l2_max": max(x["conc_rel_l2"] for x in e),
+            "deposit_rel_max": max(x["deposit_rel"] for x in e),
+            "mass_rel_max": max(x["mass_rel"] for x in e),
+            "members": e},
+        "tuning": res["tuning"],
+        "vset": dict(res["vset"], amortised_ms_per_step=res["vset_amortised_ms_per_step"],
+                     steps_per_meteo_interval=res["steps_per_meteo_interval"],
+                     mlp_train_s=res["mlp_train_s"], mlp_train_ms_device=res["mlp_train_ms_device"]),
+        "fp64_class_ms_per_step": res["fp64_class_ms_per_step"],
+    }
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local, pg = dist_setup()
     if args.impl == "reference":
-        run_reference(args, ws, rank)
+        if args.workload == "ensemble":
+            run_reference_ensemble(args, ws, rank)
+        else:
+            run_reference_c2(args, ws, rank)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.workload == "ensemble":
+        res = run_ensemble(args, ws, rank, local, pg)
+        res["roofline"] = ens_roofline(res, args.steps)
+        res["e2e"] = e2e_ensemble(res, args.steps, pg, ws)
+        if rank == 0:
+            line = line_ensemble(args, ws, res)
+            if ws == 1 and not args.no_cpu_baseline:
+                line["cpu_baseline"] = cpu_baseline_ensemble(res["workload"], res["dts"])
+            print(json.dumps(line), flush=True)
+        res["ens"].close()
+        res["sur"].close()
         if pg is not None:
             pg.destroy_process_group()
         return

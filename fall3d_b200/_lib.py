@@ -80,6 +80,9 @@ SIGNATURES = {
     "f3d_ens_step": [_vp, _dp, _dp, C.c_int, _dp],
     "f3d_ens_get_fluxes": [_vp, _dp],
     "f3d_ens_mass_volume": [_vp, C.c_int, _dp],
+    "f3d_ens_reset_state": [_vp],
+    "f3d_ens_set_profiling": [_vp, C.c_int],
+    "f3d_ens_get_profile": [_vp, _dp, _ip],
     "f3d_ens_synchronize": [_vp],
     "f3d_ens_get_stream": [_vp, C.POINTER(_vp)],
     "f3d_ens_launch_count": [_vp, C.POINTER(C.c_longlong)],

@@ -135,6 +135,10 @@ struct f3d_ens {
   std::vector<void*> work_allocs;  // rebuilt with the tuning
   cudaEvent_t vev[2] = {nullptr, nullptr};  // around the last class vset kernel
   float vset_ms = 0.0f;
+  bool prof = false;                   // per-phase event timing (no graph)
+  cudaEvent_t pev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  double prof_ms[5] = {0, 0, 0, 0, 0};  // prep+source, x, y, z, flux+clock
+  int prof_steps = 0;
 };
 
 namespace {
@@ -264,6 +268,8 @@ extern "C" int f3d_ens_destroy(f3d_ens* e) {
   for (void* p : e->allocs) cudaFree(p);
   if (e->h_pin) cudaFreeHost(e->h_pin);
   for (auto& ev : e->vev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : e->pev)
     if (ev) cudaEventDestroy(ev);
   if (e->st) cudaStreamDestroy(e->st);
   delete e;
@@ -811,7 +817,12 @@ int fused_setup(f3d_ens* e, const void** func, int* smem) {
 }
 
 // Enqueue one step.  set_host: dt/time come from the host arrays.
-int enqueue_step(f3d_ens* e, bool xfirst, bool advance) {
+// One step on the stream.  ev (profiling only, never while capturing):
+// ev[0] before the step, ev[1] after prep/source, ev[2 + q] after the q-th
+// sweep of the step's order, ev[5] at the end; in the persistent mode the
+// whole step lies between ev[0] and ev[5].
+int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullptr) {
+  if (ev) ECK(cudaEventRecord(ev[0], e->st));
   if (e->mode == F3D_ENS_MODE_PERSISTENT) {
     const void* func;
     int smem;
@@ -833,6 +844,7 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance) {
     void* args[] = {&a};
     ECK(cudaLaunchCooperativeKernel(func, dim3(e->fused_grid), dim3(128), args, (size_t)smem, e->st));
     e->launches += 1;
+    if (ev) ECK(cudaEventRecord(ev[5], e->st));
     return 0;
   }
   if (e->prec == F3D_PREC_FP64) {
@@ -842,6 +854,7 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance) {
     launch_source32(e->dm, e->nm, e->st);
   }
   e->launches += (e->prec == F3D_PREC_FP64) ? 2 : 1;
+  if (ev) ECK(cudaEventRecord(ev[1], e->st));
   const int order[3] = {xfirst ? DIR_X : DIR_Y, xfirst ? DIR_Y : DIR_X, DIR_Z};
   for (int q = 0; q < 3; ++q) {
     const int d = order[q];
@@ -850,6 +863,7 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance) {
     else
       launch_sweep32(d, e->lim, e->tm, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
     e->launches += 1;
+    if (ev) ECK(cudaEventRecord(ev[2 + q], e->st));
   }
   launch_flux_reduce(e->dm, e->nm, 7, e->st);
   e->launches += 1;
@@ -858,6 +872,29 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance) {
     e->launches += 1;
   }
   ECKL();
+  if (ev) ECK(cudaEventRecord(ev[5], e->st));
+  return 0;
+}
+
+// Accumulate the phase times of a profiled step (waits for it).
+int accumulate_profile(f3d_ens* e, bool xfirst) {
+  ECK(cudaEventSynchronize(e->pev[5]));
+  float t;
+  if (e->mode == F3D_ENS_MODE_PERSISTENT) {
+    cudaEventElapsedTime(&t, e->pev[0], e->pev[5]);
+    e->prof_ms[1] += t;  // the fused step kernel
+  } else {
+    const int order[3] = {xfirst ? DIR_X : DIR_Y, xfirst ? DIR_Y : DIR_X, DIR_Z};
+    cudaEventElapsedTime(&t, e->pev[0], e->pev[1]);
+    e->prof_ms[0] += t;
+    for (int q = 0; q < 3; ++q) {
+      cudaEventElapsedTime(&t, e->pev[1 + q], e->pev[2 + q]);
+      e->prof_ms[1 + order[q]] += t;
+    }
+    cudaEventElapsedTime(&t, e->pev[4], e->pev[5]);
+    e->prof_ms[4] += t;
+  }
+  e->prof_steps += 1;
   return 0;
 }
 
@@ -897,6 +934,15 @@ extern "C" int f3d_ens_run(f3d_ens* e, int nsteps) {
   for (const EnsClass& k : e->cls)
     if (k.rep >= 0 && (!k.meteo_set || !k.grid_set)) return set_error_msg("f3d_ens_run: class not ready");
   ECK(cudaSetDevice(e->device));
+  if (e->prof) {
+    for (int s = 0; s < nsteps; ++s) {
+      const bool xfirst = (e->mode == F3D_ENS_MODE_PERSISTENT) || (e->iiter % 2 == 0);
+      if (enqueue_step(e, xfirst, true, e->pev)) return 1;
+      if (accumulate_profile(e, xfirst)) return 1;
+      e->iiter += 1;
+    }
+    return 0;
+  }
   if (!e->graph_ok && build_graphs(e)) return 1;
   for (int s = 0; s < nsteps; ++s) {
     cudaGraphExec_t g = (e->mode == F3D_ENS_MODE_PERSISTENT) ? e->graph[0] : e->graph[e->iiter & 1];
@@ -955,6 +1001,40 @@ extern "C" int f3d_ens_mass_volume(f3d_ens* e, int mi, double* mass) {
     tot = t;
   }
   *mass = tot + comp;
+  return 0;
+}
+
+extern "C" int f3d_ens_reset_state(f3d_ens* e) {
+  if (!e) return set_error_msg("f3d_ens_reset_state: null ensemble");
+  ECK(cudaSetDevice(e->device));
+  for (int m = 0; m < e->nm; ++m) {
+    const MemberDev& d = e->hm[m];
+    const size_t ncell = (size_t)d.nx * d.ny * d.nz, nb = (size_t)e->nb;
+    if (d.c32) ECK(cudaMemsetAsync(d.c32, 0, ncell * nb * 4, e->st));
+    if (d.c64) ECK(cudaMemsetAsync(d.c64, 0, ncell * nb * 8, e->st));
+    ECK(cudaMemsetAsync(d.acum, 0, (size_t)d.nx * d.ny * nb * 8, e->st));
+  }
+  ECK(cudaMemsetAsync(e->flux_tot, 0, 12 * (size_t)e->nm * 8, e->st));
+  ECK(cudaMemsetAsync(e->flux_step, 0, 6 * (size_t)e->nm * 8, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+extern "C" int f3d_ens_set_profiling(f3d_ens* e, int on) {
+  if (!e) return set_error_msg("f3d_ens_set_profiling: null ensemble");
+  ECK(cudaSetDevice(e->device));
+  if (on && !e->pev[0])
+    for (auto& ev : e->pev) ECK(cudaEventCreate(&ev));
+  e->prof = on != 0;
+  for (double& x : e->prof_ms) x = 0.0;
+  e->prof_steps = 0;
+  return 0;
+}
+
+extern "C" int f3d_ens_get_profile(f3d_ens* e, double* ms, int* nsteps) {
+  if (!e || !ms) return set_error_msg("f3d_ens_get_profile: null argument");
+  for (int q = 0; q < 5; ++q) ms[q] = e->prof_ms[q];
+  if (nsteps) *nsteps = e->prof_steps;
   return 0;
 }
 

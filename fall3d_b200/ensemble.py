@@ -170,6 +170,21 @@ class Ensemble:
         check(lib().f3d_ens_mass_volume(self._h, m, C.byref(x)), "f3d_ens_mass_volume")
         return x.value
 
+    def reset_state(self):
+        """Zero every member's concentration, deposit and flux totals."""
+        check(lib().f3d_ens_reset_state(self._h), "f3d_ens_reset_state")
+
+    def set_profiling(self, on=True):
+        check(lib().f3d_ens_set_profiling(self._h, int(bool(on))), "f3d_ens_set_profiling")
+
+    def get_profile(self):
+        """Accumulated ms {prep, x, y, z, flux} and the number of profiled steps."""
+        ms = np.zeros(5)
+        n = C.c_int(0)
+        check(lib().f3d_ens_get_profile(self._h, ms.ctypes.data_as(_dp), C.byref(n)),
+              "f3d_ens_get_profile")
+        return ms, n.value
+
     def synchronize(self):
         check(lib().f3d_ens_synchronize(self._h), "f3d_ens_synchronize")
 

@@ -301,6 +301,16 @@ int f3d_ens_step(f3d_ens *ens, const double *dt, const double *time, int iiter,
 /* Adds the device-accumulated flux totals to fluxes[6*nmembers], zeroes them. */
 int f3d_ens_get_fluxes(f3d_ens *ens, double *fluxes);
 int f3d_ens_mass_volume(f3d_ens *ens, int member, double *mass);
+/* Zero every member's concentration, deposit and flux totals on the device
+ * (a fresh start without host transfers; the clocks are left to
+ * f3d_ens_set_clock). */
+int f3d_ens_reset_state(f3d_ens *ens);
+/* Per-phase device timing: while on, f3d_ens_run enqueues steps without the
+ * graph and records events between phases; ms[5] accumulates
+ * {prep+source, x sweep, y sweep, z sweep, flux+clock} (persistent mode: the
+ * fused step kernel in ms[1]) over nsteps steps.  Turning it on resets. */
+int f3d_ens_set_profiling(f3d_ens *ens, int on);
+int f3d_ens_get_profile(f3d_ens *ens, double *ms, int *nsteps);
 int f3d_ens_synchronize(f3d_ens *ens);
 int f3d_ens_get_stream(f3d_ens *ens, void **stream);
 int f3d_ens_launch_count(f3d_ens *ens, long long *count);

@@ -163,3 +163,31 @@ def test_autotune_picks_a_working_shape(oracle_mod, built_lib, tmp_path, monkeyp
     again = autotune(ens, "test-key")
     assert again["tuning"] == best["tuning"]
     ens.close()
+
+
+@pytest.mark.parametrize("mode", [MODE_KERNELS, MODE_PERSISTENT])
+def test_reset_and_profiled_steps_equal_graph_steps(oracle_mod, built_lib, mode):
+    """After f3d_ens_reset_state the members restart from zero; steps run
+    with per-phase profiling (no graph) give the graph's bits."""
+    cls = _classes(oracle_mod)
+    outs = []
+    for profiled in (False, True):
+        ens = _build(cls, 0, mode)
+        dt = ens.compute_time_steps(0.5, 2, 0.9, 1e30)
+        ens.set_clock(np.zeros(len(CLASSES)), 0)
+        ens.run(2)
+        ens.reset_state()
+        c0, a0 = ens.download_member_state(1)
+        assert not c0.any() and not a0.any()
+        ens.set_clock(np.zeros(len(CLASSES)), 0)
+        ens.set_profiling(profiled)
+        ens.run(3)
+        ens.synchronize()
+        if profiled:
+            ms, n = ens.get_profile()
+            assert n == 3 and ms[1] > 0 and (mode == MODE_PERSISTENT or (ms[2] > 0 and ms[3] > 0))
+        assert ens.status() == 0
+        outs.append([interior(ens.download_member_state(m)[0]) for m in range(len(CLASSES))])
+        ens.close()
+    for m in range(len(CLASSES)):
+        assert np.array_equal(outs[0][m], outs[1][m]), m
