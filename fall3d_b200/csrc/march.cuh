@@ -25,10 +25,27 @@ struct FaceV {
   T k;  // diffusion at the face (FP64: 0.5 (k_f + k_f-1); FP32: that / dxp)
 };
 
+// Asynchronous global -> shared copy of one element (cp.async, Ampere and
+// later): no register round trip, so the warp keeps computing while the copy
+// is in flight.  src_bytes < sizeof(T) zero-fills the destination.
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* dst_smem, const T* src, int src_bytes) {
+  const unsigned int d = (unsigned int)__cvta_generic_to_shared(dst_smem);
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Per-warp shared-memory staging of x pencils.  The 32 lanes of a warp own
 // 32 rows of the x-contiguous concentration; lanes read their own row from a
 // transposed tile while the warp moves whole 128-byte row segments between
-// HBM and the tile (coalesced), double-buffered in both directions.
+// HBM and the tile (coalesced), double-buffered in both directions.  Input
+// chunks are copied with cp.async a chunk ahead and waited for only by the
+// first block that reads them, so their latency overlaps W - 8 positions of
+// work.
 template <class T>
 struct XTile {
   static constexpr int W = 128 / (int)sizeof(T);  // positions per chunk
@@ -38,6 +55,7 @@ struct XTile {
   T* in;            // [2][32][LDW]
   T* out;           // [2][32][LDW]
   T* const* rows;   // [32] row base pointers, null for lanes without a pencil
+  const T* any;     // a valid row of the warp (source address of zero-filled copies)
   int lane, n, next_flush;
 
   __device__ __forceinline__ void setup(void* base, T* my_row, int lane_, int n_) {
@@ -49,19 +67,26 @@ struct XTile {
     lane = lane_;
     n = n_;
     next_flush = 0;
+    const unsigned int have = __ballot_sync(0xffffffffu, my_row != nullptr);
+    any = have ? reinterpret_cast<const T*>(__shfl_sync(
+                     0xffffffffu, reinterpret_cast<unsigned long long>(my_row), __ffs(have) - 1))
+               : nullptr;
     __syncwarp();
   }
+  // issue the copies of chunk m (one commit group); rows without a pencil and
+  // positions past the end are zero-filled
   __device__ __forceinline__ void load_chunk(int m) {
+    if (!any) return;
     const int p0 = m * W, sub = lane / W, col = lane % W;
     T* dst = in + (m & 1) * 32 * LDW;
 #pragma unroll 8
     for (int r0 = 0; r0 < 32; r0 += RPI) {
       const int r = r0 + sub, p = p0 + col;
       const T* rp = rows[r];
-      T v = T(0);
-      if (rp && p < n) v = rp[p];
-      dst[r * LDW + col] = v;
+      const bool ok = rp && p < n;
+      cp_async_elem(dst + r * LDW + col, ok ? rp + p : any, ok ? (int)sizeof(T) : 0);
     }
+    cp_async_commit();
   }
   __device__ __forceinline__ void flush_chunk(int m) {
     const int p0 = m * W, sub = lane / W, col = lane % W;
@@ -82,10 +107,17 @@ struct XTile {
   // hooks driven by the march (warp-uniform)
   __device__ __forceinline__ void init() {
     load_chunk(0);
+    cp_async_wait_all();
     __syncwarp();
   }
   __device__ __forceinline__ void block_begin(int T0) {
+    // Block T0 reads positions T0+2 .. T0+9 (the march loads c(t+2) at time
+    // t).  At T0 = mW every lane is past chunk m-1, so chunk m+1 is copied
+    // into its buffer; chunk m+1 is first read by block T0 = (m+1)W - 8,
+    // which waits for the copies.
+    __syncwarp();
     if (T0 >= 0 && T0 % W == 0 && (T0 / W + 1) * W < n) load_chunk(T0 / W + 1);
+    if (T0 + 8 >= W && (T0 + 8) % W == 0) cp_async_wait_all();
     __syncwarp();
   }
   __device__ __forceinline__ void block_end(int T0) {
@@ -98,6 +130,7 @@ struct XTile {
     }
   }
   __device__ __forceinline__ void finish() {
+    cp_async_wait_all();
     __syncwarp();
     for (int m = next_flush; m * W < n; ++m) flush_chunk(m);
   }
