@@ -79,6 +79,7 @@ struct Ops32 {
     if (DIR == DIR_Z) r.u = w - __ldg(vsub + f * vs);
     else r.u = wfac * w;
     r.k = __ldg(kf + f * vs);
+    r.r = (f >= 1) ? __ldg(rdxb + (f - 1)) : 0.f;
     return r;
   }
   __device__ __forceinline__ float ghost_l(float c0, float uL) const { return (uL > 0.f) ? -c0 : c0; }
@@ -104,7 +105,7 @@ struct Ops32 {
       const float Pd = fv.k * s.d1;
       flux = F + Pd;
       const float G0 = Pd - F;
-      if (!G || q >= 2) rhs = (G0 - s.F1) * __ldg(rdxb + p);
+      if (!G || q >= 2) rhs = (G0 - s.F1) * fv.r;  // fv is face q-1: r = 1/dxb(q-2)
       s.F1 = G0;
     }
     s.a2 = s.a1;
@@ -222,7 +223,7 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
 }
 
 template <int DIR, int LIM, int TM>
-__global__ void __launch_bounds__(128) k_sweep32(const MemberDev* __restrict__ members,
+__global__ void __launch_bounds__(128, 4) k_sweep32(const MemberDev* __restrict__ members,
                                                  const WorkItem* __restrict__ work, int bpb) {
   extern __shared__ __align__(16) unsigned char f3d_smem[];
   sweep32_item<DIR, LIM, TM>(members, work[blockIdx.x], bpb, f3d_smem);

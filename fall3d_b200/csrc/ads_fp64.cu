@@ -67,6 +67,7 @@ struct Ops64 {
     r.u = vel[f * vs];
     if (DIR == DIR_Z) r.u = r.u - vsub[f * vs];  // CB%w - my_vs  (mod_ADS.F90:670)
     r.k = kk[f * vs];
+    r.r = 0.0;  // the exact form reads its metrics from geo
     return r;
   }
   // free flow (mod_ADS.F90:1227-1326) with bvalue = 0

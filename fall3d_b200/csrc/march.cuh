@@ -23,6 +23,8 @@ template <class T>
 struct FaceV {
   T u;  // face-normal velocity (z: w - vs of the bin)
   T k;  // diffusion at the face (FP64: 0.5 (k_f + k_f-1); FP32: that / dxp)
+  T r;  // FP32 form: 1/dxb of cell f-1, so that the face ring carries it to
+        // every stage (stage s at q receives face q-1 and needs cell q-2)
 };
 
 // Asynchronous global -> shared copy of one element (cp.async, Ampere and
@@ -165,7 +167,8 @@ struct March {
   T nh[8];           // new_c(p) at nh[p & 7]
   FaceV<T> fw[8];    // face(f) at fw[f & 7]
   StageS<T> S1, S2, S3, S4;
-  T gL, gR, uR, cn1, cn2;
+  T gL, gR, uR, cn1, cn2, cn3, cn4;
+  FaceV<T> fq;       // face(t+1), loaded one step ahead
   T flux_lo, flux_hi;
 
   __device__ __forceinline__ March(Ops& ops, int n_) : o(ops), n(n_) {}
@@ -176,19 +179,28 @@ struct March {
                   m5 = (U + 3) & 7, m6 = (U + 2) & 7, m7 = (U + 1) & 7;
     T k1 = T(0), k2 = T(0), k3 = T(0), k4 = T(0), ff = T(0);
     // ---- stage 1: arrival at q = t
+    // c(p) is loaded at t = p - 4 and face(f) at t = f - 1 (a four-slot and
+    // a one-slot queue in front of the rings), so their latency is hidden
+    // behind the work of the intervening positions.
     if (!G || (t >= -2 && t <= n + 1)) {
       T a;
       if (G) {
         a = (t < 0) ? gL : ((t < n) ? cn1 : gR);
         cn1 = cn2;
-        if (t + 2 >= 0 && t + 2 < n) cn2 = o.load_c(t + 2);
+        cn2 = cn3;
+        cn3 = cn4;
+        if (t + 4 >= 0 && t + 4 < n) cn4 = o.load_c(t + 4);
         if (t == n - 1) gR = o.ghost_r(a, uR);
-        if (t >= 0 && t <= n) fw[U] = o.face(t);
+        if (t >= 0 && t <= n) fw[U] = fq;
+        if (t + 1 >= 0 && t + 1 <= n) fq = o.face(t + 1);
       } else {
         a = cn1;
         cn1 = cn2;
-        cn2 = o.load_c(min(t + 2, n - 1));
-        fw[U] = o.face(t);
+        cn2 = cn3;
+        cn3 = cn4;
+        cn4 = o.load_c(min(t + 4, n - 1));
+        fw[U] = fq;
+        fq = o.face(t + 1);
       }
       ch[U] = a;
       o.template arrive<G>(S1, t, a, fw[m1], t - 2, k1, ff);
@@ -267,7 +279,10 @@ struct March {
     gL = o.ghost_l(c0, uL);
     gR = T(0);
     cn1 = T(0);
-    cn2 = c0;  // position 0 arrives at t = 0 through the two-slot queue
+    cn2 = T(0);
+    cn3 = c0;  // positions 0 and 1 arrive at t = 0, 1 through the four-slot queue
+    cn4 = (n > 1) ? o.load_c(1) : T(0);
+    fq = o.face(0);
     flux_lo = flux_hi = T(0);
     S1 = StageS<T>{T(0), T(0), T(0), T(0), T(0), T(0)};
     S2 = S1;
@@ -277,8 +292,8 @@ struct March {
     // blocks of 8 starting at t = -8 (ring index = t & 7); positions before
     // -2 are skipped inside the guarded body.
     int T0 = -8;
-    // the queue must hold c(t+1) when t >= -1: prime it for t = -2
-    // (cn2 = c0 is consumed as cn1 at t = -1 -> a at t = 0)
+    // the queue is primed for t = -2: c0 and c1 shift down to be consumed
+    // at t = 0 and 1, the loads at t = -2, -1 bring c2 and c3
 #pragma unroll 1
     for (; T0 <= t_last; T0 += 8) {
       // steady blocks end by n-2: t = n-1 captures the right ghost value
