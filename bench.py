@@ -166,13 +166,24 @@ def sweep_bytes(wl, prec_bytes: int, d: str) -> float:
     return c_rw + face * (nz + 1) * nx * ny + prec_bytes * (nz + 1) * nx * ny * nb
 
 
-def load_traffic(kernel: str, workload: str):
+def load_traffic(kernel: str, workload: str, algorithmic: float = None):
+    """DRAM bytes per launch from an ncu capture (profiles/traffic.json).
+    Workloads too large to capture use the measured/algorithmic ratio of
+    the same kernel on the 400x300x60x20 case, scaled to their algorithmic
+    bytes."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
         e = d.get(workload, {}).get(kernel)
-        return float(e) if e is not None else None
+        if e is not None:
+            return float(e)
+        ratio = d.get("ratio_measured_to_algorithmic", {})
+        if algorithmic is not None and kernel in ratio:
+            return float(ratio[kernel]) * algorithmic
+        if algorithmic is not None and kernel == "fused32" and ratio:
+            return float(sum(ratio.values()) / len(ratio)) * algorithmic
+        return None
     except Exception:
         return None
 
@@ -566,7 +577,9 @@ def ens_roofline(r, K):
     achieved = byts / (t / 1e3) / 1e9
     return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": kind,
-            "traffic": load_traffic(tkey, "ensemble"), "algorithmic_bytes": byts,
+            "traffic": load_traffic(tkey, "ensemble", byts), "algorithmic_bytes": byts,
+            "traffic_source": "ncu DRAM bytes of the same kernel on the 400x300x60x20 case, "
+                              "as a ratio to its algorithmic bytes, times this launch's algorithmic bytes",
             "launch_ms": round(t, 3),
             "phase_ms": {k: round(float(v), 3) for k, v in zip(("prep", "x", "y", "z", "flux"), per)}}
 
@@ -654,8 +667,9 @@ def oracle_member_steps(O, ew, m, dt, steps, threads, warm=0):
 
 def cpu_baseline_ensemble(ew, dts, steps=1, warm=0):
     """The CPU FP64 oracle (restatement of the reference path), all host
-    threads, on a bounded sample: `steps` steps of the first member of each
-    grid class, weighted by the number of members of the class."""
+    threads, on a bounded sample: `steps` steps (after `warm` untimed ones)
+    of the first member of each grid class, weighted by the number of
+    members of the class."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     reps = class_reps(ew)
@@ -753,7 +767,7 @@ def main():
         if rank == 0:
             line = line_ensemble(args, ws, res)
             if ws == 1 and not args.no_cpu_baseline:
-                line["cpu_baseline"] = cpu_baseline_ensemble(res["workload"], res["dts"])
+                line["cpu_baseline"] = cpu_baseline_ensemble(res["workload"], res["dts"], steps=1, warm=1)
             print(json.dumps(line), flush=True)
         res["ens"].close()
         res["sur"].close()

@@ -30,11 +30,13 @@ __device__ __forceinline__ float half_phid(float d1, float d0) {
     pd = (d0 > 0.f) ? fmaxf(0.f, lo) : fminf(0.f, hi);
     if (fabsf(d0) < kEpsF) pd = d0;
   } else if (LIM == 2) {  // superbee, mod_ADS.F90:1170-1183
-    float t1 = 2.f * d1, t2 = 2.f * d0;
-    float pos = fmaxf(fmaxf(0.f, fminf(t1, d0)), fminf(d1, t2));
-    float neg = fminf(fminf(0.f, fmaxf(t1, d0)), fmaxf(d1, t2));
-    pd = (d0 > 0.f) ? pos : neg;
-    if (fabsf(d0) < kEpsF) pd = (fabsf(d1) < kEpsF) ? 0.f : t2;
+    // phi(r) d0 = sign(d0) max(min(2|d1|, |d0|), min(|d1|, 2|d0|)) when d1
+    // has the sign of d0, else 0: the same values as the two-sided form
+    const float a = fabsf(d0), b = fabsf(d1);
+    const float m = fmaxf(fminf(2.f * b, a), fminf(b, 2.f * a));
+    const float sd1 = (d0 > 0.f) ? d1 : -d1;
+    pd = (sd1 > 0.f) ? copysignf(m, d0) : 0.f;
+    if (a < kEpsF) pd = (b < kEpsF) ? 0.f : 2.f * d0;
   } else {  // ospre, mod_ADS.F90:1206-1219: 1.5 (r^2+r)/(r^2+r+1) * d0
     float num = d1 * (d1 + d0);
     float den = fmaf(d1, d1 + d0, d0 * d0);
