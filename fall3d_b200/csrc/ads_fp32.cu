@@ -49,7 +49,7 @@ __device__ __forceinline__ float half_phid(float d1, float d0) {
 // Per-pencil operations of the precision form.  The current wind is
 // interpolated in time on the fly from the two meteo snapshots and scaled by
 // the member's wind factor (ensemble perturbation of u, v).
-template <int LIM, int DIR>
+template <int LIM, int DIR, int TM>
 struct Ops32 {
   float* cp;
   long long cs;
@@ -61,7 +61,7 @@ struct Ops32 {
   const float* rdxb;
   float s0, s1, wfac;
   float dt, hdt, dt3, dt6;
-  XTile<float> xt;  // x pencils: shared-memory staging of the rows
+  XTile<float, (TM == 2) ? 1 : 2> xt;  // x pencils: shared-memory staging of the rows
 
   __device__ __forceinline__ float load_c(int p) const {
     if constexpr (DIR == DIR_X) return xt.load(p);
@@ -103,7 +103,8 @@ struct Ops32 {
       const float u = fv.u;
       const float cl = s.a2 + s.h2;
       const float cr = s.a1 - h1;
-      const float F = 0.5f * fmaf(-fabsf(u), cr - cl, u * (cl + cr));
+      // 0.5 u (cl + cr) - 0.5 |u| (cr - cl) in upwind form: u+ cl + u- cr
+      const float F = fmaf(fmaxf(u, 0.f), cl, fminf(u, 0.f) * cr);
       const float Pd = fv.k * s.d1;
       flux = F + Pd;
       const float G0 = Pd - F;
@@ -154,7 +155,7 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
   const long long pen = pen_raw < nsp ? pen_raw : nsp - 1;
   double clo = 0.0, chi = 0.0;
   if (run_it) {
-    Ops32<LIM, DIR> o;
+    Ops32<LIM, DIR, TM> o;
     double area;
     int n, i = 0, j = 0;
     if (DIR == DIR_X) {
@@ -162,7 +163,7 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       int k = (int)(pen / ny);
       n = nx;
       o.cp = m.c32 + (((long long)b * nz + k) * ny + j) * nx;
-      o.xt.setup(f3d_smem + warp * XTile<float>::BYTES, lane_ok ? o.cp : nullptr,
+      o.xt.setup(f3d_smem + warp * decltype(o.xt)::BYTES, lane_ok ? o.cp : nullptr,
                  threadIdx.x & 31, nx);
       o.cs = 1;
       long long fo = (long long)k * (nx + 1) * ny + j;
@@ -210,7 +211,7 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
     o.hdt = 0.5f * o.dt;
     o.dt3 = o.dt * (1.f / 3.f);
     o.dt6 = o.dt * (1.f / 6.f);
-    March<float, Ops32<LIM, DIR>, TM> M(o, n);
+    March<float, Ops32<LIM, DIR, TM>, TM> M(o, n);
     M.run();
     if (lane_ok) {
       clo = (double)M.flux_lo * area * dt;
@@ -225,6 +226,8 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
 }
 
 template <int DIR, int LIM, int TM>
+// 4 blocks of 128 threads per SM (128 registers); with one output buffer the
+// RK4 x tiles (4 x 12.6 KB per block) fit 4 blocks as well.
 __global__ void __launch_bounds__(128, 4) k_sweep32(const MemberDev* __restrict__ members,
                                                  const WorkItem* __restrict__ work, int bpb) {
   extern __shared__ __align__(16) unsigned char f3d_smem[];
@@ -235,15 +238,17 @@ template <int DIR>
 static void launch_dir32(int lim, int tm, const MemberDev* members, const WorkItem* work,
                          int nblocks, int bpb, cudaStream_t st) {
   dim3 g(nblocks), b(128);
-  const int smem = (DIR == DIR_X) ? 4 * XTile<float>::BYTES : 0;
+  // RK4 x tiles keep one output buffer (XTile<float, 1>), Euler two
+  const int smem_max = (DIR == DIR_X) ? 4 * XTile<float, 2>::BYTES : 0;
+  const int smem = (DIR == DIR_X) ? 4 * ((tm == 2) ? XTile<float, 1>::BYTES : XTile<float, 2>::BYTES) : 0;
   static bool attr_set = false;
-  if (!attr_set && smem > 0) {
-    cudaFuncSetAttribute(k_sweep32<DIR, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep32<DIR, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep32<DIR, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep32<DIR, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep32<DIR, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep32<DIR, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (!attr_set && smem_max > 0) {
+    cudaFuncSetAttribute(k_sweep32<DIR, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     attr_set = true;
   }
 #define F3D_L(L, T) k_sweep32<DIR, L, T><<<g, b, smem, st>>>(members, work, bpb)
@@ -408,7 +413,7 @@ __global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
   }
 }
 
-int fused32_smem() { return 4 * XTile<float>::BYTES; }
+int fused32_smem() { return 4 * XTile<float, 2>::BYTES; }
 
 const void* fused32_func(int lim, int tm) {
   if (tm == 1) {

@@ -44,18 +44,22 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Per-warp shared-memory staging of x pencils.  The 32 lanes of a warp own
 // 32 rows of the x-contiguous concentration; lanes read their own row from a
 // transposed tile while the warp moves whole 128-byte row segments between
-// HBM and the tile (coalesced), double-buffered in both directions.  Input
-// chunks are copied with cp.async a chunk ahead and waited for only by the
-// first block that reads them, so their latency overlaps W - 8 positions of
-// work.
-template <class T>
+// HBM and the tile (coalesced).  Input chunks are double-buffered, copied
+// with cp.async a chunk ahead and waited for only by the first block that
+// reads them, so their latency overlaps W - 8 positions of work.  Output
+// chunks are double-buffered (NOUT = 2, any time marching) or, for RK4, held
+// in one buffer (NOUT = 1): RK4 writes position p at t = p + 8, so chunk m
+// is complete at t = (m+1)W + 7 and chunk m+1's first write comes at
+// t = (m+1)W + 8, the block that flushes chunk m before writing.  The
+// smaller tile lets more blocks share an SM.
+template <class T, int NOUT = 2>
 struct XTile {
   static constexpr int W = 128 / (int)sizeof(T);  // positions per chunk
   static constexpr int LDW = W + 1;               // padded row pitch
   static constexpr int RPI = 32 / W;              // rows per warp instruction
-  static constexpr int BYTES = 4 * 32 * LDW * (int)sizeof(T) + 32 * 8;
+  static constexpr int BYTES = (2 + NOUT) * 32 * LDW * (int)sizeof(T) + 32 * 8;
   T* in;            // [2][32][LDW]
-  T* out;           // [2][32][LDW]
+  T* out;           // [NOUT][32][LDW]
   T* const* rows;   // [32] row base pointers, null for lanes without a pencil
   const T* any;     // a valid row of the warp (source address of zero-filled copies)
   int lane, n, next_flush;
@@ -63,7 +67,7 @@ struct XTile {
   __device__ __forceinline__ void setup(void* base, T* my_row, int lane_, int n_) {
     in = reinterpret_cast<T*>(base);
     out = in + 2 * 32 * LDW;
-    T** r = reinterpret_cast<T**>(out + 2 * 32 * LDW);
+    T** r = reinterpret_cast<T**>(out + NOUT * 32 * LDW);
     r[lane_] = my_row;
     rows = r;
     lane = lane_;
@@ -92,7 +96,7 @@ struct XTile {
   }
   __device__ __forceinline__ void flush_chunk(int m) {
     const int p0 = m * W, sub = lane / W, col = lane % W;
-    const T* src = out + (m & 1) * 32 * LDW;
+    const T* src = out + (NOUT == 2 ? (m & 1) : 0) * 32 * LDW;
 #pragma unroll 8
     for (int r0 = 0; r0 < 32; r0 += RPI) {
       const int r = r0 + sub, p = p0 + col;
@@ -104,7 +108,7 @@ struct XTile {
     return in[((p / W) & 1) * 32 * LDW + lane * LDW + (p % W)];
   }
   __device__ __forceinline__ void store(int p, T v) const {
-    out[((p / W) & 1) * 32 * LDW + lane * LDW + (p % W)] = v;
+    out[(NOUT == 2 ? ((p / W) & 1) : 0) * 32 * LDW + lane * LDW + (p % W)] = v;
   }
   // hooks driven by the march (warp-uniform)
   __device__ __forceinline__ void init() {
@@ -118,6 +122,13 @@ struct XTile {
     // into its buffer; chunk m+1 is first read by block T0 = (m+1)W - 8,
     // which waits for the copies.
     __syncwarp();
+    if (NOUT == 1 && T0 - 8 >= W && (T0 - 8) % W == 0) {
+      // single output buffer: chunk (T0-8)/W - 1 is complete, flush it
+      // before this block writes the next chunk over it
+      flush_chunk((T0 - 8) / W - 1);
+      next_flush = (T0 - 8) / W;
+      __syncwarp();
+    }
     if (T0 >= 0 && T0 % W == 0 && (T0 / W + 1) * W < n) load_chunk(T0 / W + 1);
     if (T0 + 8 >= W && (T0 + 8) % W == 0) cp_async_wait_all();
     __syncwarp();
@@ -125,7 +136,7 @@ struct XTile {
   __device__ __forceinline__ void block_end(int T0) {
     // chunk m is complete after block (m+1)W and its buffer is rewritten from
     // block (m+2)W on (RK4 writes position p at t = p+8, Euler at t = p+2)
-    if (T0 >= W && T0 % W == 0) {
+    if (NOUT == 2 && T0 >= W && T0 % W == 0) {
       __syncwarp();
       flush_chunk(T0 / W - 1);
       next_flush = T0 / W;
