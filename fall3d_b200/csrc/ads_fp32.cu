@@ -30,13 +30,14 @@ __device__ __forceinline__ float half_phid(float d1, float d0) {
     pd = (d0 > 0.f) ? fmaxf(0.f, lo) : fminf(0.f, hi);
     if (fabsf(d0) < kEpsF) pd = d0;
   } else if (LIM == 2) {  // superbee, mod_ADS.F90:1170-1183
-    // phi(r) d0 = sign(d0) max(min(2|d1|, |d0|), min(|d1|, 2|d0|)) when d1
-    // has the sign of d0, else 0: the same values as the two-sided form
+    // 0.5 phi(r) d0 = sign(d0) max(min(|d1|, |d0|/2), min(|d1|/2, |d0|)) when
+    // d1 has the sign of d0, else 0 (the halving is exact, so these are the
+    // values of the two-sided form times 0.5)
     const float a = fabsf(d0), b = fabsf(d1);
-    const float m = fmaxf(fminf(2.f * b, a), fminf(b, 2.f * a));
-    const float sd1 = (d0 > 0.f) ? d1 : -d1;
-    pd = (sd1 > 0.f) ? copysignf(m, d0) : 0.f;
-    if (a < kEpsF) pd = (b < kEpsF) ? 0.f : 2.f * d0;
+    const float m = fmaxf(fminf(b, 0.5f * a), fminf(0.5f * b, a));
+    float h = (d0 * d1 > 0.f) ? copysignf(m, d0) : 0.f;
+    if (a < kEpsF) h = (b < kEpsF) ? 0.f : d0;
+    return h;
   } else {  // ospre, mod_ADS.F90:1206-1219: 1.5 (r^2+r)/(r^2+r+1) * d0
     float num = d1 * (d1 + d0);
     float den = fmaf(d1, d1 + d0, d0 * d0);
