@@ -33,6 +33,8 @@ SIGNATURES = {
     "f3d_last_error": [C.c_char_p, C.c_int],
     "f3d_ads_set_grid": [_vp] + [_dp] * 9,
     "f3d_ads_set_meteo": [_vp] + [_dp] * 7 + [C.c_double, C.c_double],
+    "f3d_ads_set_terrain": [_vp, C.c_int, C.c_double, _dp, _dp, _dp, _dp],
+    "f3d_ads_set_meteo_corners": [_vp] + [_dp] * 6 + [C.c_double] * 4,
     "f3d_ads_set_source": [_vp, C.c_int, _ip, _dp],
     "f3d_ads_set_source_dense": [_vp, _dp],
     "f3d_ads_upload_state": [_vp, _dp, _dp],

@@ -83,6 +83,32 @@ class Domain:
         check(lib().f3d_ads_set_meteo(self._h, _p(u12), _p(v12), _p(w12), _p(k1), _p(k2), _p(k3),
                                       _p(vs), float(t_its), float(t_ite)), "f3d_ads_set_meteo")
 
+    def set_terrain(self):
+        """Vertical mapping and terrain slopes of the grid, for
+        set_meteo_corners (Cartesian grids need nothing)."""
+        g = self.grid
+        if g.map_v == 0:
+            check(lib().f3d_ads_set_terrain(self._h, 0, 1.0, None, None, None, None), "f3d_ads_set_terrain")
+            return
+        arr = [np.ascontiguousarray(a, dtype=np.float64).ravel(order="F")
+               for a in (g.X3_c, g.X3_p, g.dhdx_p, g.dhdy_p)]
+        check(lib().f3d_ads_set_terrain(self._h, int(g.map_v), float(g.X3max),
+                                        *[a.ctypes.data_as(_dp) for a in arr]), "f3d_ads_set_terrain")
+
+    def set_meteo_corners(self, uc_pair, vc_pair, wc_pair, k1=None, k2=None, k3=None, kh=0.0, kv=0.0,
+                          t_its=0.0, t_ite=3600.0):
+        """F3D_update_meteo_term's compute part on the device: corner winds of
+        the two time levels and unscaled diffusion (k1 (nx+4,ny,nz),
+        k2 (nx,ny+4,nz), k3 (nx,ny,nz+4)) or constants kh, kv."""
+        def pair(p):
+            return np.asfortranarray(np.stack([np.asarray(p[0], np.float64), np.asarray(p[1], np.float64)],
+                                              axis=3))
+        uc, vc, wc = pair(uc_pair), pair(vc_pair), pair(wc_pair)
+        ks = [None if a is None else np.asfortranarray(a, dtype=np.float64) for a in (k1, k2, k3)]
+        check(lib().f3d_ads_set_meteo_corners(self._h, _p(uc), _p(vc), _p(wc), *[_p(a) for a in ks],
+                                              float(kh), float(kv), float(t_its), float(t_ite)),
+              "f3d_ads_set_meteo_corners")
+
     def set_source(self, ijk, vals):
         ijk = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
         vals = np.ascontiguousarray(vals, dtype=np.float64).reshape(-1, self.nbins)

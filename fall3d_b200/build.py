@@ -25,6 +25,7 @@ SOURCES = [
     ("ens.cu", []),
     ("mlp.cu", ["--fmad=false"]),
     ("noalloc.cu", ["--fmad=false"]),
+    ("meteo_dev.cu", ["--fmad=false"]),
     ("f3d_capi.cu", ["-Xcompiler", "-ffp-contract=off"]),
 ]
 

@@ -36,6 +36,23 @@ void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* par
 void launch_vset_points(int model, int n, const double* diam, const double* rhop,
                         const double* psi, const double* rhoa, const double* visc, double* vset,
                         int* flags, int* iters, int* nfail, cudaStream_t st);
+struct MetGeo {
+  int nx, ny, nz, map_v;
+  double X3max;
+  const double* X3c;
+  const double* X3p;
+  const double* dhdx;
+  const double* dhdy;
+  const double* hm1;
+  const double* hm2;
+  const double* hm3;
+};
+void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, const double* wc,
+                          const double* k1, const double* k2, const double* k3, double* ux,
+                          double* vy, double* wz, double* k1x, double* k2y, double* k3z,
+                          cudaStream_t st);
+void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
+                         double* k3, cudaStream_t st);
 int mlp_vset_field(f3d_mlp* h, const MemberDev* dm, int mi, int nx, int ny, int nz, int nb,
                    const double* drhoc, const double* dtc, const double* diam, const double* rhop,
                    const double* psi, const int* bin_cat, const int* is_aggregate, double vset_fac,
@@ -131,6 +148,12 @@ struct f3d_ctx {
   double prof_ms[6] = {0, 0, 0, 0, 0, 0};
   int prof_steps = 0;
   long long launches = 0;  // kernels launched by this context
+  // terrain mapping for the on-device meteo term (Cartesian until set)
+  int map_v = 0;
+  double X3max = 1.0;
+  double* d_terrain = nullptr;  // X3_c (nz+1), X3_p (nz), dhdx_p, dhdy_p (nx*ny each)
+  double* d_met = nullptr;      // corner winds of two snapshots + unscaled diffusion
+  size_t met_cap = 0;
 };
 
 template <class T>
@@ -395,6 +418,99 @@ extern "C" int f3d_ads_set_meteo(f3d_ctx* c, const double* u, const double* v, c
       upload_conv(c, 5, k3, (nz + 4) * nx * ny, const_cast<double*>(m.k3z)))
     return 1;
   if (vs && upload_conv(c, 6, vs, nx * ny * (nz + 3) * nb, const_cast<double*>(m.vs))) return 1;
+  c->t_its = t_its;
+  c->t_ite = t_ite;
+  m.t_its = t_its;
+  m.t_ite = t_ite;
+  if (upload_member(c)) return 1;
+  if (c->prec == F3D_PREC_FP32) {
+    launch_fp32_fields(c->dm, 0, c->st);
+  } else {
+    launch_face_kk(c->dm, 0, c->st);
+  }
+  CKL();
+  CK(cudaStreamSynchronize(c->st));
+  c->meteo_set = true;
+  return 0;
+}
+
+extern "C" int f3d_ads_set_terrain(f3d_ctx* c, int map_v, double X3max, const double* X3_c,
+                                   const double* X3_p, const double* dhdx_p, const double* dhdy_p) {
+  if (!c) return set_err("f3d_ads_set_terrain: null context");
+  if (map_v < 0 || map_v > 2) return set_err("f3d_ads_set_terrain: mapping %d not implemented", map_v);
+  if (map_v != 0 && (!X3_c || !X3_p || !dhdx_p || !dhdy_p || !(X3max > 0.0)))
+    return set_err("f3d_ads_set_terrain: sigma mappings need X3max > 0, X3_c, X3_p and the slopes");
+  CK(cudaSetDevice(c->device));
+  const size_t nx = c->nx, ny = c->ny, nz = c->nz;
+  if (!c->d_terrain && dalloc(c, &c->d_terrain, (nz + 1) + nz + 2 * nx * ny)) return 1;
+  if (map_v != 0) {
+    CK(cudaMemcpy(c->d_terrain, X3_c, (nz + 1) * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_terrain + nz + 1, X3_p, nz * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_terrain + 2 * nz + 1, dhdx_p, nx * ny * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_terrain + 2 * nz + 1 + nx * ny, dhdy_p, nx * ny * 8, cudaMemcpyHostToDevice));
+  }
+  c->map_v = map_v;
+  c->X3max = map_v != 0 ? X3max : 1.0;
+  return 0;
+}
+
+extern "C" int f3d_ads_set_meteo_corners(f3d_ctx* c, const double* uc, const double* vc,
+                                         const double* wc, const double* k1, const double* k2,
+                                         const double* k3, double kh, double kv, double t_its,
+                                         double t_ite) {
+  if (!c) return set_err("f3d_ads_set_meteo_corners: null context");
+  if (!c->grid_set) return set_err("f3d_ads_set_meteo_corners: grid not set");
+  if (!uc || !vc || !wc) return set_err("f3d_ads_set_meteo_corners: null corner wind");
+  const bool kgiven = k1 || k2 || k3;
+  if (kgiven && !(k1 && k2 && k3)) return set_err("f3d_ads_set_meteo_corners: give all of k1, k2, k3 or none");
+  if (!(t_ite != t_its)) return set_err("f3d_ads_set_meteo_corners: t_ite == t_its");
+  CK(cudaSetDevice(c->device));
+  const size_t nx = c->nx, ny = c->ny, nz = c->nz;
+  const size_t ncor = (nx + 1) * (ny + 1) * (nz + 1);
+  const size_t n1 = (nx + 4) * ny * nz, n2 = nx * (ny + 4) * nz, n3 = nx * ny * (nz + 4);
+  const size_t need = 6 * ncor + n1 + n2 + n3;
+  if (need > c->met_cap) {
+    c->d_met = nullptr;  // the old buffer stays in the context's allocation list
+    if (dalloc(c, &c->d_met, need)) return 1;
+    c->met_cap = need;
+  }
+  double* duc = c->d_met;
+  double* dvc = duc + 2 * ncor;
+  double* dwc = dvc + 2 * ncor;
+  double* dk1 = dwc + 2 * ncor;
+  double* dk2 = dk1 + n1;
+  double* dk3 = dk2 + n2;
+  CK(cudaMemcpyAsync(duc, uc, 2 * ncor * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dvc, vc, 2 * ncor * 8, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dwc, wc, 2 * ncor * 8, cudaMemcpyHostToDevice, c->st));
+  if (kgiven) {
+    CK(cudaMemcpyAsync(dk1, k1, n1 * 8, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dk2, k2, n2 * 8, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dk3, k3, n3 * 8, cudaMemcpyHostToDevice, c->st));
+  } else {
+    launch_meteo_kconst(c->nx, c->ny, c->nz, kh, kv, dk1, dk2, dk3, c->st);
+    c->launches += 1;
+  }
+  MemberDev& m = c->hm;
+  MetGeo g;
+  g.nx = c->nx;
+  g.ny = c->ny;
+  g.nz = c->nz;
+  g.map_v = c->map_v;
+  g.X3max = c->X3max;
+  g.X3c = c->d_terrain;
+  g.X3p = c->d_terrain ? c->d_terrain + nz + 1 : nullptr;
+  g.dhdx = c->d_terrain ? c->d_terrain + 2 * nz + 1 : nullptr;
+  g.dhdy = c->d_terrain ? c->d_terrain + 2 * nz + 1 + nx * ny : nullptr;
+  g.hm1 = m.hm1;
+  g.hm2 = m.hm2;
+  g.hm3 = m.hm3;
+  launch_meteo_corners(g, duc, dvc, dwc, dk1, dk2, dk3, const_cast<double*>(m.ux[0]),
+                       const_cast<double*>(m.vy[0]), const_cast<double*>(m.wz[0]),
+                       const_cast<double*>(m.k1x), const_cast<double*>(m.k2y),
+                       const_cast<double*>(m.k3z), c->st);
+  c->launches += 9;
+  CKL();
   c->t_its = t_its;
   c->t_ite = t_ite;
   m.t_its = t_its;

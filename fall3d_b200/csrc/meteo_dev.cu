@@ -1,0 +1,197 @@
+// meteo_dev.cu -- the compute part of F3D_update_meteo_term
+// (mod_F3D.F90:673-944) on the device: from the meteo model's corner winds
+// of the two time levels of the interval and the diffusion coefficients at
+// mass points, the staggered, scaled fields of the ADS step, written straight
+// into the device layouts.
+//
+//   * ground corner winds are zero (mod_F3D.F90:676-683);
+//   * grid_get_stagered_velocity (mod_Grid.F90:685-752): 4-point corner
+//     averages at u, v and w faces;
+//   * grid_get_scaled_velocity (mod_Grid.F90:761-870): u / Hm1, v / Hm2 at
+//     v faces, and for the sigma mappings w = ((w - hx uw) - hy vw) / Hm3
+//     with the terrain slopes decayed linearly with height when asked;
+//   * the diffusion part of grid_get_scaled_variables (mod_Grid.F90:879-1017):
+//     k1 / Hm1^2, k2 / Hm2^2 and for sigma k3 = ((k3 + hx^2 k1) + hy^2 k2) / Hm3^2
+//     (with the unscaled k1, k2), vertical halos copied from the edge levels;
+//   * the transposes of mod_F3D.F90:931-944 become the output indexing.
+//
+// Compiled with --fmad=false: every sum and product is rounded separately in
+// the reference's order, so the fields equal those built on the host.
+#include <cuda_runtime.h>
+
+#include "f3d_common.cuh"
+
+namespace f3d {
+
+constexpr int kMapCartesian = 0, kMapSigmaLinearDecay = 2;  // 1: sigma, no decay
+
+struct MetGeo {
+  int nx, ny, nz, map_v;
+  double X3max;
+  const double* X3c;   // corner (w-face) heights above terrain, nz+1
+  const double* X3p;   // mass-point heights, nz
+  const double* dhdx;  // terrain slopes at mass points, nx*ny
+  const double* dhdy;
+  const double* hm1;   // ny
+  const double* hm2;   // ny+4 (jps-2 .. jpe+2)
+  const double* hm3;   // nx*ny
+};
+
+#define MGRID(e, total)                                                        \
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (total); \
+       e += (long long)gridDim.x * blockDim.x)
+
+// corner value, ground level (k = 0) forced to zero
+__device__ __forceinline__ double cw(const double* a, const MetGeo& g, int i, int j, int k) {
+  return (k == 0) ? 0.0 : a[i + (long long)(g.nx + 1) * (j + (long long)(g.ny + 1) * k)];
+}
+
+// ux[k][f=0..nx][j] of one snapshot
+__global__ void k_met_u(MetGeo g, const double* __restrict__ uc, double* __restrict__ ux) {
+  const long long tot = (long long)g.nz * (g.nx + 1) * g.ny;
+  MGRID(e, tot) {
+    const int j = (int)(e % g.ny);
+    long long t = e / g.ny;
+    const int f = (int)(t % (g.nx + 1));
+    const int k = (int)(t / (g.nx + 1));
+    const double u = 0.25 * (((cw(uc, g, f, j, k) + cw(uc, g, f, j + 1, k)) + cw(uc, g, f, j, k + 1)) +
+                             cw(uc, g, f, j + 1, k + 1));
+    ux[e] = u / g.hm1[j];
+  }
+}
+
+// vy[k][f=0..ny][i] of one snapshot; Hm2 at the face is the mean of the two
+// mass points beside it
+__global__ void k_met_v(MetGeo g, const double* __restrict__ vc, double* __restrict__ vy) {
+  const long long tot = (long long)g.nz * (g.ny + 1) * g.nx;
+  MGRID(e, tot) {
+    const int i = (int)(e % g.nx);
+    long long t = e / g.nx;
+    const int f = (int)(t % (g.ny + 1));
+    const int k = (int)(t / (g.ny + 1));
+    const double v = 0.25 * (((cw(vc, g, i, f, k) + cw(vc, g, i + 1, f, k)) + cw(vc, g, i, f, k + 1)) +
+                             cw(vc, g, i + 1, f, k + 1));
+    const double h = 0.5 * (g.hm2[f + 2] + g.hm2[f + 1]);
+    vy[e] = v / h;
+  }
+}
+
+// wz[f=0..nz][j][i] of one snapshot
+__global__ void k_met_w(MetGeo g, const double* __restrict__ uc, const double* __restrict__ vc,
+                        const double* __restrict__ wc, double* __restrict__ wz) {
+  const long long tot = (long long)(g.nz + 1) * g.ny * g.nx;
+  MGRID(e, tot) {
+    const int i = (int)(e % g.nx);
+    long long t = e / g.nx;
+    const int j = (int)(t % g.ny);
+    const int f = (int)(t / g.ny);
+    double w = 0.25 * (((cw(wc, g, i, j, f) + cw(wc, g, i + 1, j, f)) + cw(wc, g, i, j + 1, f)) +
+                       cw(wc, g, i + 1, j + 1, f));
+    if (g.map_v != kMapCartesian) {
+      const double uw = 0.25 * (((cw(uc, g, i, j, f) + cw(uc, g, i + 1, j, f)) + cw(uc, g, i, j + 1, f)) +
+                                cw(uc, g, i + 1, j + 1, f));
+      const double vw = 0.25 * (((cw(vc, g, i, j, f) + cw(vc, g, i + 1, j, f)) + cw(vc, g, i, j + 1, f)) +
+                                cw(vc, g, i + 1, j + 1, f));
+      const long long ij = i + (long long)g.nx * j;
+      double hx = g.dhdx[ij], hy = g.dhdy[ij];
+      if (g.map_v == kMapSigmaLinearDecay) {
+        const double hz = 1.0 - g.X3c[f] / g.X3max;
+        hx = hx * hz;
+        hy = hy * hz;
+      }
+      w = ((w - hx * uw) - hy * vw) / g.hm3[ij];
+    }
+    wz[e] = w;
+  }
+}
+
+// k1 (ips-2:ipe+2, jps:jpe, kps:kpe) unscaled -> k1x[k][p=-1..nx][j]
+__global__ void k_met_k1(MetGeo g, const double* __restrict__ k1, double* __restrict__ k1x) {
+  const long long tot = (long long)g.nz * (g.nx + 2) * g.ny;
+  MGRID(e, tot) {
+    const int j = (int)(e % g.ny);
+    long long t = e / g.ny;
+    const int p1 = (int)(t % (g.nx + 2));
+    const int k = (int)(t / (g.nx + 2));
+    k1x[e] = k1[(p1 + 1) + (long long)(g.nx + 4) * (j + (long long)g.ny * k)] / (g.hm1[j] * g.hm1[j]);
+  }
+}
+
+// k2 (ips:ipe, jps-2:jpe+2, kps:kpe), i fastest, unscaled -> k2y[k][p=-1..ny][i]
+__global__ void k_met_k2(MetGeo g, const double* __restrict__ k2, double* __restrict__ k2y) {
+  const long long tot = (long long)g.nz * (g.ny + 2) * g.nx;
+  MGRID(e, tot) {
+    const int i = (int)(e % g.nx);
+    long long t = e / g.nx;
+    const int p1 = (int)(t % (g.ny + 2));
+    const int k = (int)(t / (g.ny + 2));
+    const double h = g.hm2[p1 + 1];
+    k2y[e] = k2[i + (long long)g.nx * ((p1 + 1) + (long long)(g.ny + 4) * k)] / (h * h);
+  }
+}
+
+// k3 (ips:ipe, jps:jpe, kps-2:kpe+2), i fastest, unscaled -> k3z[p=-1..nz][j][i];
+// the halo levels take the scaled edge levels
+__global__ void k_met_k3(MetGeo g, const double* __restrict__ k1, const double* __restrict__ k2,
+                         const double* __restrict__ k3, double* __restrict__ k3z) {
+  const long long tot = (long long)(g.nz + 2) * g.ny * g.nx;
+  MGRID(e, tot) {
+    const int i = (int)(e % g.nx);
+    long long t = e / g.nx;
+    const int j = (int)(t % g.ny);
+    const int p = (int)(t / g.ny) - 1;
+    const int k = (p < 0) ? 0 : ((p >= g.nz) ? g.nz - 1 : p);  // level whose value fills p
+    const long long ij = i + (long long)g.nx * j;
+    double v = k3[i + (long long)g.nx * (j + (long long)g.ny * (k + 2))];
+    if (g.map_v != kMapCartesian) {
+      double hx = g.dhdx[ij], hy = g.dhdy[ij];
+      if (g.map_v == kMapSigmaLinearDecay) {
+        const double hz = 1.0 - g.X3p[k] / g.X3max;
+        hx = hx * hz;
+        hy = hy * hz;
+      }
+      const double a1 = k1[(i + 2) + (long long)(g.nx + 4) * (j + (long long)g.ny * k)];
+      const double a2 = k2[i + (long long)g.nx * ((j + 2) + (long long)(g.ny + 4) * k)];
+      v = ((v + hx * hx * a1) + hy * hy * a2) / (g.hm3[ij] * g.hm3[ij]);
+    }
+    k3z[e] = v;
+  }
+}
+
+// Constant diffusion (phys_get_kdiffu CONSTANT, mod_Phys.F90:477-480):
+// k1 = k2 = kh, k3 = kv at every mass point, written unscaled into the three
+// input layouts above.
+__global__ void k_met_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
+                             double* k3) {
+  const long long n1 = (long long)(nx + 4) * ny * nz, n2 = (long long)nx * (ny + 4) * nz,
+                  n3 = (long long)nx * ny * (nz + 4);
+  MGRID(e, n1 + n2 + n3) {
+    if (e < n1) k1[e] = kh;
+    else if (e < n1 + n2) k2[e - n1] = kh;
+    else k3[e - n1 - n2] = kv;
+  }
+}
+
+void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, const double* wc,
+                          const double* k1, const double* k2, const double* k3, double* ux,
+                          double* vy, double* wz, double* k1x, double* k2y, double* k3z,
+                          cudaStream_t st) {
+  const long long ncor = (long long)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+  const long long nu = (long long)g.nz * (g.nx + 1) * g.ny, nv = (long long)g.nz * (g.ny + 1) * g.nx,
+                  nw = (long long)(g.nz + 1) * g.ny * g.nx;
+  for (int s = 0; s < 2; ++s) {
+    k_met_u<<<592, 256, 0, st>>>(g, uc + s * ncor, ux + s * nu);
+    k_met_v<<<592, 256, 0, st>>>(g, vc + s * ncor, vy + s * nv);
+    k_met_w<<<592, 256, 0, st>>>(g, uc + s * ncor, vc + s * ncor, wc + s * ncor, wz + s * nw);
+  }
+  k_met_k1<<<592, 256, 0, st>>>(g, k1, k1x);
+  k_met_k2<<<592, 256, 0, st>>>(g, k2, k2y);
+  k_met_k3<<<592, 256, 0, st>>>(g, k1, k2, k3, k3z);
+}
+
+void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
+                         double* k3, cudaStream_t st) {
+  k_met_kconst<<<592, 256, 0, st>>>(nx, ny, nz, kh, kv, k1, k2, k3);
+}
+
+}  // namespace f3d

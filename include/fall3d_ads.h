@@ -84,6 +84,31 @@ int f3d_ads_set_meteo(f3d_ctx *ctx, const double *u, const double *v,
                       const double *k3, const double *vs, double t_its,
                       double t_ite);
 
+/* Vertical mapping of the terrain-following grid for f3d_ads_set_meteo_corners
+ * (MY_GRID%map_v, mod_Grid.F90:761-870, 879-1017): 0 Cartesian (default),
+ * 1 sigma without decay, 2 sigma with linear decay of the terrain slopes.
+ * X3_c(kbs:kbe) heights of the w levels, X3_p(kps:kpe) of the mass levels,
+ * dhdx_p, dhdy_p(ips:ipe,jps:jpe) terrain slopes; ignored for map_v = 0. */
+int f3d_ads_set_terrain(f3d_ctx *ctx, int map_v, double X3max,
+                        const double *X3_c, const double *X3_p,
+                        const double *dhdx_p, const double *dhdy_p);
+
+/* The compute part of F3D_update_meteo_term (mod_F3D.F90:673-944) on the
+ * device, in place of f3d_ads_set_meteo: from the corner winds of the two
+ * time levels of the interval, MY_MET%my_uc/my_vc/my_wc(ibs:ibe,jbs:jbe,
+ * kbs:kbe) at its and ite (two consecutive blocks each), and the unscaled
+ * diffusion at mass points k1(ips-2:ipe+2,jps:jpe,kps:kpe),
+ * k2(ips:ipe,jps-2:jpe+2,kps:kpe), k3(ips:ipe,jps:jpe,kps-2:kpe+2) -- or, with
+ * all three NULL, constants kh, kv (phys_get_kdiffu CONSTANT,
+ * mod_Phys.F90:477-480) -- builds the ground-zeroed, staggered
+ * (mod_Grid.F90:685-752), scaled (mod_Grid.F90:761-870, 879-1017) fields of
+ * the step directly in device memory.  The settling velocity stays with
+ * f3d_ads_compute_vset(_mlp). */
+int f3d_ads_set_meteo_corners(f3d_ctx *ctx, const double *uc, const double *vc,
+                              const double *wc, const double *k1,
+                              const double *k2, const double *k3, double kh,
+                              double kv, double t_its, double t_ite);
+
 /* Source term MY_TRA%my_s(ips:ipe,jps:jpe,kps:kpe,nbins) after
  * F3D_set_source_term (mod_F3D.F90:349-555), given sparsely: n cells with
  * 1-based Fortran indices ijk[3*q+0..2] and values s[nbins*q + bin] (the
