@@ -66,6 +66,8 @@ SIGNATURES = {
     "f3d_ens_destroy": [_vp],
     "f3d_ens_set_class_grid": [_vp, C.c_int] + [_dp] * 9,
     "f3d_ens_set_class_meteo": [_vp, C.c_int] + [_dp] * 7 + [C.c_double, C.c_double],
+    "f3d_ens_set_class_terrain": [_vp, C.c_int, C.c_int, C.c_double, _dp, _dp, _dp, _dp],
+    "f3d_ens_set_class_meteo_corners": [_vp, C.c_int] + [_dp] * 6 + [C.c_double] * 4,
     "f3d_ens_compute_class_vset": [_vp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
                                    C.c_double],
     "f3d_ens_compute_class_vset_mlp": [_vp, C.c_int, _vp, _dp, _dp, _dp, _dp, _dp, _ip, _ip,

@@ -41,6 +41,23 @@ int mlp_vset_field(f3d_mlp* h, const MemberDev* dm, int mi, int nx, int ny, int 
                    const double* drhoc, const double* dtc, const double* diam, const double* rhop,
                    const double* psi, const int* bin_cat, const int* is_aggregate, double vset_fac,
                    int refine, cudaStream_t st, long long* nfallback, int* nfail);
+struct MetGeo {
+  int nx, ny, nz, map_v;
+  double X3max;
+  const double* X3c;
+  const double* X3p;
+  const double* dhdx;
+  const double* dhdy;
+  const double* hm1;
+  const double* hm2;
+  const double* hm3;
+};
+void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, const double* wc,
+                          const double* k1, const double* k2, const double* k3, double* ux,
+                          double* vy, double* wz, double* k1x, double* k2y, double* k3z,
+                          cudaStream_t st);
+void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
+                         double* k3, cudaStream_t st);
 void launch_face_kk(MemberDev* members, int mi, cudaStream_t st);
 void launch_fp32_fields(MemberDev* members, int mi, cudaStream_t st);
 void launch_set_steps(MemberDev* members, int n, const double* dt, const double* time, int iiter,
@@ -96,6 +113,9 @@ struct EnsClass {
   std::vector<double> dX1_p, dX2_p, dX3_p, Hm1_p, Hm2_p, Hm3_p;
   double t_its = 0.0, t_ite = 1.0;
   bool grid_set = false, meteo_set = false;
+  int map_v = 0;                 // terrain mapping for the on-device meteo term
+  double X3max = 1.0;
+  double* terrain = nullptr;     // X3_c, X3_p, dhdx_p, dhdy_p
 };
 
 }  // namespace
@@ -135,6 +155,8 @@ struct f3d_ens {
   std::vector<void*> work_allocs;  // rebuilt with the tuning
   cudaEvent_t vev[2] = {nullptr, nullptr};  // around the last class vset kernel
   float vset_ms = 0.0f;
+  double* d_met = nullptr;             // corner winds + unscaled diffusion staging
+  size_t met_cap = 0;
   bool prof = false;                   // per-phase event timing (no graph)
   cudaEvent_t pev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   double prof_ms[5] = {0, 0, 0, 0, 0};  // prep+source, x, y, z, flux+clock
@@ -266,6 +288,7 @@ extern "C" int f3d_ens_destroy(f3d_ens* e) {
   drop_graphs(e);
   for (void* p : e->work_allocs) cudaFree(p);
   for (void* p : e->allocs) cudaFree(p);
+  if (e->d_met) cudaFree(e->d_met);
   if (e->h_pin) cudaFreeHost(e->h_pin);
   for (auto& ev : e->vev)
     if (ev) cudaEventDestroy(ev);
@@ -515,6 +538,100 @@ extern "C" int f3d_ens_set_class_meteo(f3d_ens* e, int ci, const double* u, cons
       ens_upload_conv(e, k, 5, k3, (nz + 4) * nx * ny, k.k3z))
     return 1;
   if (vs && ens_upload_conv(e, k, 6, vs, nx * ny * (nz + 3) * nb, k.vs)) return 1;
+  k.t_its = t_its;
+  k.t_ite = t_ite;
+  for (int m = 0; m < e->nm; ++m)
+    if (e->member_class[m] == ci) {
+      e->hm[m].t_its = t_its;
+      e->hm[m].t_ite = t_ite;
+    }
+  if (upload_members(e)) return 1;
+  k.meteo_set = true;
+  return class_derived_fields(e, ci);
+}
+
+extern "C" int f3d_ens_set_class_terrain(f3d_ens* e, int ci, int map_v, double X3max,
+                                         const double* X3_c, const double* X3_p,
+                                         const double* dhdx_p, const double* dhdy_p) {
+  if (!e || ci < 0 || ci >= e->ncls) return set_error_msg("f3d_ens_set_class_terrain: bad class");
+  if (map_v < 0 || map_v > 2) return set_error_msg("f3d_ens_set_class_terrain: mapping %d not implemented", map_v);
+  if (map_v != 0 && (!X3_c || !X3_p || !dhdx_p || !dhdy_p || !(X3max > 0.0)))
+    return set_error_msg("f3d_ens_set_class_terrain: sigma mappings need X3max > 0, X3_c, X3_p and the slopes");
+  ECK(cudaSetDevice(e->device));
+  EnsClass& k = e->cls[ci];
+  const size_t nx = k.nx, ny = k.ny, nz = k.nz;
+  if (!k.terrain && ealloc(e, &k.terrain, (nz + 1) + nz + 2 * nx * ny)) return 1;
+  if (map_v != 0) {
+    ECK(cudaMemcpy(k.terrain, X3_c, (nz + 1) * 8, cudaMemcpyHostToDevice));
+    ECK(cudaMemcpy(k.terrain + nz + 1, X3_p, nz * 8, cudaMemcpyHostToDevice));
+    ECK(cudaMemcpy(k.terrain + 2 * nz + 1, dhdx_p, nx * ny * 8, cudaMemcpyHostToDevice));
+    ECK(cudaMemcpy(k.terrain + 2 * nz + 1 + nx * ny, dhdy_p, nx * ny * 8, cudaMemcpyHostToDevice));
+  }
+  k.map_v = map_v;
+  k.X3max = map_v != 0 ? X3max : 1.0;
+  return 0;
+}
+
+extern "C" int f3d_ens_set_class_meteo_corners(f3d_ens* e, int ci, const double* uc, const double* vc,
+                                               const double* wc, const double* k1, const double* k2,
+                                               const double* k3, double kh, double kv, double t_its,
+                                               double t_ite) {
+  if (!e || ci < 0 || ci >= e->ncls) return set_error_msg("f3d_ens_set_class_meteo_corners: bad class");
+  if (!uc || !vc || !wc) return set_error_msg("f3d_ens_set_class_meteo_corners: null corner wind");
+  const bool kgiven = k1 || k2 || k3;
+  if (kgiven && !(k1 && k2 && k3))
+    return set_error_msg("f3d_ens_set_class_meteo_corners: give all of k1, k2, k3 or none");
+  if (!(t_ite != t_its)) return set_error_msg("f3d_ens_set_class_meteo_corners: t_ite == t_its");
+  EnsClass& k = e->cls[ci];
+  if (!k.grid_set) return set_error_msg("f3d_ens_set_class_meteo_corners: grid not set");
+  ECK(cudaSetDevice(e->device));
+  const size_t nx = k.nx, ny = k.ny, nz = k.nz;
+  const size_t ncor = (nx + 1) * (ny + 1) * (nz + 1);
+  const size_t n1 = (nx + 4) * ny * nz, n2 = nx * (ny + 4) * nz, n3 = nx * ny * (nz + 4);
+  const size_t need = 6 * ncor + n1 + n2 + n3;
+  if (need > e->met_cap) {
+    if (e->d_met) {
+      ECK(cudaStreamSynchronize(e->st));
+      cudaFree(e->d_met);
+      e->d_met = nullptr;
+      e->met_cap = 0;
+    }
+    ECK(cudaMalloc(&e->d_met, need * 8));
+    e->met_cap = need;
+  }
+  double* duc = e->d_met;
+  double* dvc = duc + 2 * ncor;
+  double* dwc = dvc + 2 * ncor;
+  double* dk1 = dwc + 2 * ncor;
+  double* dk2 = dk1 + n1;
+  double* dk3 = dk2 + n2;
+  ECK(cudaMemcpyAsync(duc, uc, 2 * ncor * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(dvc, vc, 2 * ncor * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaMemcpyAsync(dwc, wc, 2 * ncor * 8, cudaMemcpyHostToDevice, e->st));
+  if (kgiven) {
+    ECK(cudaMemcpyAsync(dk1, k1, n1 * 8, cudaMemcpyHostToDevice, e->st));
+    ECK(cudaMemcpyAsync(dk2, k2, n2 * 8, cudaMemcpyHostToDevice, e->st));
+    ECK(cudaMemcpyAsync(dk3, k3, n3 * 8, cudaMemcpyHostToDevice, e->st));
+  } else {
+    launch_meteo_kconst(k.nx, k.ny, k.nz, kh, kv, dk1, dk2, dk3, e->st);
+    e->launches += 1;
+  }
+  MetGeo g;
+  g.nx = k.nx;
+  g.ny = k.ny;
+  g.nz = k.nz;
+  g.map_v = k.map_v;
+  g.X3max = k.X3max;
+  g.X3c = k.terrain;
+  g.X3p = k.terrain ? k.terrain + nz + 1 : nullptr;
+  g.dhdx = k.terrain ? k.terrain + 2 * nz + 1 : nullptr;
+  g.dhdy = k.terrain ? k.terrain + 2 * nz + 1 + nx * ny : nullptr;
+  g.hm1 = k.hm[0];
+  g.hm2 = k.hm[1];
+  g.hm3 = k.hm[2];
+  launch_meteo_corners(g, duc, dvc, dwc, dk1, dk2, dk3, k.ux, k.vy, k.wz, k.k1x, k.k2y, k.k3z, e->st);
+  e->launches += 9;
+  ECKL();
   k.t_its = t_its;
   k.t_ite = t_ite;
   for (int m = 0; m < e->nm; ++m)

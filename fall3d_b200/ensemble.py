@@ -86,6 +86,31 @@ class Ensemble:
                                             _p(k3), _p(vs), float(t_its), float(t_ite)),
               "f3d_ens_set_class_meteo")
 
+    def set_class_terrain(self, ci, g):
+        """Vertical mapping and terrain slopes of class ci's grid g."""
+        if g.map_v == 0:
+            check(lib().f3d_ens_set_class_terrain(self._h, ci, 0, 1.0, None, None, None, None),
+                  "f3d_ens_set_class_terrain")
+            return
+        arr = [np.ascontiguousarray(a, dtype=np.float64).ravel(order="F")
+               for a in (g.X3_c, g.X3_p, g.dhdx_p, g.dhdy_p)]
+        check(lib().f3d_ens_set_class_terrain(self._h, ci, int(g.map_v), float(g.X3max),
+                                              *[a.ctypes.data_as(_dp) for a in arr]),
+              "f3d_ens_set_class_terrain")
+
+    def set_class_meteo_corners(self, ci, uc_pair, vc_pair, wc_pair, k1=None, k2=None, k3=None,
+                                kh=0.0, kv=0.0, t_its=0.0, t_ite=3600.0):
+        """The meteo term of class ci built on the device from corner winds
+        of the two time levels and unscaled (or constant) diffusion."""
+        def pair(p):
+            return np.asfortranarray(np.stack([np.asarray(p[0], np.float64), np.asarray(p[1], np.float64)],
+                                              axis=3))
+        uc, vc, wc = pair(uc_pair), pair(vc_pair), pair(wc_pair)
+        ks = [None if a is None else np.asfortranarray(a, dtype=np.float64) for a in (k1, k2, k3)]
+        check(lib().f3d_ens_set_class_meteo_corners(self._h, ci, _p(uc), _p(vc), _p(wc), *[_p(a) for a in ks],
+                                                    float(kh), float(kv), float(t_its), float(t_ite)),
+              "f3d_ens_set_class_meteo_corners")
+
     def compute_class_vset(self, ci, model, rhoc, tc, diam, rhop, psi, bin_cat):
         cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
         check(lib().f3d_ens_compute_class_vset(

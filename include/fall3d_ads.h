@@ -284,6 +284,15 @@ int f3d_ens_set_class_meteo(f3d_ens *ens, int cls, const double *u,
                             const double *v, const double *w, const double *k1,
                             const double *k2, const double *k3, const double *vs,
                             double t_its, double t_ite);
+/* f3d_ads_set_terrain and f3d_ads_set_meteo_corners for a grid class. */
+int f3d_ens_set_class_terrain(f3d_ens *ens, int cls, int map_v, double X3max,
+                              const double *X3_c, const double *X3_p,
+                              const double *dhdx_p, const double *dhdy_p);
+int f3d_ens_set_class_meteo_corners(f3d_ens *ens, int cls, const double *uc,
+                                    const double *vc, const double *wc,
+                                    const double *k1, const double *k2,
+                                    const double *k3, double kh, double kv,
+                                    double t_its, double t_ite);
 /* phys_get_vset + vs/Hm3 of a class on the device (see f3d_ads_compute_vset). */
 int f3d_ens_compute_class_vset(f3d_ens *ens, int cls, int model,
                                const double *rhoc, const double *tc,

@@ -98,3 +98,35 @@ def test_device_meteo_constant_diffusion(built_lib):
     dev.close()
     assert r_host[0] == r_dev[0]
     assert np.array_equal(r_host[1], r_dev[1])
+
+
+def test_ensemble_class_meteo_corners(built_lib):
+    """Two grid classes set from corner winds on the device give the members
+    the bits of the same classes set from host-built step-layout arrays."""
+    from fall3d_b200.ensemble import Ensemble
+    cases = [_case(G.MAP_V_SIGMA_LINEAR_DECAY, seed=5), _case(G.MAP_V_SIGMA_NO_DECAY, seed=6)]
+    grids = [c[0] for c in cases]
+    members, factors = [0, 1, 1], [1.0, 0.9, 1.1]
+    T, rho = meteo.std_atmosphere(grids[0].z_c)
+    diam = np.array([5e-4, 1e-4, 2e-5])
+    outs = []
+    for path in ("host", "device"):
+        ens = Ensemble(grids, NB, members, factors, 2, 2, 0)
+        for ci, (g, winds, ks, _) in enumerate(cases):
+            if path == "host":
+                ens.set_class_meteo(ci, *_host_arrays(g, winds, ks), None, 0.0, 3600.0)
+            else:
+                ens.set_class_terrain(ci, g)
+                ens.set_class_meteo_corners(ci, winds[0], winds[1], winds[2], *ks, t_its=0.0, t_ite=3600.0)
+            ens.compute_class_vset(ci, 2, np.asfortranarray(rho), np.asfortranarray(T), diam,
+                                   np.full(NB, 2000.0), np.full(NB, 0.8), np.ones(NB, np.int32))
+        for m, ci in enumerate(members):
+            ens.upload_member_state(m, cases[ci][3], np.zeros((NX + 4, NY + 4, NB), order="F"))
+        dts = ens.compute_time_steps(0.5, 2, 0.9, 1e30)
+        ens.set_clock(np.zeros(len(members)), 0)
+        ens.run(3)
+        outs.append((dts, [ens.download_member_state(m)[0] for m in range(len(members))]))
+        ens.close()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    for m in range(len(members)):
+        assert np.array_equal(outs[0][1][m], outs[1][1][m]), m
