@@ -34,6 +34,9 @@ SIGNATURES = {
     "f3d_ads_set_grid": [_vp] + [_dp] * 9,
     "f3d_ads_set_meteo": [_vp] + [_dp] * 7 + [C.c_double, C.c_double],
     "f3d_ads_set_terrain": [_vp, C.c_int, C.c_double, _dp, _dp, _dp, _dp],
+    "f3d_ads_set_wet_deposition": [_vp, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _ip, _dp],
+    "f3d_ads_set_radionuclides": [_vp, _ip, _ip],
+    "f3d_ads_get_awet": [_vp, _dp],
     "f3d_ads_set_meteo_corners": [_vp] + [_dp] * 6 + [C.c_double] * 4,
     "f3d_ads_set_source": [_vp, C.c_int, _ip, _dp],
     "f3d_ads_set_source_dense": [_vp, _dp],

@@ -109,6 +109,36 @@ class Domain:
                                               float(kh), float(kv), float(t_its), float(t_ite)),
               "f3d_ads_set_meteo_corners")
 
+    def phys_wet_deposition(self, a, b, pre, pblh, bin_cat, bin_diam):
+        """Switch on wet deposition for this meteo interval (precipitation
+        rate and boundary-layer height per column); bin_cat=None switches it
+        off.  Topography and corner heights come from the grid."""
+        g = self.grid
+        if bin_cat is None:
+            check(lib().f3d_ads_set_wet_deposition(self._h, 0.0, 0.0, None, None, None, None, None, None),
+                  "f3d_ads_set_wet_deposition")
+            return
+        arr = [np.asfortranarray(x, dtype=np.float64) for x in (pre, pblh, g.h_c, g.z_c)]
+        cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
+        check(lib().f3d_ads_set_wet_deposition(self._h, float(a), float(b), *[_p(x) for x in arr], _ip(cat),
+                                               _p(np.ascontiguousarray(bin_diam, np.float64))),
+              "f3d_ads_set_wet_deposition")
+
+    def phys_radionuclides(self, bin_cat, bin_spe):
+        """Switch on radioactive decay of the category-3 bins (species 5..9)."""
+        if bin_cat is None:
+            check(lib().f3d_ads_set_radionuclides(self._h, None, None), "f3d_ads_set_radionuclides")
+            return
+        cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
+        spe = np.ascontiguousarray(bin_spe, dtype=np.int32)
+        check(lib().f3d_ads_set_radionuclides(self._h, _ip(cat), _ip(spe)), "f3d_ads_set_radionuclides")
+
+    def get_awet(self):
+        g = self.grid
+        aw = np.zeros((g.nx + 4, g.ny + 4, self.nbins), order="F")
+        check(lib().f3d_ads_get_awet(self._h, _p(aw)), "f3d_ads_get_awet")
+        return aw
+
     def set_source(self, ijk, vals):
         ijk = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
         vals = np.ascontiguousarray(vals, dtype=np.float64).reshape(-1, self.nbins)

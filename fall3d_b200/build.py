@@ -26,6 +26,7 @@ SOURCES = [
     ("mlp.cu", ["--fmad=false"]),
     ("noalloc.cu", ["--fmad=false"]),
     ("meteo_dev.cu", ["--fmad=false"]),
+    ("deposit_dev.cu", ["--fmad=false"]),
     ("f3d_capi.cu", ["-Xcompiler", "-ffp-contract=off"]),
 ]
 

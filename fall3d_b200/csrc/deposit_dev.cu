@@ -1,0 +1,104 @@
+// deposit_dev.cu -- the two processes F3D_time_step applies after the sweeps
+// (mod_F3D.F90:1493-1520):
+//
+//   * wet deposition, phys_wet_deposition (mod_Phys.F90:1358-1427): in every
+//     column, scavenging coefficient lambda = min(1, dt a P^b) from the
+//     precipitation rate P; every cell of a particle or radionuclide bin of
+//     diameter <= 100 um below the boundary-layer top loses lambda c, which is
+//     added (times dX3_p) to the wet deposit awet, in k order;
+//   * radioactive decay, phys_radionuclides (mod_Phys.F90:1216-1342): every
+//     radionuclide bin (and its dry and wet deposits) is multiplied by
+//     exp(-kn dt); a Y90 bin is then set from its Sr90 parent,
+//     c(Y90) = c(Sr90) (1 - exp(-kn_Sr90 dt)), as the reference does (an
+//     assignment: the decayed Y90 value is overwritten), with the parent's
+//     value as it stands at that point of the bin loop.
+//
+// P^b, the boundary-layer test and the decay factors are evaluated on the
+// host, with the same C library as the CPU restatement; the kernels do the
+// per-cell arithmetic in the reference's order (compiled with --fmad=false).
+#include <cuda_runtime.h>
+
+#include "f3d_common.cuh"
+
+namespace f3d {
+
+struct WetArgs {
+  int nx, ny, nz, nb;
+  double dta;              // dt * a
+  const double* powpb;     // P^b per column, nx*ny
+  const int* ktop;         // cells k < ktop of the column are below the PBL top
+  const double* dx3p;      // dX3_p with the reference offset (kps-2)
+  double* awet;            // [bin][j][i]
+  double* c64;             // exact form state (or null)
+  float* c32;              // precision form state (or null)
+  unsigned long long mask; // bins that take wet deposition
+};
+
+__global__ void k_wet(WetArgs a) {
+  const long long ncol = (long long)a.nx * a.ny;
+  const long long tot = ncol * a.nb;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long ij = e % ncol;
+    const int b = (int)(e / ncol);
+    if (!((a.mask >> b) & 1ull)) continue;
+    double lambda = a.dta * a.powpb[ij];
+    if (lambda > 1.0) lambda = 1.0;
+    const int kt = a.ktop[ij];
+    double aw = a.awet[e];
+    for (int k = 0; k < kt; ++k) {
+      const long long q = ((long long)b * a.nz + k) * ncol + ij;
+      if (a.c64) {
+        const double cv = a.c64[q];
+        aw = aw + a.dx3p[k + 2] * lambda * cv;
+        a.c64[q] = cv * (1.0 - lambda);
+      } else {
+        const double cv = (double)a.c32[q];
+        aw = aw + a.dx3p[k + 2] * lambda * cv;
+        a.c32[q] = (float)(cv * (1.0 - lambda));
+      }
+    }
+    a.awet[e] = aw;
+  }
+}
+
+struct RadioArgs {
+  int nx, ny, nz, nr;       // nr radionuclide bins, in bin order
+  int bin[64];              // their bin indices
+  int parent[64];           // Y90: bin index of the Sr90 parent, else -1
+  double fact[64];          // exp(-kn dt) of the bin
+  double pfact[64];         // exp(-kn dt) of the parent
+  double* c64;
+  float* c32;
+  double* acum;             // [bin][j][i]
+  double* awet;             // [bin][j][i] or null
+};
+
+template <class T>
+__device__ __forceinline__ void decay_cell(const RadioArgs& a, T* c, long long q, long long stride) {
+  for (int r = 0; r < a.nr; ++r) {
+    T* p = c + (long long)a.bin[r] * stride + q;
+    *p = (T)((double)*p * a.fact[r]);
+    if (a.parent[r] >= 0) *p = (T)((double)c[(long long)a.parent[r] * stride + q] * (1.0 - a.pfact[r]));
+  }
+}
+
+__global__ void k_radio(RadioArgs a) {
+  const long long n2 = (long long)a.nx * a.ny, n3 = n2 * a.nz;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n3 + n2;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (e < n3) {
+      if (a.c64) decay_cell(a, a.c64, e, n3);
+      else decay_cell(a, a.c32, e, n3);
+    } else {
+      const long long q = e - n3;
+      decay_cell(a, a.acum, q, n2);
+      if (a.awet) decay_cell(a, a.awet, q, n2);
+    }
+  }
+}
+
+void launch_wet(const WetArgs& a, cudaStream_t st) { k_wet<<<592, 256, 0, st>>>(a); }
+void launch_radio(const RadioArgs& a, cudaStream_t st) { k_radio<<<592, 256, 0, st>>>(a); }
+
+}  // namespace f3d

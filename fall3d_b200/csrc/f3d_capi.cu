@@ -53,6 +53,30 @@ void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, c
                           cudaStream_t st);
 void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
                          double* k3, cudaStream_t st);
+struct WetArgs {
+  int nx, ny, nz, nb;
+  double dta;
+  const double* powpb;
+  const int* ktop;
+  const double* dx3p;
+  double* awet;
+  double* c64;
+  float* c32;
+  unsigned long long mask;
+};
+struct RadioArgs {
+  int nx, ny, nz, nr;
+  int bin[64];
+  int parent[64];
+  double fact[64];
+  double pfact[64];
+  double* c64;
+  float* c32;
+  double* acum;
+  double* awet;
+};
+void launch_wet(const WetArgs& a, cudaStream_t st);
+void launch_radio(const RadioArgs& a, cudaStream_t st);
 int mlp_vset_field(f3d_mlp* h, const MemberDev* dm, int mi, int nx, int ny, int nz, int nb,
                    const double* drhoc, const double* dtc, const double* diam, const double* rhop,
                    const double* psi, const int* bin_cat, const int* is_aggregate, double vset_fac,
@@ -154,6 +178,16 @@ struct f3d_ctx {
   double* d_terrain = nullptr;  // X3_c (nz+1), X3_p (nz), dhdx_p, dhdy_p (nx*ny each)
   double* d_met = nullptr;      // corner winds of two snapshots + unscaled diffusion
   size_t met_cap = 0;
+  // wet deposition (after the z sweep) and radioactive decay
+  bool wet_on = false;
+  double wet_a = 0.0;
+  double* d_powpb = nullptr;    // P^b per column
+  int* d_ktop = nullptr;        // levels below the boundary-layer top per column
+  double* d_awet = nullptr;     // wet deposit [bin][j][i]
+  unsigned long long wet_mask = 0;
+  bool radio_on = false;
+  std::vector<int> rad_bin, rad_parent;
+  std::vector<double> rad_kn, rad_pkn;
 };
 
 template <class T>
@@ -527,6 +561,119 @@ extern "C" int f3d_ads_set_meteo_corners(f3d_ctx* c, const double* uc, const dou
   return 0;
 }
 
+extern "C" int f3d_ads_set_wet_deposition(f3d_ctx* c, double a, double b, const double* pre,
+                                          const double* pblh, const double* h_c, const double* z_c,
+                                          const int* bin_cat, const double* bin_diam) {
+  if (!c) return set_err("f3d_ads_set_wet_deposition: null context");
+  if (!bin_cat) {
+    c->wet_on = false;
+    return 0;
+  }
+  if (!pre || !pblh || !h_c || !z_c || !bin_diam) return set_err("f3d_ads_set_wet_deposition: null array");
+  if (!c->grid_set) return set_err("f3d_ads_set_wet_deposition: grid not set");
+  if (c->nb > 64) return set_err("f3d_ads_set_wet_deposition: at most 64 bins");
+  CK(cudaSetDevice(c->device));
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  const size_t ncol = (size_t)nx * ny;
+  std::vector<double> powpb(ncol);
+  std::vector<int> ktop(ncol);
+#define HC(i, j) h_c[(i) + (size_t)(nx + 1) * (j)]
+#define ZC(i, j, k) z_c[(i) + (size_t)(nx + 1) * ((j) + (size_t)(ny + 1) * (k))]
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t ij = i + (size_t)nx * j;
+      powpb[ij] = pow(pre[ij], b);
+      // cells below the boundary-layer top (mod_Phys.F90:1404-1414); heights
+      // grow with k, so they are the first ktop levels of the column
+      const double ho = 0.25 * (HC(i, j) + HC(i + 1, j) + HC(i, j + 1) + HC(i + 1, j + 1));
+      int kt = 0;
+      for (int k = 0; k < nz; ++k) {
+        const double zp1 = 0.25 * (ZC(i, j, k) + ZC(i + 1, j, k) + ZC(i, j + 1, k) + ZC(i + 1, j + 1, k));
+        const double zp2 = 0.25 * (ZC(i, j, k + 1) + ZC(i + 1, j, k + 1) + ZC(i, j + 1, k + 1) +
+                                   ZC(i + 1, j + 1, k + 1));
+        const double zp = 0.5 * (zp1 + zp2);
+        const bool below = ho + zp <= pblh[ij];
+        if (below && kt != k) return set_err("f3d_ads_set_wet_deposition: heights not increasing with k");
+        if (below) kt = k + 1;
+      }
+      ktop[ij] = kt;
+    }
+#undef HC
+#undef ZC
+  if (!c->d_powpb) {
+    if (dalloc(c, &c->d_powpb, ncol) || dalloc(c, &c->d_ktop, ncol) ||
+        dalloc(c, &c->d_awet, ncol * c->nb))
+      return 1;
+    CK(cudaMemset(c->d_awet, 0, ncol * c->nb * 8));
+  }
+  CK(cudaMemcpy(c->d_powpb, powpb.data(), ncol * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_ktop, ktop.data(), ncol * 4, cudaMemcpyHostToDevice));
+  unsigned long long mask = 0;
+  for (int q = 0; q < c->nb; ++q)  // particles and radionuclides below 100 um (mod_F3D.F90:1499-1506)
+    if ((bin_cat[q] == 1 || bin_cat[q] == 3) && bin_diam[q] <= 1e-4) mask |= 1ull << q;
+  c->wet_mask = mask;
+  c->wet_a = a;
+  c->wet_on = true;
+  return 0;
+}
+
+extern "C" int f3d_ads_set_radionuclides(f3d_ctx* c, const int* bin_cat, const int* bin_spe) {
+  if (!c) return set_err("f3d_ads_set_radionuclides: null context");
+  c->radio_on = false;
+  c->rad_bin.clear();
+  c->rad_parent.clear();
+  c->rad_kn.clear();
+  c->rad_pkn.clear();
+  if (!bin_cat || !bin_spe) return 0;
+  if (c->nb > 64) return set_err("f3d_ads_set_radionuclides: at most 64 bins");
+  auto rate = [](int spe) {  // mod_Phys.F90:79-83
+    switch (spe) {
+      case 5: return 1.06e-8;
+      case 6: return 9.29e-10;
+      case 7: return 1.00e-6;
+      case 8: return 7.63e-10;
+      case 9: return 2.98e-6;
+    }
+    return -1.0;
+  };
+  int ny90 = 0, nsr90 = 0, shift = 0;
+  for (int q = 0; q < c->nb; ++q) {
+    if (bin_cat[q] == 3 && bin_spe[q] == 9 && ++ny90 == 1) shift -= q;
+    if (bin_cat[q] == 3 && bin_spe[q] == 8 && ++nsr90 == 1) shift += q;
+  }
+  if (ny90 != nsr90) return set_err("The number of SR90 and Y90 classes must be equal.");
+  for (int q = 0; q < c->nb; ++q) {
+    if (bin_cat[q] != 3) continue;
+    const double kn = rate(bin_spe[q]);
+    if (kn < 0.0) return set_err("Invalid radionuclide type: species %d", bin_spe[q]);
+    const int par = (bin_spe[q] == 9) ? q + shift : -1;
+    c->rad_bin.push_back(q);
+    c->rad_parent.push_back(par);
+    c->rad_kn.push_back(kn);
+    c->rad_pkn.push_back(par >= 0 ? rate(bin_spe[par]) : 0.0);
+  }
+  c->radio_on = !c->rad_bin.empty();
+  return 0;
+}
+
+extern "C" int f3d_ads_get_awet(f3d_ctx* c, double* my_awet) {
+  if (!c || !my_awet) return set_err("f3d_ads_get_awet: null argument");
+  const size_t nx = c->nx, ny = c->ny, nb = c->nb;
+  std::vector<double> d(nx * ny * nb, 0.0);
+  if (c->d_awet) {
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaMemcpy(d.data(), c->d_awet, d.size() * 8, cudaMemcpyDeviceToHost));
+  }
+  // my_awet(ips-2:ipe+2, jps-2:jpe+2, nbins), halos zero
+  std::fill(my_awet, my_awet + (nx + 4) * (ny + 4) * nb, 0.0);
+  for (size_t b = 0; b < nb; ++b)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i)
+        my_awet[(i + 2) + (nx + 4) * ((j + 2) + (ny + 4) * b)] = d[(b * ny + j) * nx + i];
+  return 0;
+}
+
 extern "C" int f3d_ads_set_source(f3d_ctx* c, int n, const int* ijk, const double* s) {
   if (!c) return set_err("f3d_ads_set_source: null context");
   if (n < 0 || (n > 0 && (!ijk || !s))) return set_err("f3d_ads_set_source: bad arguments");
@@ -706,6 +853,51 @@ static int check_ready(f3d_ctx* c, const char* who) {
   return 0;
 }
 
+// Wet deposition and radioactive decay after the sweeps (mod_F3D.F90:1497-1520).
+static int enqueue_wet_radio(f3d_ctx* c, double dt) {
+  MemberDev& m = c->hm;
+  if (c->wet_on) {
+    WetArgs a;
+    a.nx = c->nx;
+    a.ny = c->ny;
+    a.nz = c->nz;
+    a.nb = c->nb;
+    a.dta = dt * c->wet_a;
+    a.powpb = c->d_powpb;
+    a.ktop = c->d_ktop;
+    a.dx3p = m.dx3p;
+    a.awet = c->d_awet;
+    a.c64 = m.c64;
+    a.c32 = m.c32;
+    a.mask = c->wet_mask;
+    launch_wet(a, c->st);
+    c->launches += 1;
+    CKL();
+  }
+  if (c->radio_on) {
+    RadioArgs r;
+    memset(&r, 0, sizeof(r));
+    r.nx = c->nx;
+    r.ny = c->ny;
+    r.nz = c->nz;
+    r.nr = (int)c->rad_bin.size();
+    for (int q = 0; q < r.nr; ++q) {
+      r.bin[q] = c->rad_bin[q];
+      r.parent[q] = c->rad_parent[q];
+      r.fact[q] = exp(-c->rad_kn[q] * dt);
+      r.pfact[q] = c->rad_parent[q] >= 0 ? exp(-c->rad_pkn[q] * dt) : 1.0;
+    }
+    r.c64 = m.c64;
+    r.c32 = m.c32;
+    r.acum = m.acum;
+    r.awet = c->wet_on ? c->d_awet : nullptr;
+    launch_radio(r, c->st);
+    c->launches += 1;
+    CKL();
+  }
+  return 0;
+}
+
 static int enqueue_step(f3d_ctx* c, double dt, double time, int iiter) {
   // event slots: 0 start, 1 after prep+source, 2..4 after the 1st/2nd/z sweep, 5 end
   auto rec = [&](int k) { if (c->prof) cudaEventRecord(c->ev[k], c->st); };
@@ -725,6 +917,7 @@ static int enqueue_step(f3d_ctx* c, double dt, double time, int iiter) {
   launch_flux_reduce(c->dm, 1, 7, c->st);
   c->launches += 1;
   CKL();
+  if (enqueue_wet_radio(c, dt)) return 1;
   rec(5);
   if (c->prof) {
     CK(cudaEventSynchronize(c->ev[5]));

@@ -109,6 +109,28 @@ int f3d_ads_set_meteo_corners(f3d_ctx *ctx, const double *uc, const double *vc,
                               const double *k2, const double *k3, double kh,
                               double kv, double t_its, double t_ite);
 
+/* Wet deposition, phys_wet_deposition (mod_Phys.F90:1358-1427), applied in
+ * every step after the sweeps (mod_F3D.F90:1497-1513) to the bins of
+ * category 1 (particle) or 3 (radionuclide) with diameter <= 1e-4 m:
+ * scavenging lambda = min(1, dt a P^b) (MY_MOD%wet_deposition_a/_b),
+ * below the boundary-layer top only.  pre, pblh(ips:ipe,jps:jpe) precipitation
+ * rate and boundary-layer height of the meteo interval; h_c(ibs:ibe,jbs:jbe)
+ * topography and z_c(ibs:ibe,jbs:jbe,kbs:kbe) heights of the cell corners.
+ * Call again at each meteo update; bin_cat = NULL switches it off.  The wet
+ * deposit starts at zero and is read with f3d_ads_get_awet. */
+int f3d_ads_set_wet_deposition(f3d_ctx *ctx, double a, double b,
+                               const double *pre, const double *pblh,
+                               const double *h_c, const double *z_c,
+                               const int *bin_cat, const double *bin_diam);
+/* Radioactive decay, phys_radionuclides (mod_Phys.F90:1216-1342), applied in
+ * every step after wet deposition to the bins of category 3 in the air and in
+ * the dry and wet deposits.  bin_spe: species 5 Cs134, 6 Cs137, 7 I131,
+ * 8 Sr90, 9 Y90 (mod_KindType.F90:62-66); NULL switches it off. */
+int f3d_ads_set_radionuclides(f3d_ctx *ctx, const int *bin_cat,
+                              const int *bin_spe);
+/* MY_TRA%my_awet(ips-2:ipe+2, jps-2:jpe+2, nbins), halos zero. */
+int f3d_ads_get_awet(f3d_ctx *ctx, double *my_awet);
+
 /* Source term MY_TRA%my_s(ips:ipe,jps:jpe,kps:kpe,nbins) after
  * F3D_set_source_term (mod_F3D.F90:349-555), given sparsely: n cells with
  * 1-based Fortran indices ijk[3*q+0..2] and values s[nbins*q + bin] (the

@@ -713,3 +713,97 @@ double or_perturb(int var_id, int ptype, double var, double random,
   }
   return out;
 }
+
+/* ---- wet deposition and radionuclide decay ------------------------------ */
+void or_wet_deposition(const or_dims *d, double dt, double a, double b,
+                       const double *pre, const double *pblh,
+                       const double *h_c, const double *z_c,
+                       const double *dX3_p, double *awet, double *c) {
+  const int nx = d->nx, ny = d->ny, nz = d->nz;
+  const long hx = nx + 4, hy = ny + 4;
+#define HC(i, j) h_c[(i) + (long)(nx + 1) * (j)]
+#define ZC(i, j, k) z_c[(i) + (long)(nx + 1) * ((j) + (long)(ny + 1) * (k))]
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      /* lambda = min(1, dt*a*pre**b)  (mod_Phys.F90:1402) */
+      double lambda = dt * a * pow(pre[i + (long)nx * j], b);
+      if (lambda > 1.0) lambda = 1.0;
+      const double pb = pblh[i + (long)nx * j];
+      const double ho = 0.25 * (HC(i, j) + HC(i + 1, j) + HC(i, j + 1) + HC(i + 1, j + 1));
+      double *aw = &awet[(i + 2) + hx * (j + 2)];
+      for (int k = 0; k < nz; ++k) {
+        const double zp1 = 0.25 * (ZC(i, j, k) + ZC(i + 1, j, k) + ZC(i, j + 1, k) + ZC(i + 1, j + 1, k));
+        const double zp2 = 0.25 * (ZC(i, j, k + 1) + ZC(i + 1, j, k + 1) + ZC(i, j + 1, k + 1) +
+                                   ZC(i + 1, j + 1, k + 1));
+        const double zp = 0.5 * (zp1 + zp2);
+        if (ho + zp <= pb) {
+          double *cc = &c[(i + 2) + hx * ((j + 2) + hy * (long)(k + 2))];
+          *aw = *aw + dX3_p[k + 2] * lambda * (*cc);
+          *cc = *cc * (1.0 - lambda);
+        }
+      }
+    }
+#undef HC
+#undef ZC
+}
+
+static double or_decay_rate(int spe) {
+  switch (spe) { /* mod_Phys.F90:79-83 */
+    case 5: return 1.06e-8;   /* Cs134 */
+    case 6: return 9.29e-10;  /* Cs137 */
+    case 7: return 1.00e-6;   /* I131 */
+    case 8: return 7.63e-10;  /* Sr90 */
+    case 9: return 2.98e-6;   /* Y90 */
+  }
+  return -1.0;
+}
+
+int or_radionuclides(const or_dims *d, double dt, const int *bin_cat,
+                     const int *bin_spe, double *c, double *acum,
+                     double *awet) {
+  const int nb = d->nbins;
+  const long n2 = (long)(d->nx + 4) * (d->ny + 4), n3 = n2 * (d->nz + 4);
+  int ny90 = 0, nsr90 = 0, shift = 0;
+  for (int b = 0; b < nb; ++b) {
+    if (bin_cat[b] == 3 && bin_spe[b] == 9) {
+      ++ny90;
+      if (ny90 == 1) shift -= b;
+    }
+    if (bin_cat[b] == 3 && bin_spe[b] == 8) {
+      ++nsr90;
+      if (nsr90 == 1) shift += b;
+    }
+  }
+  if (ny90 != nsr90 || nb > 64) return 1;
+  double fact[64];
+  for (int b = 0; b < nb && b < 64; ++b) {
+    fact[b] = 1.0;
+    if (bin_cat[b] == 3) {
+      const double kn = or_decay_rate(bin_spe[b]);
+      if (kn < 0.0) return 1;
+      fact[b] = exp(-kn * dt);
+    }
+  }
+  /* in the air: bins in order; Y90 is then set from its Sr90 parent
+   * (mod_Phys.F90:1303-1318) */
+  for (int b = 0; b < nb; ++b) {
+    if (bin_cat[b] != 3) continue;
+    for (long q = 0; q < n3; ++q) {
+      c[q + n3 * b] = c[q + n3 * b] * fact[b];
+      if (bin_spe[b] == 9) c[q + n3 * b] = c[q + n3 * (b + shift)] * (1.0 - fact[b + shift]);
+    }
+  }
+  /* in the deposits (mod_Phys.F90:1320-1340) */
+  for (int b = 0; b < nb; ++b) {
+    if (bin_cat[b] != 3) continue;
+    for (long q = 0; q < n2; ++q) {
+      acum[q + n2 * b] = acum[q + n2 * b] * fact[b];
+      awet[q + n2 * b] = awet[q + n2 * b] * fact[b];
+      if (bin_spe[b] == 9) {
+        acum[q + n2 * b] = acum[q + n2 * (b + shift)] * (1.0 - fact[b + shift]);
+        awet[q + n2 * b] = awet[q + n2 * (b + shift)] * (1.0 - fact[b + shift]);
+      }
+    }
+  }
+  return 0;
+}

@@ -126,6 +126,23 @@ void or_place_source(const or_dims *d, const or_grid *g, double lonmin,
                      const double *y, const double *z, const double *M,
                      double *s);
 
+/* phys_wet_deposition (mod_Phys.F90:1358-1427) for one bin on a single-rank
+ * grid.  c(ips-2:ipe+2, jps-2:jpe+2, kps-2:kpe+2) and awet(ips-2:ipe+2,
+ * jps-2:jpe+2) in the reference layouts (INOUT); pre, pblh (nx, ny);
+ * h_c (nx+1, ny+1); z_c (nx+1, ny+1, nz+1); dX3_p (kps-2:kpe+2). */
+void or_wet_deposition(const or_dims *d, double dt, double a, double b,
+                       const double *pre, const double *pblh,
+                       const double *h_c, const double *z_c,
+                       const double *dX3_p, double *awet, double *c);
+
+/* phys_radionuclides (mod_Phys.F90:1216-1342): decay of the radionuclide
+ * bins (bin_cat 3, species 5 Cs134 .. 9 Y90) in the air, c(...,nbins) with
+ * two halos, and in the deposits acum, awet(ips-2:ipe+2, jps-2:jpe+2, nbins).
+ * Returns 1 when the numbers of Sr90 and Y90 bins differ. */
+int or_radionuclides(const or_dims *d, double dt, const int *bin_cat,
+                     const int *bin_spe, double *c, double *acum,
+                     double *awet);
+
 /* ensemble_perturbate_variable (mod_Ensemble.F90:888-935). */
 double or_perturb(int var_id, int ptype, double var, double random,
                   double range);

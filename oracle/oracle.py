@@ -73,6 +73,8 @@ def lib():
         L.or_place_source.argtypes = [D, G, C.c_double, C.c_double, C.c_double, C.c_double, dp,
                                       dp, dp, C.c_int, dp, dp, dp, dp, dp]
         L.or_perturb.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.or_wet_deposition.argtypes = [D, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp, dp]
+        L.or_radionuclides.argtypes = [D, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int), dp, dp, dp]
         L.or_perturb.restype = C.c_double
         _lib = L
     return _lib
@@ -146,6 +148,25 @@ class Oracle:
                                  _p(np.asarray(psi, np.float64)), cat, agg[0] if agg else None,
                                  vset_fac, _p(vs))
         return vs, flag
+
+    def wet_deposition(self, dt, a, b, pre, pblh, h_c, z_c, c, awet, bins):
+        """phys_wet_deposition for each bin in `bins` (0-based), in place on
+        c (nx+4, ny+4, nz+4, nbins) and awet (nx+4, ny+4, nbins)."""
+        pre, pblh, h_c, z_c = (np.asfortranarray(a, dtype=np.float64) for a in (pre, pblh, h_c, z_c))
+        n2 = (self.g.nx + 4) * (self.g.ny + 4)
+        n3 = n2 * (self.g.nz + 4)
+        dp = C.POINTER(C.c_double)
+        for b_ in bins:
+            cb = c.ctypes.data_as(C.c_void_p).value + 8 * n3 * b_
+            ab = awet.ctypes.data_as(C.c_void_p).value + 8 * n2 * b_
+            lib().or_wet_deposition(C.byref(self.dims), dt, a, b, _p(pre), _p(pblh), _p(h_c), _p(z_c),
+                                    _p(np.ascontiguousarray(self.g.dX3_p, np.float64)),
+                                    C.cast(ab, dp), C.cast(cb, dp))
+
+    def radionuclides(self, dt, bin_cat, bin_spe, c, acum, awet):
+        cat = (C.c_int * len(bin_cat))(*[int(x) for x in bin_cat])
+        spe = (C.c_int * len(bin_spe))(*[int(x) for x in bin_spe])
+        return lib().or_radionuclides(C.byref(self.dims), dt, cat, spe, _p(c), _p(acum), _p(awet))
 
     def place_source(self, lonmin, latmin, dlon, dlat, lon_c, lat_c, z_c, x, y, z, M):
         nb = self.dims.nbins
