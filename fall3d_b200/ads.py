@@ -139,6 +139,31 @@ class Domain:
         check(lib().f3d_ads_get_awet(self._h, _p(aw)), "f3d_ads_get_awet")
         return aw
 
+    def keep_boundary_halo(self, on=True):
+        """Keep the state's boundary halo layers (the free-flow ghosts the
+        sweeps write, mod_ADS.F90:1227-1326) for the output reductions and
+        for download_state/upload_state."""
+        check(lib().f3d_ads_keep_boundary_halo(self._h, int(bool(on))), "f3d_ads_keep_boundary_halo")
+
+    def nc_IO_out_res(self, bins, col_du=False):
+        """Per-species output fields of nc_IO_out_res (mod_nc_IO.F90:3206-4335)
+        at the cell corners: dict of con_sur (g/m3), col_mass (g/m2, DU with
+        col_du), cloud_top (m) and grn_load (kg/m2), each (nx+1, ny+1).
+        bins: indices of the bins summed (a species, or its bins below a PM
+        diameter for the PMxx column loads)."""
+        g = self.grid
+        if not getattr(self, "_zc_set", False):
+            check(lib().f3d_ads_set_corner_heights(self._h, _p(np.asfortranarray(g.z_c, dtype=np.float64))),
+                  "f3d_ads_set_corner_heights")
+            self._zc_set = True
+        sel = np.zeros(self.nbins, np.int32)
+        sel[list(bins)] = 1
+        keys = ("con_sur", "col_mass", "cloud_top", "grn_load")
+        out = {k: np.zeros((g.nx + 1, g.ny + 1), order="F") for k in keys}
+        check(lib().f3d_ads_output_species(self._h, _ip(sel), int(bool(col_du)), *[_p(out[k]) for k in keys]),
+              "f3d_ads_output_species")
+        return out
+
     def set_source(self, ijk, vals):
         ijk = np.ascontiguousarray(ijk, dtype=np.int32).reshape(-1, 3)
         vals = np.ascontiguousarray(vals, dtype=np.float64).reshape(-1, self.nbins)

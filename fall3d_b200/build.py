@@ -27,6 +27,7 @@ SOURCES = [
     ("noalloc.cu", ["--fmad=false"]),
     ("meteo_dev.cu", ["--fmad=false"]),
     ("deposit_dev.cu", ["--fmad=false"]),
+    ("output_dev.cu", ["--fmad=false"]),
     ("f3d_capi.cu", ["-Xcompiler", "-ffp-contract=off"]),
 ]
 

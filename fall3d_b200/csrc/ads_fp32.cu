@@ -217,6 +217,11 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
     if (lane_ok) {
       clo = (double)M.flux_lo * area * dt;
       chi = (double)M.flux_hi * area * dt;
+      if (m.gh32) {  // the free-flow ghosts of this pencil, kept for the output reductions
+        float* g = m.gh32 + (long long)b * gh_per_bin(nx, ny, nz);
+        g[gh_offset(DIR, 0, pen, nx, ny, nz)] = M.gL;
+        g[gh_offset(DIR, 1, pen, nx, ny, nz)] = M.gR;
+      }
     }
     if (DIR == DIR_Z) {
       double* a = m.acum + ((long long)b * ny + j) * nx + i;

@@ -208,6 +208,11 @@ __device__ __forceinline__ void sweep64_item(const MemberDev* __restrict__ membe
     if (lane_ok) {
       clo = M.flux_lo * area * dt;
       chi = M.flux_hi * area * dt;
+      if (m.gh64) {  // the free-flow ghosts of this pencil (mod_ADS.F90:1227-1326)
+        double* g = m.gh64 + (long long)b * gh_per_bin(nx, ny, nz);
+        g[gh_offset(DIR, 0, pen, nx, ny, nz)] = M.gL;
+        g[gh_offset(DIR, 1, pen, nx, ny, nz)] = M.gR;
+      }
     }
     if (DIR == DIR_Z) {
       double* a = m.acum + ((long long)b * ny + j) * nx + i;

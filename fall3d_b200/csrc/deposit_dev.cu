@@ -11,7 +11,9 @@
 //     exp(-kn dt); a Y90 bin is then set from its Sr90 parent,
 //     c(Y90) = c(Sr90) (1 - exp(-kn_Sr90 dt)), as the reference does (an
 //     assignment: the decayed Y90 value is overwritten), with the parent's
-//     value as it stands at that point of the bin loop.
+//     value as it stands at that point of the bin loop.  The loop covers the
+//     halo cells of the state too (my_ips_2h:my_ipe_2h, ...), so the kept
+//     boundary halo layers decay with it.
 //
 // P^b, the boundary-layer test and the decay factors are evaluated on the
 // host, with the same C library as the CPU restatement; the kernels do the
@@ -19,20 +21,9 @@
 #include <cuda_runtime.h>
 
 #include "f3d_common.cuh"
+#include "phys_dev.cuh"
 
 namespace f3d {
-
-struct WetArgs {
-  int nx, ny, nz, nb;
-  double dta;              // dt * a
-  const double* powpb;     // P^b per column, nx*ny
-  const int* ktop;         // cells k < ktop of the column are below the PBL top
-  const double* dx3p;      // dX3_p with the reference offset (kps-2)
-  double* awet;            // [bin][j][i]
-  double* c64;             // exact form state (or null)
-  float* c32;              // precision form state (or null)
-  unsigned long long mask; // bins that take wet deposition
-};
 
 __global__ void k_wet(WetArgs a) {
   const long long ncol = (long long)a.nx * a.ny;
@@ -62,18 +53,6 @@ __global__ void k_wet(WetArgs a) {
   }
 }
 
-struct RadioArgs {
-  int nx, ny, nz, nr;       // nr radionuclide bins, in bin order
-  int bin[64];              // their bin indices
-  int parent[64];           // Y90: bin index of the Sr90 parent, else -1
-  double fact[64];          // exp(-kn dt) of the bin
-  double pfact[64];         // exp(-kn dt) of the parent
-  double* c64;
-  float* c32;
-  double* acum;             // [bin][j][i]
-  double* awet;             // [bin][j][i] or null
-};
-
 template <class T>
 __device__ __forceinline__ void decay_cell(const RadioArgs& a, T* c, long long q, long long stride) {
   for (int r = 0; r < a.nr; ++r) {
@@ -85,15 +64,20 @@ __device__ __forceinline__ void decay_cell(const RadioArgs& a, T* c, long long q
 
 __global__ void k_radio(RadioArgs a) {
   const long long n2 = (long long)a.nx * a.ny, n3 = n2 * a.nz;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n3 + n2;
+  const long long ng = (a.gh64 || a.gh32) ? a.ngh : 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n3 + n2 + ng;
        e += (long long)gridDim.x * blockDim.x) {
     if (e < n3) {
       if (a.c64) decay_cell(a, a.c64, e, n3);
       else decay_cell(a, a.c32, e, n3);
-    } else {
+    } else if (e < n3 + n2) {
       const long long q = e - n3;
       decay_cell(a, a.acum, q, n2);
       if (a.awet) decay_cell(a, a.awet, q, n2);
+    } else {
+      const long long q = e - n3 - n2;
+      if (a.gh64) decay_cell(a, a.gh64, q, ng);
+      else decay_cell(a, a.gh32, q, ng);
     }
   }
 }

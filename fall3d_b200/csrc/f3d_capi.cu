@@ -13,6 +13,7 @@
 
 #include "../../include/fall3d_ads.h"
 #include "f3d_common.cuh"
+#include "phys_dev.cuh"
 
 namespace f3d {
 // ads_fp64.cu
@@ -53,30 +54,6 @@ void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, c
                           cudaStream_t st);
 void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
                          double* k3, cudaStream_t st);
-struct WetArgs {
-  int nx, ny, nz, nb;
-  double dta;
-  const double* powpb;
-  const int* ktop;
-  const double* dx3p;
-  double* awet;
-  double* c64;
-  float* c32;
-  unsigned long long mask;
-};
-struct RadioArgs {
-  int nx, ny, nz, nr;
-  int bin[64];
-  int parent[64];
-  double fact[64];
-  double pfact[64];
-  double* c64;
-  float* c32;
-  double* acum;
-  double* awet;
-};
-void launch_wet(const WetArgs& a, cudaStream_t st);
-void launch_radio(const RadioArgs& a, cudaStream_t st);
 int mlp_vset_field(f3d_mlp* h, const MemberDev* dm, int mi, int nx, int ny, int nz, int nb,
                    const double* drhoc, const double* dtc, const double* diam, const double* rhop,
                    const double* psi, const int* bin_cat, const int* is_aggregate, double vset_fac,
@@ -185,6 +162,10 @@ struct f3d_ctx {
   int* d_ktop = nullptr;        // levels below the boundary-layer top per column
   double* d_awet = nullptr;     // wet deposit [bin][j][i]
   unsigned long long wet_mask = 0;
+  double* d_zc = nullptr;       // corner heights for the output reductions
+  double* d_gh64 = nullptr;     // boundary halo layers (f3d_ads_keep_boundary_halo)
+  float* d_gh32 = nullptr;
+  double* d_out = nullptr;      // four (nx+1)(ny+1) output fields
   bool radio_on = false;
   std::vector<int> rad_bin, rad_parent;
   std::vector<double> rad_kn, rad_pkn;
@@ -674,6 +655,151 @@ extern "C" int f3d_ads_get_awet(f3d_ctx* c, double* my_awet) {
   return 0;
 }
 
+// Boundary halo layers <-> the reference's halo-inclusive state arrays: the
+// first halo cell at both ends of every pencil (both halo layers hold it
+// after a sweep, mod_ADS.F90:1246,1258,...).
+static void gh_gather(const f3d_ctx* c, const double* my_c, std::vector<double>& g) {
+  const long long nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb;
+  const long long X = nx + 4, Y = ny + 4, Z = nz + 4, per = gh_per_bin(c->nx, c->ny, c->nz);
+  g.assign((size_t)(per * nb), 0.0);
+  auto at = [&](long long i, long long j, long long k, long long b) {
+    return my_c[(i + 2) + X * ((j + 2) + Y * ((k + 2) + Z * b))];
+  };
+  for (long long b = 0; b < nb; ++b) {
+    double* gb = g.data() + b * per;
+    for (long long k = 0; k < nz; ++k)
+      for (long long j = 0; j < ny; ++j) {
+        gb[gh_offset(0, 0, k * ny + j, c->nx, c->ny, c->nz)] = at(-1, j, k, b);
+        gb[gh_offset(0, 1, k * ny + j, c->nx, c->ny, c->nz)] = at(nx, j, k, b);
+      }
+    for (long long k = 0; k < nz; ++k)
+      for (long long i = 0; i < nx; ++i) {
+        gb[gh_offset(1, 0, k * nx + i, c->nx, c->ny, c->nz)] = at(i, -1, k, b);
+        gb[gh_offset(1, 1, k * nx + i, c->nx, c->ny, c->nz)] = at(i, ny, k, b);
+      }
+    for (long long j = 0; j < ny; ++j)
+      for (long long i = 0; i < nx; ++i) {
+        gb[gh_offset(2, 0, j * nx + i, c->nx, c->ny, c->nz)] = at(i, j, -1, b);
+        gb[gh_offset(2, 1, j * nx + i, c->nx, c->ny, c->nz)] = at(i, j, nz, b);
+      }
+  }
+}
+
+static void gh_scatter(const f3d_ctx* c, const std::vector<double>& g, double* my_c) {
+  const long long nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb;
+  const long long X = nx + 4, Y = ny + 4, Z = nz + 4, per = gh_per_bin(c->nx, c->ny, c->nz);
+  auto at = [&](long long i, long long j, long long k, long long b) -> double& {
+    return my_c[(i + 2) + X * ((j + 2) + Y * ((k + 2) + Z * b))];
+  };
+  for (long long b = 0; b < nb; ++b) {
+    const double* gb = g.data() + b * per;
+    for (long long k = 0; k < nz; ++k)
+      for (long long j = 0; j < ny; ++j) {
+        at(-1, j, k, b) = at(-2, j, k, b) = gb[gh_offset(0, 0, k * ny + j, c->nx, c->ny, c->nz)];
+        at(nx, j, k, b) = at(nx + 1, j, k, b) = gb[gh_offset(0, 1, k * ny + j, c->nx, c->ny, c->nz)];
+      }
+    for (long long k = 0; k < nz; ++k)
+      for (long long i = 0; i < nx; ++i) {
+        at(i, -1, k, b) = at(i, -2, k, b) = gb[gh_offset(1, 0, k * nx + i, c->nx, c->ny, c->nz)];
+        at(i, ny, k, b) = at(i, ny + 1, k, b) = gb[gh_offset(1, 1, k * nx + i, c->nx, c->ny, c->nz)];
+      }
+    for (long long j = 0; j < ny; ++j)
+      for (long long i = 0; i < nx; ++i) {
+        at(i, j, -1, b) = at(i, j, -2, b) = gb[gh_offset(2, 0, j * nx + i, c->nx, c->ny, c->nz)];
+        at(i, j, nz, b) = at(i, j, nz + 1, b) = gb[gh_offset(2, 1, j * nx + i, c->nx, c->ny, c->nz)];
+      }
+  }
+}
+
+static int gh_upload(f3d_ctx* c, const std::vector<double>& g) {
+  MemberDev& m = c->hm;
+  if (m.gh64) {
+    CK(cudaMemcpy(m.gh64, g.data(), g.size() * 8, cudaMemcpyHostToDevice));
+  } else if (m.gh32) {
+    std::vector<float> t(g.size());
+    for (size_t q = 0; q < g.size(); ++q) t[q] = (float)g[q];
+    CK(cudaMemcpy(m.gh32, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+extern "C" int f3d_ads_keep_boundary_halo(f3d_ctx* c, int on) {
+  if (!c) return set_err("f3d_ads_keep_boundary_halo: null context");
+  CK(cudaSetDevice(c->device));
+  MemberDev& m = c->hm;
+  if (!on) {
+    m.gh64 = nullptr;  // the buffers stay with the context until it is destroyed
+    m.gh32 = nullptr;
+    return upload_member(c);
+  }
+  const size_t n = (size_t)gh_per_bin(c->nx, c->ny, c->nz) * c->nb;
+  if (c->prec == F3D_PREC_FP64) {
+    if (!c->d_gh64 && dalloc(c, &c->d_gh64, n)) return 1;
+    CK(cudaMemset(c->d_gh64, 0, n * 8));
+    m.gh64 = c->d_gh64;
+  } else {
+    if (!c->d_gh32 && dalloc(c, &c->d_gh32, n)) return 1;
+    CK(cudaMemset(c->d_gh32, 0, n * 4));
+    m.gh32 = c->d_gh32;
+  }
+  return upload_member(c);
+}
+
+extern "C" int f3d_ads_set_corner_heights(f3d_ctx* c, const double* z_c) {
+  if (!c || !z_c) return set_err("f3d_ads_set_corner_heights: null argument");
+  CK(cudaSetDevice(c->device));
+  const size_t n = (size_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+  if (!c->d_zc && dalloc(c, &c->d_zc, n)) return 1;
+  CK(cudaMemcpy(c->d_zc, z_c, n * 8, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+extern "C" int f3d_ads_output_species(f3d_ctx* c, const int* bin_in, int col_du, double* con_sur,
+                                      double* col_mass, double* cloud_top, double* grn_load) {
+  if (!c || !bin_in) return set_err("f3d_ads_output_species: null argument");
+  if (!c->grid_set) return set_err("f3d_ads_output_species: grid not set");
+  if (c->nb > 64) return set_err("f3d_ads_output_species: at most 64 bins");
+  if ((con_sur || col_mass || cloud_top) && !c->d_zc)
+    return set_err("f3d_ads_output_species: corner heights not set (f3d_ads_set_corner_heights)");
+  CK(cudaSetDevice(c->device));
+  const size_t ncol = (size_t)(c->nx + 1) * (c->ny + 1);
+  if (!c->d_out && dalloc(c, &c->d_out, 4 * ncol)) return 1;
+  MemberDev& m = c->hm;
+  OutArgs a;
+  a.nx = c->nx;
+  a.ny = c->ny;
+  a.nz = c->nz;
+  a.nb = c->nb;
+  a.mask = 0;
+  for (int q = 0; q < c->nb; ++q)
+    if (bin_in[q]) a.mask |= 1ull << q;
+  a.col_du = col_du;
+  a.c64 = m.c64;
+  a.c32 = m.c32;
+  a.acum = m.acum;
+  a.awet = c->d_awet;
+  a.hm1 = m.hm1;
+  a.hm2 = m.hm2;
+  a.hm3 = m.hm3;
+  a.zc = c->d_zc;
+  a.gh64 = m.gh64;
+  a.gh32 = m.gh32;
+  double* outs[4] = {con_sur, col_mass, cloud_top, grn_load};
+  double* dev[4];
+  for (int q = 0; q < 4; ++q) dev[q] = outs[q] ? c->d_out + q * ncol : nullptr;
+  a.con_sur = dev[0];
+  a.col_mass = dev[1];
+  a.cloud_top = dev[2];
+  a.grn_load = dev[3];
+  launch_out_columns(a, c->st);
+  c->launches += 1;
+  CKL();
+  for (int q = 0; q < 4; ++q)
+    if (outs[q]) CK(cudaMemcpyAsync(outs[q], dev[q], ncol * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
 extern "C" int f3d_ads_set_source(f3d_ctx* c, int n, const int* ijk, const double* s) {
   if (!c) return set_err("f3d_ads_set_source: null context");
   if (n < 0 || (n > 0 && (!ijk || !s))) return set_err("f3d_ads_set_source: bad arguments");
@@ -756,6 +882,11 @@ extern "C" int f3d_ads_upload_state(f3d_ctx* c, const double* my_c, const double
     }
   }
   if (my_acum && upload_conv(c, 8, my_acum, (nx + 4) * (ny + 4) * nb, m.acum)) return 1;
+  if (my_c && (m.gh64 || m.gh32)) {
+    std::vector<double> g;
+    gh_gather(c, my_c, g);
+    if (gh_upload(c, g)) return 1;
+  }
   return 0;
 }
 
@@ -805,6 +936,17 @@ extern "C" int f3d_ads_download_state(f3d_ctx* c, double* my_c, double* my_acum)
             my_c[(i + 2) + X * ((j + 2) + Y * ((nz + 2 + g) + Z * b))] = hi;
           }
         }
+    if (m.gh64 || m.gh32) {  // the kept boundary halo layers replace the zero-gradient ghosts
+      std::vector<double> g((size_t)gh_per_bin(c->nx, c->ny, c->nz) * nb);
+      if (m.gh64) {
+        CK(cudaMemcpy(g.data(), m.gh64, g.size() * 8, cudaMemcpyDeviceToHost));
+      } else {
+        std::vector<float> t(g.size());
+        CK(cudaMemcpy(t.data(), m.gh32, t.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < t.size(); ++q) g[q] = t[q];
+      }
+      gh_scatter(c, g, my_c);
+    }
   }
   if (my_acum) {
     std::vector<double> tmp(nx * ny * nb);
@@ -891,6 +1033,9 @@ static int enqueue_wet_radio(f3d_ctx* c, double dt) {
     r.c32 = m.c32;
     r.acum = m.acum;
     r.awet = c->wet_on ? c->d_awet : nullptr;
+    r.gh64 = m.gh64;
+    r.gh32 = m.gh32;
+    r.ngh = gh_per_bin(c->nx, c->ny, c->nz);
     launch_radio(r, c->st);
     c->launches += 1;
     CKL();

@@ -96,7 +96,26 @@ struct MemberDev {
   int part_count[3];  // number of partial slots (blocks) per direction
   double* flux_tot;   // running totals {W,E,S,N,U,D} and compensations [12]
   double* flux_step;  // this step's increments {W,E,S,N,U,D}
+  // boundary halo layers (null unless kept): the free-flow ghost value each
+  // sweep puts in the first halo cell at both ends of its pencils, laid out
+  // per bin as gh_offset() gives (exact form gh64, precision form gh32)
+  double* gh64;
+  float* gh32;
 };
+
+// Boundary halo layers of one bin: x sweep W, E [k][j]; y sweep S, N [k][i];
+// z sweep D, U [j][i].  Element of pencil pen (the sweep's spatial pencil
+// index) on side s (0 low, 1 high) of direction dir:
+__host__ __device__ __forceinline__ long long gh_per_bin(int nx, int ny, int nz) {
+  return 2LL * ((long long)ny * nz + (long long)nx * nz + (long long)nx * ny);
+}
+__host__ __device__ __forceinline__ long long gh_offset(int dir, int side, long long pen, int nx, int ny,
+                                                        int nz) {
+  const long long ax = (long long)ny * nz, ay = (long long)nx * nz, az = (long long)nx * ny;
+  const long long base = (dir == 0) ? 0 : (dir == 1) ? 2 * ax : 2 * (ax + ay);
+  const long long n = (dir == 0) ? ax : (dir == 1) ? ay : az;
+  return base + side * n + pen;
+}
 
 // A block of one sweep: 32 consecutive spatial pencils [pen0, pen0+32) of
 // one member, one warp per bin [bin0, bin0 + blockDim/32).  Spatial pencil

@@ -131,6 +131,33 @@ int f3d_ads_set_radionuclides(f3d_ctx *ctx, const int *bin_cat,
 /* MY_TRA%my_awet(ips-2:ipe+2, jps-2:jpe+2, nbins), halos zero. */
 int f3d_ads_get_awet(f3d_ctx *ctx, double *my_awet);
 
+/* Keep (on != 0) the state's boundary halo layers on the device: the
+ * free-flow ghost value each sweep writes into the first halo cell at both
+ * ends of its pencils (freeflow, mod_ADS.F90:1227-1326, applied to MY_TRA%my_c
+ * at :270, :460, :676), decayed with the state by phys_radionuclides.  The
+ * output reductions read them at the domain edges, f3d_ads_upload_state takes
+ * them from the halo of my_c and f3d_ads_download_state returns them there.
+ * Off (the default), the halo reads as zero in the output reductions. */
+int f3d_ads_keep_boundary_halo(f3d_ctx *ctx, int on);
+/* Heights of the cell corners MY_GRID%z_c(ibs:ibe,jbs:jbe,kbs:kbe), for the
+ * output reductions. */
+int f3d_ads_set_corner_heights(f3d_ctx *ctx, const double *z_c);
+/* The per-species reductions of nc_IO_out_res (mod_nc_IO.F90:3206-4335) on
+ * the device, at the cell corners (ibs:ibe, jbs:jbe), Fortran order:
+ *   CON_SUR   surface concentration, g/m3 (:3624-3633)
+ *   COL_MASS  column load, g/m2, or DU when col_du != 0 (SO2, :3682-3703)
+ *   CLOUD_TOP z_c of the highest corner above 50 ug/m3, else 0 (:3828-3858)
+ *   GRN_LOAD  dry + wet deposit, kg/m2 (:3428-3446, :3909-3920)
+ * from 1e3 c/(Hm1 Hm2 Hm3) clipped at 0 and averaged to corners as grid_p2c
+ * and grid_p2c_2D do (mod_Grid.F90:1150-1220).  bin_in[nbins] selects the
+ * bins summed: those of the species, or of the species with diameter <= PM
+ * for the PMxx column loads (:3753-3777).  Any output may be NULL.  Mass
+ * points outside the domain are the state's halo: the kept boundary halo
+ * layers (f3d_ads_keep_boundary_halo), else zero. */
+int f3d_ads_output_species(f3d_ctx *ctx, const int *bin_in, int col_du,
+                           double *con_sur, double *col_mass,
+                           double *cloud_top, double *grn_load);
+
 /* Source term MY_TRA%my_s(ips:ipe,jps:jpe,kps:kpe,nbins) after
  * F3D_set_source_term (mod_F3D.F90:349-555), given sparsely: n cells with
  * 1-based Fortran indices ijk[3*q+0..2] and values s[nbins*q + bin] (the
