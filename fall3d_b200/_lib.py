@@ -39,6 +39,9 @@ SIGNATURES = {
     "f3d_ads_get_awet": [_vp, _dp],
     "f3d_ads_set_corner_heights": [_vp, _dp],
     "f3d_ads_keep_boundary_halo": [_vp, C.c_int],
+    "f3d_ads_set_gravity_current": [_vp, _dp, _dp, _dp, _dp, _dp, _dp],
+    "f3d_ads_gravity_current_time_step": [_vp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double,
+                                          _ip, _dp, _dp, _dp],
     "f3d_ads_output_species": [_vp, _ip, C.c_int, _dp, _dp, _dp, _dp],
     "f3d_ads_set_meteo_corners": [_vp] + [_dp] * 6 + [C.c_double] * 4,
     "f3d_ads_set_source": [_vp, C.c_int, _ip, _dp],

@@ -139,6 +139,38 @@ class Domain:
         check(lib().f3d_ads_get_awet(self._h, _p(aw)), "f3d_ads_get_awet")
         return aw
 
+    def _ensure_corner_heights(self):
+        if not getattr(self, "_zc_set", False):
+            zc = np.asfortranarray(self.grid.z_c, dtype=np.float64)
+            check(lib().f3d_ads_set_corner_heights(self._h, _p(zc)), "f3d_ads_set_corner_heights")
+            self._zc_set = True
+
+    def set_gravity_current(self, lon, lat, start_time, end_time, c_flow_rate, k_entrain, brunt_vaisala,
+                            lambda_grav, mass_flow_rate, h_tot, input_min_radius=0.0):
+        """MY_MOD%MY_GC for F3D_add_radial_wind (mod_F3D.F90:978-1226): every
+        later F3D_time_step inside [start_time, end_time] adds the radial wind."""
+        g = self.grid
+        self._ensure_corner_heights()
+        p = np.array([lon, lat, start_time, end_time, c_flow_rate, k_entrain, brunt_vaisala, lambda_grav,
+                      mass_flow_rate, h_tot, input_min_radius], dtype=np.float64)
+        xy = [np.ascontiguousarray(getattr(g, n), dtype=np.float64) for n in
+              ("lon_c", "lat_c", "lon_p", "lat_p", "Hm1_c")]
+        check(lib().f3d_ads_set_gravity_current(self._h, _p(p), *[_p(a) for a in xy]),
+              "f3d_ads_set_gravity_current")
+
+    def gravity_current_time_step(self, time, stime, criterion=2, cfl=0.9, run_end=1e30):
+        """(active, my_dt, gl_dt, state): the update_step time step of a
+        gravity-current step (mod_F3D.F90:1443-1452); state = (vol_flow_rate,
+        min_radius, radius_grav, c_grav_factor, th_grav, hmin, hmax)."""
+        act = C.c_int()
+        a, b = C.c_double(), C.c_double()
+        st = np.zeros(7)
+        check(lib().f3d_ads_gravity_current_time_step(self._h, float(time), float(stime), int(criterion),
+                                                      float(cfl), float(run_end), C.byref(act), C.byref(a),
+                                                      C.byref(b), _p(st)),
+              "f3d_ads_gravity_current_time_step")
+        return bool(act.value), a.value, b.value, st
+
     def keep_boundary_halo(self, on=True):
         """Keep the state's boundary halo layers (the free-flow ghosts the
         sweeps write, mod_ADS.F90:1227-1326) for the output reductions and
@@ -152,10 +184,7 @@ class Domain:
         bins: indices of the bins summed (a species, or its bins below a PM
         diameter for the PMxx column loads)."""
         g = self.grid
-        if not getattr(self, "_zc_set", False):
-            check(lib().f3d_ads_set_corner_heights(self._h, _p(np.asfortranarray(g.z_c, dtype=np.float64))),
-                  "f3d_ads_set_corner_heights")
-            self._zc_set = True
+        self._ensure_corner_heights()
         sel = np.zeros(self.nbins, np.int32)
         sel[list(bins)] = 1
         keys = ("con_sur", "col_mass", "cloud_top", "grn_load")

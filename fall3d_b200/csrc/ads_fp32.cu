@@ -208,6 +208,15 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
     o.s1 = (float)m.stime;
     o.s0 = 1.f - o.s1;
     o.wfac = m.wfac;
+    if (DIR != DIR_Z && m.gc_cur) {  // current winds precomputed: u = fmaf(1, u, 0 * u)
+      const float* cur = (DIR == DIR_X) ? m.ucur32 : m.vcur32;
+      const long long fo = o.v1 - ((DIR == DIR_X) ? m.ux32[0] : m.vy32[0]);
+      o.v1 = cur + fo;
+      o.v2 = cur + fo;
+      o.s0 = 1.f;
+      o.s1 = 0.f;
+      o.wfac = 1.f;
+    }
     o.dt = (float)dt;
     o.hdt = 0.5f * o.dt;
     o.dt3 = o.dt * (1.f / 3.f);

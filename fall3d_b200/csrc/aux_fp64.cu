@@ -5,10 +5,12 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "f3d_common.cuh"
 #include "step_dev.cuh"
 #include "vset.cuh"
+#include "phys_dev.cuh"
 
 namespace f3d {
 
@@ -319,7 +321,7 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
 }
 
 __global__ void k_cfl(const MemberDev* __restrict__ members, int mi, double s, int criterion,
-                      double* out3) {
+                      double* out3, GcArgs gc) {
   const MemberDev& m = members[mi];
   const int nx = m.nx, ny = m.ny, nz = m.nz, nb = m.nb;
   const long long tot = (long long)nx * ny * nz;
@@ -336,6 +338,11 @@ __global__ void k_cfl(const MemberDev* __restrict__ members, int mi, double s, i
     double u = (1.0 - s) * (f * m.ux[0][iu]) + s * (f * m.ux[1][iu]);
     double v = (1.0 - s) * (f * m.vy[0][iv]) + s * (f * m.vy[1][iv]);
     double w = (1.0 - s) * m.wz[0][iw] + s * m.wz[1][iw];
+    if (gc.on) {  // the winds the step uses, with the radial wind (mod_F3D.F90:1443-1452)
+      double r;
+      if (gc_rvel_u(gc, nx, ny, i, j, k, &r)) u = u + r;
+      if (gc_rvel_v(gc, nx, ny, i, j, k, &r)) v = v + r;
+    }
     double k1 = m.k1x[((long long)k * (nx + 2) + (i + 1)) * ny + j];
     double k2 = m.k2y[((long long)k * (ny + 2) + (j + 1)) * nx + i];
     double k3 = m.k3z[((long long)(k + 1) * ny + j) * nx + i];
@@ -366,8 +373,11 @@ __global__ void k_cfl(const MemberDev* __restrict__ members, int mi, double s, i
   }
 }
 void launch_cfl(const MemberDev* members, int mi, double s, int criterion, double* out3,
-                cudaStream_t st) {
-  k_cfl<<<1184, 256, 0, st>>>(members, mi, s, criterion, out3);
+                cudaStream_t st, const GcArgs* gc) {
+  GcArgs g;
+  memset(&g, 0, sizeof(g));
+  if (gc) g = *gc;
+  k_cfl<<<1184, 256, 0, st>>>(members, mi, s, criterion, out3, g);
 }
 
 // ---- mass in the volume: grid_get_mass_volume (mod_Grid.F90:1340-1389) ------

@@ -15,6 +15,7 @@
 
 #include "../../include/fall3d_ads.h"
 #include "f3d_common.cuh"
+#include "phys_dev.cuh"
 #include "step_dev.cuh"
 
 namespace f3d {
@@ -31,7 +32,7 @@ void launch_conv(int which, const double* in, double* out, int nx, int ny, int n
                  cudaStream_t st);
 void launch_flux_reduce(const MemberDev* members, int nmembers, int dirmask, cudaStream_t st);
 void launch_cfl(const MemberDev* members, int mi, double s, int criterion, double* out3,
-                cudaStream_t st);
+                cudaStream_t st, const GcArgs* gc = nullptr);
 void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* partials, int nblk,
                  double* out, cudaStream_t st);
 void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc,

@@ -31,7 +31,7 @@ void launch_set_dt_stime(MemberDev* members, int mi, double dt, double stime, cu
 void launch_flux_reduce(const MemberDev* members, int nmembers, int dirmask, cudaStream_t st);
 void launch_zero_step(const MemberDev* members, int nmembers, cudaStream_t st);
 void launch_cfl(const MemberDev* members, int mi, double s, int criterion, double* out3,
-                cudaStream_t st);
+                cudaStream_t st, const GcArgs* gc = nullptr);
 void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* partials, int nblk,
                  double* out, cudaStream_t st);
 void launch_vset_points(int model, int n, const double* diam, const double* rhop,
@@ -54,6 +54,8 @@ void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, c
                           cudaStream_t st);
 void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
                          double* k3, cudaStream_t st);
+void launch_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, int fp32, const GcArgs& g,
+                     cudaStream_t st);
 int mlp_vset_field(f3d_mlp* h, const MemberDev* dm, int mi, int nx, int ny, int nz, int nb,
                    const double* drhoc, const double* dtc, const double* diam, const double* rhop,
                    const double* psi, const int* bin_cat, const int* is_aggregate, double vset_fac,
@@ -163,6 +165,10 @@ struct f3d_ctx {
   double* d_awet = nullptr;     // wet deposit [bin][j][i]
   unsigned long long wet_mask = 0;
   double* d_zc = nullptr;       // corner heights for the output reductions
+  bool gc_set = false;          // gravity current (f3d_ads_set_gravity_current)
+  double gc_p[11] = {};
+  std::vector<double> gc_host;  // lon_c, lat_c, lon_p, lat_p, Hm1_c
+  double* d_gc_xy = nullptr;    // the same on the device
   double* d_gh64 = nullptr;     // boundary halo layers (f3d_ads_keep_boundary_halo)
   float* d_gh32 = nullptr;
   double* d_out = nullptr;      // four (nx+1)(ny+1) output fields
@@ -745,6 +751,135 @@ extern "C" int f3d_ads_keep_boundary_halo(f3d_ctx* c, int on) {
   return upload_member(c);
 }
 
+static int check_ready(f3d_ctx* c, const char* who);
+
+// ---- gravity current: F3D_add_radial_wind (mod_F3D.F90:978-1226) ----------
+// The scalars of the current for a time, on the host with the C library's
+// sqrt and pow (mod_F3D.F90:1026-1070).  Returns false where the routine
+// returns early (outside [start_time, end_time] or no mass flow).
+static bool gc_args(const f3d_ctx* c, double time, GcArgs* g, double st[7]) {
+  const double* p = c->gc_p;
+  const double PI = 4.0 * std::atan(1.0), REARTH = 6356000.0;  // mod_KindType.F90:43-44
+  memset(g, 0, sizeof(*g));
+  for (int q = 0; q < 7; ++q) st[q] = 0.0;
+  if (!c->gc_set) return false;
+  if (time < p[2] || time > p[3] || p[8] <= 0.0) return false;
+  const double* lon_c = c->gc_host.data();          // layout of f3d_ads_set_gravity_current
+  const double* lat_c = lon_c + (c->nx + 1);
+  const double* hm1_c = lat_c + (c->ny + 1) + c->nx + c->ny;
+  double deltax = REARTH * hm1_c[0] * (lon_c[0] - lon_c[1]) * PI / 180.0;
+  double deltay = REARTH * (lat_c[0] - lat_c[1]) * PI / 180.0;
+  double radius = 1.5 * std::sqrt(deltax * deltax + deltay * deltay);
+  double min_radius = radius;  // parallel_max over one rank
+  if (p[10] > 0.0) min_radius = p[10];
+  const double c_flow_rate = p[4], k_entrain = p[5], brunt_vaisala = p[6], lambda_grav = p[7],
+               mass_flow_rate = p[8], h_tot = p[9];
+  const double tse = time - p[2];
+  const double vol_flow_rate = c_flow_rate * std::sqrt(k_entrain) * std::pow(mass_flow_rate, 0.75) /
+                               std::pow(brunt_vaisala, 1.25);
+  const double c_gravr = 3.0 * lambda_grav * brunt_vaisala * vol_flow_rate / (2.0 * PI);
+  double radius_grav = std::pow(c_gravr * (tse * tse), 0.33333);
+  radius_grav = std::fmax(radius_grav, min_radius);
+  const double c_gravu = std::sqrt(2.0 * lambda_grav * brunt_vaisala * vol_flow_rate / (3.0 * PI));
+  const double c_grav_factor = 0.75 * c_gravu * std::sqrt(radius_grav);
+  const double th_grav = c_gravu / (std::sqrt(radius_grav) * lambda_grav * brunt_vaisala);
+  const double h_umbr = h_tot / 1.2;
+  const double hmin = std::fmax(h_umbr - 0.5 * th_grav, 0.5 * h_tot);
+  const double hmax = std::fmin(h_umbr + 0.5 * th_grav, h_tot);
+  g->on = 1;
+  g->xc = p[0];
+  g->yc = p[1];
+  g->rearth = REARTH;
+  g->pi = PI;
+  g->min_radius = min_radius;
+  g->radius_grav = radius_grav;
+  g->c_grav_factor = c_grav_factor;
+  g->hmin = hmin;
+  g->hmax = hmax;
+  g->lon_c = c->d_gc_xy;
+  g->lat_c = g->lon_c + (c->nx + 1);
+  g->lon_p = g->lat_c + (c->ny + 1);
+  g->lat_p = g->lon_p + c->nx;
+  g->hm1_c = g->lat_p + c->ny;
+  g->hm1_p = c->hm.hm1;
+  g->zc = c->d_zc;
+  st[0] = vol_flow_rate;
+  st[1] = min_radius;
+  st[2] = radius_grav;
+  st[3] = c_grav_factor;
+  st[4] = th_grav;
+  st[5] = hmin;
+  st[6] = hmax;
+  return true;
+}
+
+extern "C" int f3d_ads_set_gravity_current(f3d_ctx* c, const double params[11], const double* lon_c,
+                                           const double* lat_c, const double* lon_p,
+                                           const double* lat_p, const double* Hm1_c) {
+  if (!c || !params) return set_err("f3d_ads_set_gravity_current: null argument");
+  if (!c->grid_set) return set_err("f3d_ads_set_gravity_current: grid not set");
+  if (!c->d_zc)
+    return set_err("f3d_ads_set_gravity_current: corner heights not set (f3d_ads_set_corner_heights)");
+  CK(cudaSetDevice(c->device));
+  const size_t n = (size_t)(c->nx + 1) + (c->ny + 1) + c->nx + c->ny + (c->ny + 1);
+  if (lon_c || lat_c || lon_p || lat_p || Hm1_c) {
+    if (!lon_c || !lat_c || !lon_p || !lat_p || !Hm1_c)
+      return set_err("f3d_ads_set_gravity_current: give all five coordinate arrays");
+    c->gc_host.resize(n);
+    double* h = c->gc_host.data();
+    const size_t o_lat_c = c->nx + 1, o_lon_p = o_lat_c + c->ny + 1, o_lat_p = o_lon_p + c->nx,
+                 o_hm1_c = o_lat_p + c->ny;
+    memcpy(h, lon_c, (c->nx + 1) * 8);
+    memcpy(h + o_lat_c, lat_c, (c->ny + 1) * 8);
+    memcpy(h + o_lon_p, lon_p, c->nx * 8);
+    memcpy(h + o_lat_p, lat_p, c->ny * 8);
+    memcpy(h + o_hm1_c, Hm1_c, (c->ny + 1) * 8);
+    if (!c->d_gc_xy && dalloc(c, &c->d_gc_xy, n)) return 1;
+    CK(cudaMemcpy(c->d_gc_xy, h, n * 8, cudaMemcpyHostToDevice));
+  } else if (c->gc_host.size() != n) {
+    return set_err("f3d_ads_set_gravity_current: coordinates not given");
+  }
+  if (c->prec == F3D_PREC_FP32 && !c->hm.ucur32) {
+    MemberDev& m = c->hm;
+    if (dalloc(c, &m.ucur32, (size_t)(c->nx + 1) * c->ny * c->nz) ||
+        dalloc(c, &m.vcur32, (size_t)(c->ny + 1) * c->nx * c->nz))
+      return 1;
+    if (upload_member(c)) return 1;
+  }
+  memcpy(c->gc_p, params, sizeof(c->gc_p));
+  c->gc_set = true;
+  return 0;
+}
+
+extern "C" int f3d_ads_gravity_current_time_step(f3d_ctx* c, double time, double stime,
+                                                 int criterion, double cfl, double run_end,
+                                                 int* active, double* my_dt, double* gl_dt,
+                                                 double state[7]) {
+  if (check_ready(c, "f3d_ads_gravity_current_time_step")) return 1;
+  if (!active || !my_dt || !gl_dt)
+    return set_err("f3d_ads_gravity_current_time_step: null output");
+  if (criterion != 1 && criterion != 2)
+    return set_err("f3d_ads_gravity_current_time_step: criterion %d not in 1..2", criterion);
+  GcArgs g;
+  double st[7];
+  *active = gc_args(c, time, &g, st) ? 1 : 0;
+  if (state)
+    for (int q = 0; q < 7; ++q) state[q] = st[q];
+  if (!*active) return 0;
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemsetAsync(c->d_red, 0, 3 * sizeof(double), c->st));
+  launch_cfl(c->dm, 0, stime, criterion, c->d_red, c->st, &g);
+  CKL();
+  CK(cudaMemcpyAsync(c->h_pin, c->d_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double m = std::max(std::max(c->h_pin[0], c->h_pin[1]), c->h_pin[2]);  // mod_Grid.F90:1125-1127
+  if (m > 0.0) m = 1.0 / m;
+  m = cfl * m;
+  *my_dt = std::min(m, run_end);
+  *gl_dt = std::min(m, run_end);
+  return 0;
+}
+
 extern "C" int f3d_ads_set_corner_heights(f3d_ctx* c, const double* z_c) {
   if (!c || !z_c) return set_err("f3d_ads_set_corner_heights: null argument");
   CK(cudaSetDevice(c->device));
@@ -1047,10 +1182,27 @@ static int enqueue_step(f3d_ctx* c, double dt, double time, int iiter) {
   // event slots: 0 start, 1 after prep+source, 2..4 after the 1st/2nd/z sweep, 5 end
   auto rec = [&](int k) { if (c->prof) cudaEventRecord(c->ev[k], c->st); };
   rec(0);
+  // gravity current at this time; the precision form's sweeps are switched to
+  // the precomputed winds before the step's parameters are set on the device
+  // (the descriptor upload carries the host's copy of dt and stime)
+  GcArgs gc;
+  double gst[7];
+  const bool gc_on = c->gc_set && gc_args(c, time, &gc, gst);
+  const int fp32 = c->prec == F3D_PREC_FP32;
+  if (fp32 && c->hm.gc_cur != (gc_on ? 1 : 0)) {
+    c->hm.gc_cur = gc_on ? 1 : 0;
+    if (upload_member(c)) return 1;
+  }
   launch_set_step(c->dm, 0, dt, time, iiter, c->st);
   c->launches += 1;
   CKL();
-  if (enqueue_prep(c, 7) || enqueue_source(c)) return 1;
+  if (enqueue_prep(c, 7)) return 1;
+  if (gc_on) {  // F3D_add_radial_wind on the interpolated winds (mod_F3D.F90:1443-1445)
+    launch_gc_winds(c->dm, 0, c->nx, c->ny, c->nz, fp32, gc, c->st);
+    c->launches += 1;
+    CKL();
+  }
+  if (enqueue_source(c)) return 1;
   rec(1);
   const bool xfirst = (iiter % 2 == 0);  // mod_F3D.F90:1477-1487
   if (enqueue_sweep(c, xfirst ? DIR_X : DIR_Y)) return 1;

@@ -89,7 +89,9 @@ struct MemberDev {
   double time;
   double t_its, t_ite;
   int iiter;
-  int pad0;
+  int gc_cur;  // precision form: the x and y sweeps read this step's current
+               // winds from ucur32/vcur32 (gravity current) instead of
+               // interpolating the snapshots
   // flux bookkeeping
   double* flux_part;  // per-block partial sums, [slot][2]
   int part_base[3];   // first partial slot of this member for x, y, z

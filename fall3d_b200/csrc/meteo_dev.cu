@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include "f3d_common.cuh"
+#include "phys_dev.cuh"
 
 namespace f3d {
 
@@ -187,6 +188,51 @@ void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, c
   k_met_k1<<<592, 256, 0, st>>>(g, k1, k1x);
   k_met_k2<<<592, 256, 0, st>>>(g, k2, k2y);
   k_met_k3<<<592, 256, 0, st>>>(g, k1, k2, k3, k3z);
+}
+
+// Current winds of a step with the gravity current's radial wind
+// (mod_F3D.F90:1437-1445): the exact form adds rvel to the interpolated
+// winds the prep kernel wrote (my_u = my_u + rvel, :1171, :1208); the
+// precision form writes the interpolated FP64 wind plus rvel, rounded to
+// FP32, for the sweeps to read in place of their own interpolation.
+__global__ void k_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, int fp32, GcArgs g) {
+  MemberDev& m = members[mi];
+  const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)(ny + 1) * nx * nz;
+  const double s = m.stime, f = m.wfacd;
+  MGRID(e, nu + nv) {
+    double rvel = 0.0;
+    if (e < nu) {
+      const int j = (int)(e % ny);
+      const long long t = e / ny;
+      const int i = (int)(t % (nx + 1)), k = (int)(t / (nx + 1));
+      const bool add = gc_rvel_u(g, nx, ny, i, j, k, &rvel);
+      if (!fp32) {
+        if (add) m.ucur[e] = m.ucur[e] + rvel;
+      } else {
+        double u = (1.0 - s) * (f * m.ux[0][e]) + s * (f * m.ux[1][e]);
+        if (add) u = u + rvel;
+        m.ucur32[e] = (float)u;
+      }
+    } else {
+      const long long q = e - nu;
+      const int i = (int)(q % nx);
+      const long long t = q / nx;
+      const int j = (int)(t % (ny + 1)), k = (int)(t / (ny + 1));
+      const bool add = gc_rvel_v(g, nx, ny, i, j, k, &rvel);
+      if (!fp32) {
+        if (add) m.vcur[q] = m.vcur[q] + rvel;
+      } else {
+        double v = (1.0 - s) * (f * m.vy[0][q]) + s * (f * m.vy[1][q]);
+        if (add) v = v + rvel;
+        m.vcur32[q] = (float)v;
+      }
+    }
+  }
+}
+
+void launch_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, int fp32, const GcArgs& g,
+                     cudaStream_t st) {
+  k_gc_winds<<<592, 256, 0, st>>>(members, mi, nx, ny, nz, fp32, g);
 }
 
 void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,

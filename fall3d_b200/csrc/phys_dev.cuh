@@ -4,6 +4,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "f3d_common.cuh"
+
 namespace f3d {
 
 // wet deposition, phys_wet_deposition (mod_Phys.F90:1358-1427)
@@ -56,8 +58,64 @@ struct OutArgs {
   double* grn_load;
 };
 
+// gravity current, F3D_add_radial_wind (mod_F3D.F90:978-1226): the radial
+// wind of one time, added to the current winds in the layer [hmin, hmax]
+// within radius_grav of the centre (xc, yc).  The scalars are evaluated on
+// the host for the step's time.
+struct GcArgs {
+  int on;
+  double xc, yc;
+  double rearth, pi;  // REARTH, PI (mod_KindType.F90:43-44)
+  double min_radius, radius_grav, c_grav_factor, hmin, hmax;
+  const double* lon_c;  // ibs:ibe
+  const double* lat_c;  // jbs:jbe
+  const double* lon_p;  // ips:ipe
+  const double* lat_p;  // jps:jpe
+  const double* hm1_p;  // jps:jpe
+  const double* hm1_c;  // jbs:jbe
+  const double* zc;     // corner heights (nx+1)(ny+1)(nz+1)
+};
+
+// rvel of the radial wind at a face of the given offsets (mod_F3D.F90:1148-1164
+// for x faces, :1186-1202 for y faces); false where the routine skips it.
+// Written operation by operation as the reference evaluates it (compile the
+// caller with --fmad=false).
+__device__ __forceinline__ bool gc_rvel(const GcArgs& g, double hm1, double dlon, double dlat,
+                                        bool xface, double* rvel) {
+  const double deltax = g.rearth * hm1 * dlon * g.pi / 180.0;
+  const double deltay = g.rearth * dlat * g.pi / 180.0;
+  double radius = sqrt(deltax * deltax + deltay * deltay);
+  if (radius > g.radius_grav) return false;
+  double fu;
+  if (radius < 1e-3) fu = 0.0;
+  else fu = xface ? deltax / radius / hm1 : deltay / radius;
+  radius = fmax(radius, g.min_radius);
+  *rvel = fu * g.c_grav_factor / radius *
+          (1.0 + radius * radius / (3.0 * (g.radius_grav * g.radius_grav)));
+  return true;
+}
+
+// x face i (0..nx) of mass row j, level k
+__device__ __forceinline__ bool gc_rvel_u(const GcArgs& g, int nx, int ny, int i, int j, int k,
+                                          double* rvel) {
+  const double zp = g.zc[i + (long long)(nx + 1) * (j + (long long)(ny + 1) * k)];
+  if (!(zp >= g.hmin && zp <= g.hmax)) return false;
+  return gc_rvel(g, g.hm1_p[j], g.lon_c[i] - g.xc, g.lat_p[j] - g.yc, true, rvel);
+}
+
+// y face j (0..ny) of mass column i, level k
+__device__ __forceinline__ bool gc_rvel_v(const GcArgs& g, int nx, int ny, int i, int j, int k,
+                                          double* rvel) {
+  const double zp = g.zc[i + (long long)(nx + 1) * (j + (long long)(ny + 1) * k)];
+  if (!(zp >= g.hmin && zp <= g.hmax)) return false;
+  return gc_rvel(g, g.hm1_c[j], g.lon_p[i] - g.xc, g.lat_c[j] - g.yc, false, rvel);
+}
+
 void launch_wet(const WetArgs& a, cudaStream_t st);
 void launch_radio(const RadioArgs& a, cudaStream_t st);
 void launch_out_columns(const OutArgs& a, cudaStream_t st);
+// current winds of the step with the radial wind (meteo_dev.cu)
+void launch_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, int fp32, const GcArgs& g,
+                     cudaStream_t st);
 
 }  // namespace f3d

@@ -131,6 +131,31 @@ int f3d_ads_set_radionuclides(f3d_ctx *ctx, const int *bin_cat,
 /* MY_TRA%my_awet(ips-2:ipe+2, jps-2:jpe+2, nbins), halos zero. */
 int f3d_ads_get_awet(f3d_ctx *ctx, double *my_awet);
 
+/* Gravity current, F3D_add_radial_wind (mod_F3D.F90:978-1226).  params =
+ * MY_MOD%MY_GC {lon, lat, start_time, end_time, c_flow_rate, k_entrain,
+ * brunt_vaisala, lambda, mass_flow_rate, h_tot, input_min_radius}; the
+ * coordinates MY_GRID%lon_c(ibs:ibe), lat_c(jbs:jbe), lon_p(ips:ipe),
+ * lat_p(jps:jpe), Hm1_c(jbs:jbe) (all five, or all NULL to keep the ones
+ * given before, e.g. when only mass_flow_rate changes).  Needs the corner
+ * heights (f3d_ads_set_corner_heights).  From then on every f3d_ads_step at a
+ * time inside [start_time, end_time] with mass_flow_rate > 0 adds the radial
+ * wind to the interpolated u and v before its sweeps (:1443-1445). */
+int f3d_ads_set_gravity_current(f3d_ctx *ctx, const double params[11],
+                                const double *lon_c, const double *lat_c,
+                                const double *lon_p, const double *lat_p,
+                                const double *Hm1_c);
+/* The update_step time step of a gravity-current step (mod_F3D.F90:1449-1452):
+ * *active = 1 when the current acts at `time`, and then my_dt, gl_dt are
+ * grid_get_time_step on the winds that step uses (interpolated at stime, with
+ * the radial wind).  *active = 0 leaves them untouched.  state (may be NULL)
+ * gets {vol_flow_rate, min_radius, radius_grav, c_grav_factor, th_grav, hmin,
+ * hmax}, the values the reference stores in MY_MOD%MY_GC. */
+int f3d_ads_gravity_current_time_step(f3d_ctx *ctx, double time, double stime,
+                                      int criterion, double cfl,
+                                      double run_end, int *active,
+                                      double *my_dt, double *gl_dt,
+                                      double state[7]);
+
 /* Keep (on != 0) the state's boundary halo layers on the device: the
  * free-flow ghost value each sweep writes into the first halo cell at both
  * ends of its pencils (freeflow, mod_ADS.F90:1227-1326, applied to MY_TRA%my_c

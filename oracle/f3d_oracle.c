@@ -326,18 +326,25 @@ void or_solve_z(const or_dims *d, const or_grid *g, double dt, double *c,
 }
 
 /* ---- F3D_time_step body: mod_F3D.F90:1435-1491 */
-void or_time_step(const or_dims *d, const or_grid *g, double dt, double time,
-                  double t_its, double t_ite, int iiter, double *c,
-                  double *acum, const double *s, const double *u12,
-                  const double *v12, const double *w12, const double *k1,
-                  const double *k2, const double *k3, const double *vs,
-                  double fluxes[6], int nthreads) {
+double or_current_winds(const or_dims *d, double time, double t_its,
+                        double t_ite, const double *u12, const double *v12,
+                        const double *w12, double *u, double *v, double *w) {
   const size_t nu = n_u(d), nv = n_v(d), nw = n_w(d);
-  double s_time = (time - t_its) / (t_ite - t_its);
-  double *u = (double *)malloc(sizeof(double) * nu);
-  double *v = (double *)malloc(sizeof(double) * nv);
+  double s_time = (time - t_its) / (t_ite - t_its); /* :1437 */
   for (size_t q = 0; q < nu; ++q) u[q] = (1.0 - s_time) * u12[q] + s_time * u12[q + nu];
   for (size_t q = 0; q < nv; ++q) v[q] = (1.0 - s_time) * v12[q] + s_time * v12[q + nv];
+  if (w)
+    for (size_t q = 0; q < nw; ++q) w[q] = (1.0 - s_time) * w12[q] + s_time * w12[q + nw];
+  return s_time;
+}
+
+void or_time_step_uv(const or_dims *d, const or_grid *g, double dt,
+                     double s_time, int iiter, double *c, double *acum,
+                     const double *s, const double *u, const double *v,
+                     const double *w12, const double *k1, const double *k2,
+                     const double *k3, const double *vs, double fluxes[6],
+                     int nthreads) {
+  const size_t nw = n_w(d);
   /* source term (:1456-1473) */
   for (int k = 0; k < d->nz; ++k) {
     double dZ = g->dX3_p[k + 2];
@@ -360,8 +367,109 @@ void or_time_step(const or_dims *d, const or_grid *g, double dt, double time,
   }
   or_solve_z(d, g, dt, c, acum, k3, w12, w12 + nw, s_time, vs, &fluxes[5],
              &fluxes[4], nthreads);
+}
+
+void or_time_step(const or_dims *d, const or_grid *g, double dt, double time,
+                  double t_its, double t_ite, int iiter, double *c,
+                  double *acum, const double *s, const double *u12,
+                  const double *v12, const double *w12, const double *k1,
+                  const double *k2, const double *k3, const double *vs,
+                  double fluxes[6], int nthreads) {
+  double *u = (double *)malloc(sizeof(double) * n_u(d));
+  double *v = (double *)malloc(sizeof(double) * n_v(d));
+  double s_time = or_current_winds(d, time, t_its, t_ite, u12, v12, NULL, u, v, NULL);
+  or_time_step_uv(d, g, dt, s_time, iiter, c, acum, s, u, v, w12, k1, k2, k3,
+                  vs, fluxes, nthreads);
   free(u);
   free(v);
+}
+
+/* ---- gravity current: F3D_add_radial_wind, mod_F3D.F90:978-1226.
+ * PI = 4 atan(1) and REARTH = 6356000 m (mod_KindType.F90:43-44). */
+#define GC_REARTH 6356000.0
+
+int or_gc_state(const or_dims *d, const double p[11], double time,
+                const double *lon_c, const double *lat_c, const double *Hm1_c,
+                double st[7]) {
+  const double PI = 4.0 * atan(1.0);
+  const double c_flow_rate = p[4], k_entrain = p[5], brunt_vaisala = p[6],
+               lambda_grav = p[7], mass_flow_rate = p[8], h_tot = p[9];
+  (void)d;
+  for (int q = 0; q < 7; ++q) st[q] = 0.0;
+  if (time < p[2]) return 0; /* :1026-1027 */
+  if (time > p[3]) return 0;
+  if (mass_flow_rate <= 0.0) return 0; /* :1031 */
+  /* minimum radius from the first cell's diagonal (:1036-1045) */
+  double deltax = GC_REARTH * Hm1_c[0] * (lon_c[0] - lon_c[1]) * PI / 180.0;
+  double deltay = GC_REARTH * (lat_c[0] - lat_c[1]) * PI / 180.0;
+  double radius = 1.5 * sqrt(deltax * deltax + deltay * deltay);
+  double min_radius = radius; /* parallel_max over a single rank */
+  if (p[10] > 0.0) min_radius = p[10];
+  double tse = time - p[2]; /* :1049 */
+  double vol_flow_rate = c_flow_rate * sqrt(k_entrain) * pow(mass_flow_rate, 0.75) /
+                         pow(brunt_vaisala, 1.25);
+  double c_gravr = 3.0 * lambda_grav * brunt_vaisala * vol_flow_rate / (2.0 * PI);
+  double radius_grav = pow(c_gravr * (tse * tse), 0.33333);
+  radius_grav = fmax(radius_grav, min_radius);
+  double c_gravu = sqrt(2.0 * lambda_grav * brunt_vaisala * vol_flow_rate / (3.0 * PI));
+  double c_grav_factor = 0.75 * c_gravu * sqrt(radius_grav);
+  double th_grav = c_gravu / (sqrt(radius_grav) * lambda_grav * brunt_vaisala);
+  double h_umbr = h_tot / 1.2;
+  double hmin = fmax(h_umbr - 0.5 * th_grav, 0.5 * h_tot);
+  double hmax = fmin(h_umbr + 0.5 * th_grav, h_tot);
+  st[0] = vol_flow_rate;
+  st[1] = min_radius;
+  st[2] = radius_grav;
+  st[3] = c_grav_factor;
+  st[4] = th_grav;
+  st[5] = hmin;
+  st[6] = hmax;
+  return 1;
+}
+
+void or_add_radial_wind(const or_dims *d, const double p[11],
+                        const double st[7], const double *lon_c,
+                        const double *lat_c, const double *lon_p,
+                        const double *lat_p, const double *Hm1_p,
+                        const double *Hm1_c, const double *z_c, double *u,
+                        double *v) {
+  const double PI = 4.0 * atan(1.0);
+  const double xc = p[0], yc = p[1];
+  const double min_radius = st[1], radius_grav = st[2], c_grav_factor = st[3],
+               hmin = st[5], hmax = st[6];
+  const size_t nxc = (size_t)d->nx + 1, nyc = (size_t)d->ny + 1;
+  /* x faces (:1144-1180) */
+  for (int j = 0; j < d->ny; ++j)
+    for (int i = 0; i <= d->nx; ++i) {
+      double deltax = GC_REARTH * Hm1_p[j] * (lon_c[i] - xc) * PI / 180.0;
+      double deltay = GC_REARTH * (lat_p[j] - yc) * PI / 180.0;
+      double radius = sqrt(deltax * deltax + deltay * deltay);
+      if (radius > radius_grav) continue;
+      double fu = (radius < 1e-3) ? 0.0 : deltax / radius / Hm1_p[j];
+      radius = fmax(radius, min_radius);
+      double rvel = fu * c_grav_factor / radius *
+                    (1.0 + radius * radius / (3.0 * (radius_grav * radius_grav)));
+      for (int k = 0; k < d->nz; ++k) {
+        double zp = z_c[i + nxc * (j + nyc * k)];
+        if (zp >= hmin && zp <= hmax) u[IU(i, j, k)] = u[IU(i, j, k)] + rvel;
+      }
+    }
+  /* y faces (:1184-1214) */
+  for (int j = 0; j <= d->ny; ++j)
+    for (int i = 0; i < d->nx; ++i) {
+      double deltax = GC_REARTH * Hm1_c[j] * (lon_p[i] - xc) * PI / 180.0;
+      double deltay = GC_REARTH * (lat_c[j] - yc) * PI / 180.0;
+      double radius = sqrt(deltax * deltax + deltay * deltay);
+      if (radius > radius_grav) continue;
+      double fu = (radius < 1e-3) ? 0.0 : deltay / radius;
+      radius = fmax(radius, min_radius);
+      double rvel = fu * c_grav_factor / radius *
+                    (1.0 + radius * radius / (3.0 * (radius_grav * radius_grav)));
+      for (int k = 0; k < d->nz; ++k) {
+        double zp = z_c[i + nxc * (j + nyc * k)];
+        if (zp >= hmin && zp <= hmax) v[IV(j, i, k)] = v[IV(j, i, k)] + rvel;
+      }
+    }
 }
 
 /* ---- grid_get_time_step: mod_Grid.F90:1026-1141 */

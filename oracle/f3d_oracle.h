@@ -83,6 +83,45 @@ void or_time_step(const or_dims *d, const or_grid *g, double dt, double time,
                   const double *k2, const double *k3, const double *vs,
                   double fluxes[6], int nthreads);
 
+/* The same body with the current winds given: u(ibs-1:ibe+1, jps:jpe,
+ * kps:kpe) and v(jbs-1:jbe+1, ips:ipe, kps:kpe) as F3D_time_step holds them
+ * after the time interpolation and F3D_add_radial_wind; w12 and s_time for
+ * the z sweep. */
+void or_time_step_uv(const or_dims *d, const or_grid *g, double dt,
+                     double s_time, int iiter, double *c, double *acum,
+                     const double *s, const double *u, const double *v,
+                     const double *w12, const double *k1, const double *k2,
+                     const double *k3, const double *vs, double fluxes[6],
+                     int nthreads);
+
+/* Current winds at s_time = (time - t_its)/(t_ite - t_its)
+ * (mod_F3D.F90:1437-1439, 1450): u, v, w in the single-snapshot layouts.
+ * Returns s_time. */
+double or_current_winds(const or_dims *d, double time, double t_its,
+                        double t_ite, const double *u12, const double *v12,
+                        const double *w12, double *u, double *v, double *w);
+
+/* Gravity current, F3D_add_radial_wind (mod_F3D.F90:978-1226).
+ * p: lon, lat, start_time, end_time, c_flow_rate, k_entrain, brunt_vaisala,
+ * lambda, mass_flow_rate, h_tot, input_min_radius (MY_MOD%MY_GC).
+ * or_gc_state fills st = {vol_flow_rate, min_radius, radius_grav,
+ * c_grav_factor, th_grav, hmin, hmax} for the given time and returns 1 when
+ * the current is active (the wind is then modified and update_step set), 0
+ * when the routine returns early.  lon_c(ibs:ibe), lat_c(jbs:jbe),
+ * Hm1_c(jbs:jbe). */
+int or_gc_state(const or_dims *d, const double p[11], double time,
+                const double *lon_c, const double *lat_c, const double *Hm1_c,
+                double st[7]);
+/* Adds the radial wind of state st to the current u and v (layouts as in
+ * or_time_step_uv); lon_p(ips:ipe), lat_p(jps:jpe), Hm1_p(jps:jpe),
+ * z_c(ibs:ibe, jbs:jbe, kbs:kbe). */
+void or_add_radial_wind(const or_dims *d, const double p[11],
+                        const double st[7], const double *lon_c,
+                        const double *lat_c, const double *lon_p,
+                        const double *lat_p, const double *Hm1_p,
+                        const double *Hm1_c, const double *z_c, double *u,
+                        double *v);
+
 /* grid_get_time_step (mod_Grid.F90:1026-1141) for one rank. */
 void or_get_time_step(const or_dims *d, const or_grid *g, int criterion,
                       double cfl, double run_end, const double *u,

@@ -76,6 +76,13 @@ def lib():
         L.or_wet_deposition.argtypes = [D, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp, dp]
         L.or_radionuclides.argtypes = [D, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int), dp, dp, dp]
         L.or_perturb.restype = C.c_double
+        L.or_time_step_uv.argtypes = [D, G, C.c_double, C.c_double, C.c_int, dp, dp, dp, dp, dp, dp,
+                                      dp, dp, dp, dp, dp, C.c_int]
+        L.or_current_winds.argtypes = [D, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp]
+        L.or_current_winds.restype = C.c_double
+        L.or_gc_state.argtypes = [D, dp, C.c_double, dp, dp, dp, dp]
+        L.or_gc_state.restype = C.c_int
+        L.or_add_radial_wind.argtypes = [D, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -127,6 +134,38 @@ class Oracle:
         lib().or_time_step(C.byref(self.dims), C.byref(self.cgrid), dt, time, t_its, t_ite, iiter,
                            _p(c), _p(acum), _p(s), _p(u12), _p(v12), _p(w12), _p(k1), _p(k2),
                            _p(k3), _p(vs), _p(fluxes), self.threads)
+
+    def current_winds(self, time, t_its, t_ite, u12, v12, w12):
+        """(u, v, w, s_time) at time, the snapshot layouts without the last axis."""
+        u = np.zeros(u12.shape[:-1], order="F")
+        v = np.zeros(v12.shape[:-1], order="F")
+        w = np.zeros(w12.shape[:-1], order="F")
+        st = lib().or_current_winds(C.byref(self.dims), time, t_its, t_ite, _p(u12), _p(v12), _p(w12),
+                                    _p(u), _p(v), _p(w))
+        return u, v, w, st
+
+    def time_step_uv(self, dt, s_time, iiter, c, acum, s, u, v, w12, k1, k2, k3, vs, fluxes):
+        lib().or_time_step_uv(C.byref(self.dims), C.byref(self.cgrid), dt, s_time, iiter, _p(c), _p(acum),
+                              _p(s), _p(u), _p(v), _p(w12), _p(k1), _p(k2), _p(k3), _p(vs), _p(fluxes),
+                              self.threads)
+
+    def gc_state(self, params, time):
+        """(active, [vol_flow_rate, min_radius, radius_grav, c_grav_factor,
+        th_grav, hmin, hmax]) of F3D_add_radial_wind at time."""
+        g = self.g
+        p = np.asarray(params, np.float64)
+        st = np.zeros(7)
+        a = lib().or_gc_state(C.byref(self.dims), _p(p), time, _p(np.asarray(g.lon_c, np.float64)),
+                              _p(np.asarray(g.lat_c, np.float64)), _p(np.asarray(g.Hm1_c, np.float64)),
+                              _p(st))
+        return bool(a), st
+
+    def add_radial_wind(self, params, st, u, v):
+        g = self.g
+        arrs = [np.asfortranarray(getattr(g, n), dtype=np.float64) for n in
+                ("lon_c", "lat_c", "lon_p", "lat_p", "Hm1_p", "Hm1_c", "z_c")]
+        lib().or_add_radial_wind(C.byref(self.dims), _p(np.asarray(params, np.float64)), _p(st),
+                                 *[_p(a) for a in arrs], _p(u), _p(v))
 
     def get_time_step(self, criterion, cfl, run_end, u, v, w, k1, k2, k3, vs):
         a, b = C.c_double(), C.c_double()
