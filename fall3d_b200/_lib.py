@@ -23,6 +23,13 @@ class F3DDims(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nbins", C.c_int)]
 
 
+class F3DKdiffu(C.Structure):
+    """f3d_kdiffu: the diffusion model of phys_get_kdiffu."""
+    _fields_ = [("modkh", C.c_int), ("modkv", C.c_int), ("map_h", C.c_int), ("kh0", C.c_double),
+                ("kv0", C.c_double), ("rams_cs", C.c_double), ("dlon", C.c_double), ("dlat", C.c_double),
+                ("s_time", C.c_double)]
+
+
 class F3DEnsMember(C.Structure):
     _fields_ = [("grid_class", C.c_int), ("wind_factor", C.c_double)]
 
@@ -44,6 +51,7 @@ SIGNATURES = {
                                           _ip, _dp, _dp, _dp],
     "f3d_ads_output_species": [_vp, _ip, C.c_int, _dp, _dp, _dp, _dp],
     "f3d_ads_set_meteo_corners": [_vp] + [_dp] * 6 + [C.c_double] * 4,
+    "f3d_ads_set_meteo_corners_kdiffu": [_vp] + [_dp] * 8 + [C.POINTER(F3DKdiffu), C.c_double, C.c_double],
     "f3d_ads_set_source": [_vp, C.c_int, _ip, _dp],
     "f3d_ads_set_source_dense": [_vp, _dp],
     "f3d_ads_upload_state": [_vp, _dp, _dp],

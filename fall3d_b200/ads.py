@@ -22,7 +22,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import F3DDims, F3DError, F3DNoConvergence, check, lib
+from ._lib import F3DDims, F3DError, F3DKdiffu, F3DNoConvergence, check, lib
 from .grid import ArakawaCGrid
 
 PREC_FP64, PREC_FP32 = 0, 1
@@ -108,6 +108,30 @@ class Domain:
         check(lib().f3d_ads_set_meteo_corners(self._h, _p(uc), _p(vc), _p(wc), *[_p(a) for a in ks],
                                               float(kh), float(kv), float(t_its), float(t_ite)),
               "f3d_ads_set_meteo_corners")
+
+    def set_meteo_corners_kdiffu(self, uc_pair, vc_pair, wc_pair, modkh, modkv, s_time, tvc_pair=None,
+                                 pblh=None, mon=None, ust=None, kh0=0.0, kv0=0.0, rams_cs=0.2275,
+                                 t_its=0.0, t_ite=3600.0):
+        """set_meteo_corners with phys_get_kdiffu on the device (mod_Phys.F90:406-664):
+        modkh 1 CONSTANT / 2 CMAQ / 4 RAMS, modkv 1 CONSTANT / 3 SIMILARITY,
+        from the corner fields interpolated at s_time; pblh, mon, ust at mass
+        points (nx, ny)."""
+        g = self.grid
+
+        def pair(p):
+            return None if p is None else np.asfortranarray(
+                np.stack([np.asarray(p[0], np.float64), np.asarray(p[1], np.float64)], axis=3))
+        uc, vc, wc, tvc = pair(uc_pair), pair(vc_pair), pair(wc_pair), pair(tvc_pair)
+        two = [None if a is None else np.asfortranarray(a, dtype=np.float64) for a in (pblh, mon, ust)]
+        hc = np.asfortranarray(g.h_c, dtype=np.float64) if modkv == 3 else None
+        if modkv == 3:
+            self._ensure_corner_heights()
+        kd = F3DKdiffu(int(modkh), int(modkv), int(g.map_h), float(kh0), float(kv0), float(rams_cs),
+                       float(g.dlon), float(g.dlat), float(s_time))
+        check(lib().f3d_ads_set_meteo_corners_kdiffu(self._h, _p(uc), _p(vc), _p(wc), _p(tvc),
+                                                     *[_p(a) for a in two], _p(hc), C.byref(kd),
+                                                     float(t_its), float(t_ite)),
+              "f3d_ads_set_meteo_corners_kdiffu")
 
     def phys_wet_deposition(self, a, b, pre, pblh, bin_cat, bin_diam):
         """Switch on wet deposition for this meteo interval (precipitation

@@ -475,21 +475,23 @@ extern "C" int f3d_ads_set_terrain(f3d_ctx* c, int map_v, double X3max, const do
   return 0;
 }
 
-extern "C" int f3d_ads_set_meteo_corners(f3d_ctx* c, const double* uc, const double* vc,
-                                         const double* wc, const double* k1, const double* k2,
-                                         const double* k3, double kh, double kv, double t_its,
-                                         double t_ite) {
-  if (!c) return set_err("f3d_ads_set_meteo_corners: null context");
-  if (!c->grid_set) return set_err("f3d_ads_set_meteo_corners: grid not set");
-  if (!uc || !vc || !wc) return set_err("f3d_ads_set_meteo_corners: null corner wind");
-  const bool kgiven = k1 || k2 || k3;
-  if (kgiven && !(k1 && k2 && k3)) return set_err("f3d_ads_set_meteo_corners: give all of k1, k2, k3 or none");
-  if (!(t_ite != t_its)) return set_err("f3d_ads_set_meteo_corners: t_ite == t_its");
+// The meteo term from corner fields (F3D_update_meteo_term compute part):
+// uploads the corner winds of both snapshots, lets fill_k write the
+// unscaled diffusion into dk1..dk3 (reference layouts), then staggers and
+// scales on the device.
+template <class FillK>
+static int meteo_corners_impl(f3d_ctx* c, const char* who, const double* uc, const double* vc,
+                              const double* wc, size_t extra, double t_its, double t_ite,
+                              FillK fill_k) {
+  if (!c) return set_err("%s: null context", who);
+  if (!c->grid_set) return set_err("%s: grid not set", who);
+  if (!uc || !vc || !wc) return set_err("%s: null corner wind", who);
+  if (!(t_ite != t_its)) return set_err("%s: t_ite == t_its", who);
   CK(cudaSetDevice(c->device));
   const size_t nx = c->nx, ny = c->ny, nz = c->nz;
   const size_t ncor = (nx + 1) * (ny + 1) * (nz + 1);
   const size_t n1 = (nx + 4) * ny * nz, n2 = nx * (ny + 4) * nz, n3 = nx * ny * (nz + 4);
-  const size_t need = 6 * ncor + n1 + n2 + n3;
+  const size_t need = 6 * ncor + n1 + n2 + n3 + extra;
   if (need > c->met_cap) {
     c->d_met = nullptr;  // the old buffer stays in the context's allocation list
     if (dalloc(c, &c->d_met, need)) return 1;
@@ -501,17 +503,11 @@ extern "C" int f3d_ads_set_meteo_corners(f3d_ctx* c, const double* uc, const dou
   double* dk1 = dwc + 2 * ncor;
   double* dk2 = dk1 + n1;
   double* dk3 = dk2 + n2;
+  double* dextra = dk3 + n3;
   CK(cudaMemcpyAsync(duc, uc, 2 * ncor * 8, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(dvc, vc, 2 * ncor * 8, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(dwc, wc, 2 * ncor * 8, cudaMemcpyHostToDevice, c->st));
-  if (kgiven) {
-    CK(cudaMemcpyAsync(dk1, k1, n1 * 8, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(dk2, k2, n2 * 8, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(dk3, k3, n3 * 8, cudaMemcpyHostToDevice, c->st));
-  } else {
-    launch_meteo_kconst(c->nx, c->ny, c->nz, kh, kv, dk1, dk2, dk3, c->st);
-    c->launches += 1;
-  }
+  if (fill_k(duc, dvc, dk1, dk2, dk3, dextra)) return 1;
   MemberDev& m = c->hm;
   MetGeo g;
   g.nx = c->nx;
@@ -546,6 +542,120 @@ extern "C" int f3d_ads_set_meteo_corners(f3d_ctx* c, const double* uc, const dou
   CK(cudaStreamSynchronize(c->st));
   c->meteo_set = true;
   return 0;
+}
+
+extern "C" int f3d_ads_set_meteo_corners(f3d_ctx* c, const double* uc, const double* vc,
+                                         const double* wc, const double* k1, const double* k2,
+                                         const double* k3, double kh, double kv, double t_its,
+                                         double t_ite) {
+  const bool kgiven = k1 || k2 || k3;
+  if (kgiven && !(k1 && k2 && k3))
+    return set_err("f3d_ads_set_meteo_corners: give all of k1, k2, k3 or none");
+  return meteo_corners_impl(
+      c, "f3d_ads_set_meteo_corners", uc, vc, wc, 0, t_its, t_ite,
+      [&](double*, double*, double* dk1, double* dk2, double* dk3, double*) -> int {
+        const size_t nx = c->nx, ny = c->ny, nz = c->nz;
+        if (kgiven) {
+          CK(cudaMemcpyAsync(dk1, k1, (nx + 4) * ny * nz * 8, cudaMemcpyHostToDevice, c->st));
+          CK(cudaMemcpyAsync(dk2, k2, nx * (ny + 4) * nz * 8, cudaMemcpyHostToDevice, c->st));
+          CK(cudaMemcpyAsync(dk3, k3, nx * ny * (nz + 4) * 8, cudaMemcpyHostToDevice, c->st));
+        } else {
+          launch_meteo_kconst(c->nx, c->ny, c->nz, kh, kv, dk1, dk2, dk3, c->st);
+          c->launches += 1;
+        }
+        return 0;
+      });
+}
+
+extern "C" int f3d_ads_set_meteo_corners_kdiffu(f3d_ctx* c, const double* uc, const double* vc,
+                                                const double* wc, const double* tvc,
+                                                const double* pblh, const double* mon,
+                                                const double* ust, const double* h_c,
+                                                const f3d_kdiffu* kd, double t_its, double t_ite) {
+  const char* who = "f3d_ads_set_meteo_corners_kdiffu";
+  if (!c || !kd) return set_err("%s: null argument", who);
+  if (kd->modkh != 1 && kd->modkh != 2 && kd->modkh != 4)
+    return set_err("Horizontal diffusion parameterization not implemented ");
+  if (kd->modkv != 1 && kd->modkv != 3)
+    return set_err("Horizontal diffusion parameterization not implemented ");  // sic, mod_Phys.F90:660
+  if (kd->map_h == 2 || kd->map_h == 3) return set_err("Mapping not implemented yet");
+  if (kd->map_h != 0 && kd->map_h != 1) return set_err("Incorrect horizontal mapping");
+  const bool vsim = kd->modkv == 3;
+  if (vsim && (!tvc || !pblh || !mon || !ust || !h_c))
+    return set_err("%s: the similarity K needs tvc, pblh, mon, ust and h_c", who);
+  if (vsim && !c->d_zc)
+    return set_err("%s: corner heights not set (f3d_ads_set_corner_heights)", who);
+  const size_t nx = c->grid_set ? c->nx : 0, ny = c->grid_set ? c->ny : 0, nz = c->grid_set ? c->nz : 0;
+  const size_t ncor = (nx + 1) * (ny + 1) * (nz + 1), n2d = nx * ny, nc2 = (nx + 1) * (ny + 1);
+  const size_t extra = (vsim ? 2 * ncor + 3 * n2d + nc2 : 0) + (kd->modkh == 4 ? n2d : 0);
+  return meteo_corners_impl(
+      c, who, uc, vc, wc, extra, t_its, t_ite,
+      [&](double* duc, double* dvc, double* dk1, double* dk2, double* dk3, double* dx) -> int {
+        MemberDev& m = c->hm;
+        KdArgs a;
+        memset(&a, 0, sizeof(a));
+        a.nx = c->nx;
+        a.ny = c->ny;
+        a.nz = c->nz;
+        a.modkh = kd->modkh;
+        a.modkv = kd->modkv;
+        a.kh0 = kd->kh0;
+        a.kv0 = kd->kv0;
+        a.rams_cs = kd->rams_cs;
+        a.khn0 = kd->map_h == 0 ? 4000.0 : 0.036;  // mod_Phys.F90:449-459
+        a.dlon = kd->dlon;
+        a.dlat = kd->dlat;
+        a.s = kd->s_time;
+        a.uc0 = duc;
+        a.uc1 = duc + ncor;
+        a.vc0 = dvc;
+        a.vc1 = dvc + ncor;
+        a.dx1p = m.dx1p;
+        a.dx2p = m.dx2p;
+        a.hm1 = m.hm1;
+        a.hm2 = m.hm2;
+        a.k1 = dk1;
+        a.k2 = dk2;
+        a.k3 = dk3;
+        a.zc = c->d_zc;
+        double* p = dx;
+        if (vsim) {
+          CK(cudaMemcpyAsync(p, tvc, 2 * ncor * 8, cudaMemcpyHostToDevice, c->st));
+          a.tvc0 = p;
+          a.tvc1 = p + ncor;
+          p += 2 * ncor;
+          const double* src[3] = {pblh, mon, ust};
+          const double** dst[3] = {&a.pblh, &a.mon, &a.ust};
+          for (int q = 0; q < 3; ++q) {
+            CK(cudaMemcpyAsync(p, src[q], n2d * 8, cudaMemcpyHostToDevice, c->st));
+            *dst[q] = p;
+            p += n2d;
+          }
+          CK(cudaMemcpyAsync(p, h_c, nc2 * 8, cudaMemcpyHostToDevice, c->st));
+          a.hc = p;
+          p += nc2;
+        }
+        if (kd->modkh == 4) {  // kmh = 0.075 (dx dy)^(2/3) with the host's pow (mod_Phys.F90:537)
+          std::vector<double> dx1(nx + 4), dx2(ny + 4), h1(ny), h2(ny + 4), kmh(n2d);
+          CK(cudaMemcpyAsync(dx1.data(), m.dx1p, dx1.size() * 8, cudaMemcpyDeviceToHost, c->st));
+          CK(cudaMemcpyAsync(dx2.data(), m.dx2p, dx2.size() * 8, cudaMemcpyDeviceToHost, c->st));
+          CK(cudaMemcpyAsync(h1.data(), m.hm1, h1.size() * 8, cudaMemcpyDeviceToHost, c->st));
+          CK(cudaMemcpyAsync(h2.data(), m.hm2, h2.size() * 8, cudaMemcpyDeviceToHost, c->st));
+          CK(cudaStreamSynchronize(c->st));
+          for (size_t j = 0; j < ny; ++j)
+            for (size_t i = 0; i < nx; ++i) {
+              const double ddx = dx1[i + 2] * h1[j], ddy = dx2[j + 2] * h2[j + 2];
+              kmh[i + nx * j] = 0.075 * std::pow(ddx * ddy, 2.0 / 3.0);
+            }
+          CK(cudaMemcpyAsync(p, kmh.data(), n2d * 8, cudaMemcpyHostToDevice, c->st));
+          CK(cudaStreamSynchronize(c->st));  // kmh is freed when this scope ends
+          a.kmh = p;
+          p += n2d;
+        }
+        launch_kdiffu(a, c->st);
+        c->launches += 2;
+        return 0;
+      });
 }
 
 extern "C" int f3d_ads_set_wet_deposition(f3d_ctx* c, double a, double b, const double* pre,

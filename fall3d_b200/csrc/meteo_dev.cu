@@ -235,6 +235,139 @@ void launch_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, int fp3
   k_gc_winds<<<592, 256, 0, st>>>(members, mi, nx, ny, nz, fp32, g);
 }
 
+// ---- phys_get_kdiffu (mod_Phys.F90:406-664) -------------------------------
+// Thread per mass point; the corner fields are interpolated where read, as
+// F3D_update_meteo_term interpolates them first (mod_F3D.F90:760-767).
+__device__ __forceinline__ double kd_at(const double* a0, const double* a1, double s, long long q) {
+  return (1.0 - s) * a0[q] + s * a1[q];
+}
+
+__global__ void k_kdiff_h(KdArgs a) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const long long NX1 = nx + 1, NY1 = ny + 1;
+  const double alfa = 0.28, khf = 8000.0, rkhmin = 100.0;  // :444-446
+  MGRID(e, (long long)nx * ny * nz) {
+    const int i = (int)(e % nx);
+    const long long t = e / nx;
+    const int j = (int)(t % ny), k = (int)(t / ny);
+    double kv;
+    if (a.modkh == 1) {
+      kv = a.kh0;
+    } else {
+      auto C = [&](const double* p0, const double* p1, int ii, int jj) {
+        return kd_at(p0, p1, a.s, ii + NX1 * (jj + NY1 * k));
+      };
+      const double dx = a.dx1p[i + 2] * a.hm1[j];
+      const double dy = a.dx2p[j + 2] * a.hm2[j + 2];
+      const double u00 = C(a.uc0, a.uc1, i, j), u10 = C(a.uc0, a.uc1, i + 1, j);
+      const double u01 = C(a.uc0, a.uc1, i, j + 1), u11 = C(a.uc0, a.uc1, i + 1, j + 1);
+      const double v00 = C(a.vc0, a.vc1, i, j), v10 = C(a.vc0, a.vc1, i + 1, j);
+      const double v01 = C(a.vc0, a.vc1, i, j + 1), v11 = C(a.vc0, a.vc1, i + 1, j + 1);
+      const double dudx = 0.5 * (u10 - u00 + u11 - u01) / dx;
+      const double dvdx = 0.5 * (v10 - v00 + v11 - v01) / dx;
+      const double dudy = 0.5 * (u01 - u00 + u11 - u10) / dy;
+      const double dvdy = 0.5 * (v01 - v00 + v11 - v10) / dy;
+      if (a.modkh == 2) {  // CMAQ (:484-499)
+        const double kht = alfa * alfa * dx * dy *
+                           sqrt((dudx - dvdy) * (dudx - dvdy) + (dvdx + dudy) * (dvdx + dudy));
+        const double khn = khf * (a.khn0 / (a.hm1[j] * a.dlon)) * (a.khn0 / (a.hm2[j + 2] * a.dlat));
+        if (kht < 1.0 && khn < 1.0) kv = rkhmin;
+        else kv = fmax(kht * khn / (kht + khn), rkhmin);
+      } else {  // RAMS (:528-550)
+        kv = a.rams_cs * a.rams_cs * dx * dy *
+             sqrt((dudy + dvdx) * (dudy + dvdx) + 2.0 * (dudx * dudx + dvdy * dvdy));
+        kv = fmax(fmax(kv, a.kmh[i + (long long)nx * j]), rkhmin);
+      }
+    }
+    // k1(i, j, k) and its halo copies at the x ends (:501-504); k2 likewise in y
+    double* r1 = a.k1 + (long long)(nx + 4) * (j + (long long)ny * k);
+    r1[i + 2] = kv;
+    if (i == 0) r1[0] = r1[1] = kv;
+    if (i == nx - 1) r1[nx + 3] = r1[nx + 2] = kv;
+    double* c2 = a.k2 + i + (long long)nx * (long long)(ny + 4) * k;
+    c2[(long long)nx * (j + 2)] = kv;
+    if (j == 0) c2[0] = c2[nx] = kv;
+    if (j == ny - 1) c2[(long long)nx * (ny + 3)] = c2[(long long)nx * (ny + 2)] = kv;
+  }
+}
+
+__global__ void k_kdiff_v(KdArgs a) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const long long NX1 = nx + 1, NY1 = ny + 1;
+  const double KARMAN = 0.4, GI = 9.81, landac = 30.0;  // mod_KindType.F90:45-46, :447
+  MGRID(e, (long long)nx * ny * nz) {
+    const int i = (int)(e % nx);
+    const long long t = e / nx;
+    const int j = (int)(t % ny), k = (int)(t / ny);
+    double kv;
+    if (a.modkv == 1) {
+      kv = a.kv0;
+    } else {  // SIMILARITY (:595-645)
+      auto Z = [&](int ii, int jj, int kk) { return a.zc[ii + NX1 * (jj + NY1 * kk)]; };
+      auto C = [&](const double* p0, const double* p1, int ii, int jj, int kk) {
+        return kd_at(p0, p1, a.s, ii + NX1 * (jj + NY1 * kk));
+      };
+      const double hp = (a.hc[i + NX1 * j] + a.hc[i + 1 + NX1 * j] + a.hc[i + NX1 * (j + 1)] +
+                         a.hc[i + 1 + NX1 * (j + 1)]) / 4.0;
+      const long long ij = i + (long long)nx * j;
+      const double pb = a.pblh[ij], L = a.mon[ij], us = a.ust[ij];
+      const double zp = (Z(i, j, k) + Z(i + 1, j, k) + Z(i, j + 1, k) + Z(i + 1, j + 1, k) + Z(i, j, k + 1) +
+                         Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1)) / 8.0;
+      const double z = fmax(0.0, zp - hp);
+      if (z < pb) {
+        const double zl = z / L;  // phys_get_Fih (:1702-1721)
+        const double fih = (zl < 0.0) ? 1.0 / sqrt(1.0 - 15.0 * zl) : 1.0 + 5.0 * zl;
+        kv = KARMAN * z * us * (1.0 - z / pb) * (1.0 - z / pb) / fih;
+        kv = fmax(0.0, kv);
+      } else {
+        double lc = 1.0 / (KARMAN * z) + 1.0 / landac;
+        lc = 1.0 / lc;
+        double z1 = 0.25 * (Z(i, j, k) + Z(i + 1, j, k) + Z(i, j + 1, k) + Z(i + 1, j + 1, k));
+        z1 = z1 - hp;
+        double z2 = 0.25 * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1));
+        z2 = z2 - hp;
+        const double u1 = 0.25 * (C(a.uc0, a.uc1, i, j, k) + C(a.uc0, a.uc1, i + 1, j, k) +
+                                  C(a.uc0, a.uc1, i, j + 1, k) + C(a.uc0, a.uc1, i + 1, j + 1, k));
+        const double v1 = 0.25 * (C(a.vc0, a.vc1, i, j, k) + C(a.vc0, a.vc1, i + 1, j, k) +
+                                  C(a.vc0, a.vc1, i, j + 1, k) + C(a.vc0, a.vc1, i + 1, j + 1, k));
+        const double u2 = 0.25 * (C(a.uc0, a.uc1, i, j, k + 1) + C(a.uc0, a.uc1, i + 1, j, k + 1) +
+                                  C(a.uc0, a.uc1, i, j + 1, k + 1) + C(a.uc0, a.uc1, i + 1, j + 1, k + 1));
+        const double v2 = 0.25 * (C(a.vc0, a.vc1, i, j, k + 1) + C(a.vc0, a.vc1, i + 1, j, k + 1) +
+                                  C(a.vc0, a.vc1, i, j + 1, k + 1) + C(a.vc0, a.vc1, i + 1, j + 1, k + 1));
+        const double umod1 = sqrt(u1 * u1 + v1 * v1);
+        const double umod2 = sqrt(u2 * u2 + v2 * v2);
+        const double umod = 0.5 * (umod1 + umod2);
+        const double tv1 = 0.25 * (C(a.tvc0, a.tvc1, i, j, k) + C(a.tvc0, a.tvc1, i + 1, j, k) +
+                                   C(a.tvc0, a.tvc1, i, j + 1, k) + C(a.tvc0, a.tvc1, i + 1, j + 1, k));
+        const double tv2 = 0.25 * (C(a.tvc0, a.tvc1, i, j, k + 1) + C(a.tvc0, a.tvc1, i + 1, j, k + 1) +
+                                   C(a.tvc0, a.tvc1, i, j + 1, k + 1) + C(a.tvc0, a.tvc1, i + 1, j + 1, k + 1));
+        const double um2 = fmax(umod * umod, 1e-18);  // phys_get_Rib (:1684-1696)
+        const double Ri = GI * (z2 - z1) * (tv2 - tv1) / (um2 * 0.5 * (tv2 + tv1));
+        double fc;  // phys_get_Fc (:1727-1741)
+        if (Ri > 0.0) {
+          fc = 1.0 + 10.0 * Ri * (1.0 + 8.0 * Ri);
+          fc = 1.0 / fc;
+        } else {
+          fc = sqrt(1.0 - 18.0 * Ri);
+        }
+        kv = lc * lc * fabs((umod2 - umod1) / (z2 - z1)) * fc;
+        kv = fmax(0.0, kv);
+      }
+    }
+    // k3(i, j, k) and its halo copies at the bottom and top (:647-650)
+    const long long pl = (long long)nx * ny;
+    double* c3 = a.k3 + i + (long long)nx * j;
+    c3[pl * (k + 2)] = kv;
+    if (k == 0) c3[0] = c3[pl] = kv;
+    if (k == nz - 1) c3[pl * (nz + 3)] = c3[pl * (nz + 2)] = kv;
+  }
+}
+
+void launch_kdiffu(const KdArgs& a, cudaStream_t st) {
+  k_kdiff_h<<<592, 256, 0, st>>>(a);
+  k_kdiff_v<<<592, 256, 0, st>>>(a);
+}
+
 void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
                          double* k3, cudaStream_t st) {
   k_met_kconst<<<592, 256, 0, st>>>(nx, ny, nz, kh, kv, k1, k2, k3);

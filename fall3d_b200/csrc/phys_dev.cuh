@@ -111,6 +111,35 @@ __device__ __forceinline__ bool gc_rvel_v(const GcArgs& g, int nx, int ny, int i
   return gc_rvel(g, g.hm1_c[j], g.lon_p[i] - g.xc, g.lat_c[j] - g.yc, false, rvel);
 }
 
+// diffusion coefficients, phys_get_kdiffu (mod_Phys.F90:406-664): from the
+// corner fields of the two meteo snapshots at interpolation factor s, into the
+// reference layouts k1(ips-2:ipe+2, jps:jpe, kps:kpe), k2(ips:ipe,
+// jps-2:jpe+2, kps:kpe), k3(ips:ipe, jps:jpe, kps-2:kpe+2), unscaled
+struct KdArgs {
+  int nx, ny, nz, modkh, modkv;  // MOD_CONSTANT 1, CMAQ 2, SIMILARITY 3, RAMS 4
+  double kh0, kv0, rams_cs, khn0, dlon, dlat, s;
+  const double* uc0;  // corner fields (nx+1)(ny+1)(nz+1), snapshots its and ite
+  const double* uc1;
+  const double* vc0;
+  const double* vc1;
+  const double* tvc0;
+  const double* tvc1;
+  const double* dx1p;  // (nx+4)
+  const double* dx2p;  // (ny+4)
+  const double* hm1;   // ny
+  const double* hm2;   // ny+4
+  const double* kmh;   // RAMS: 0.075 (dx dy)^(2/3) per column, nx*ny (host libm)
+  const double* pblh;  // nx*ny
+  const double* mon;
+  const double* ust;
+  const double* zc;    // corner heights
+  const double* hc;    // (nx+1)(ny+1) terrain at corners
+  double* k1;
+  double* k2;
+  double* k3;
+};
+void launch_kdiffu(const KdArgs& a, cudaStream_t st);
+
 void launch_wet(const WetArgs& a, cudaStream_t st);
 void launch_radio(const RadioArgs& a, cudaStream_t st);
 void launch_out_columns(const OutArgs& a, cudaStream_t st);

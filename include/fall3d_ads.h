@@ -131,6 +131,34 @@ int f3d_ads_set_radionuclides(f3d_ctx *ctx, const int *bin_cat,
 /* MY_TRA%my_awet(ips-2:ipe+2, jps-2:jpe+2, nbins), halos zero. */
 int f3d_ads_get_awet(f3d_ctx *ctx, double *my_awet);
 
+/* Diffusion model of phys_get_kdiffu (mod_Phys.F90:406-664). */
+typedef struct {
+  int modkh;       /* MY_MOD%modkh: 1 CONSTANT, 2 CMAQ, 4 RAMS */
+  int modkv;       /* MY_MOD%modkv: 1 CONSTANT, 3 SIMILARITY */
+  int map_h;       /* MY_GRID%map_h: 0 Cartesian, 1 spherical */
+  double kh0, kv0; /* MY_MOD%kh0, kv0 (CONSTANT) */
+  double rams_cs;  /* MY_MOD%RAMS_CS */
+  double dlon, dlat; /* MY_GRID%dlon, dlat */
+  double s_time;   /* interpolation factor of the corner fields at the update
+                      time (mod_F3D.F90:760-767) */
+} f3d_kdiffu;
+
+/* f3d_ads_set_meteo_corners with the diffusion computed on the device by
+ * phys_get_kdiffu from the corner winds and virtual temperature interpolated
+ * at kd->s_time (CMAQ/RAMS horizontal, similarity vertical, or constants),
+ * then scaled like the given K's.  tvc: MY_MET%my_tvc(ibs:ibe, jbs:jbe,
+ * kbs:kbe, its:ite) (2 snapshots); pblh, mon, ust: MY_MET%my_pblh, my_mon
+ * (already limited to |L| >= 10, mod_F3D.F90:740), my_ust at mass points;
+ * h_c: MY_GRID%h_c.  These five may be NULL unless modkv is SIMILARITY, which
+ * also needs the corner heights (f3d_ads_set_corner_heights).  Errors as
+ * phys_get_kdiffu's. */
+int f3d_ads_set_meteo_corners_kdiffu(f3d_ctx *ctx, const double *uc,
+                                     const double *vc, const double *wc,
+                                     const double *tvc, const double *pblh,
+                                     const double *mon, const double *ust,
+                                     const double *h_c, const f3d_kdiffu *kd,
+                                     double t_its, double t_ite);
+
 /* Gravity current, F3D_add_radial_wind (mod_F3D.F90:978-1226).  params =
  * MY_MOD%MY_GC {lon, lat, start_time, end_time, c_flow_rate, k_entrain,
  * brunt_vaisala, lambda, mass_flow_rate, h_tot, input_min_radius}; the

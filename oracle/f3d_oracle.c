@@ -472,6 +472,145 @@ void or_add_radial_wind(const or_dims *d, const double p[11],
     }
 }
 
+/* ---- phys_get_kdiffu: mod_Phys.F90:406-664 */
+#define KARMAN 0.4 /* mod_KindType.F90:46 */
+
+int or_kdiffu(const or_dims *d, const or_grid *g, const int kdf[3],
+              const double par[5], const double *uc, const double *vc,
+              const double *tvc, const double *pblh, const double *mon,
+              const double *ust, const double *z_c, const double *h_c,
+              double *k1, double *k2, double *k3) {
+  const int nx = d->nx, ny = d->ny, nz = d->nz;
+  const size_t NX1 = (size_t)nx + 1, NY1 = (size_t)ny + 1;
+  const int modkh = kdf[0], modkv = kdf[1], map_h = kdf[2];
+  const double kh0 = par[0], kv0 = par[1], rams_cs = par[2], dlon = par[3], dlat = par[4];
+  const double alfa = 0.28, khf = 8000.0, rkhmin = 100.0, landac = 30.0; /* :444-447 */
+  double khn0;
+  if (map_h == 0) khn0 = 4000.0; /* :449-459 */
+  else if (map_h == 1) khn0 = 0.036;
+  else return 1;
+#define UC(a, i, j, k) a[(size_t)(i) + NX1 * ((size_t)(j) + NY1 * (size_t)(k))]
+#define K1(p, j, k) k1[(size_t)((p) + 2) + (size_t)(nx + 4) * ((size_t)(j) + (size_t)ny * (size_t)(k))]
+#define K2(i, p, k) k2[(size_t)(i) + (size_t)nx * ((size_t)((p) + 2) + (size_t)(ny + 4) * (size_t)(k))]
+#define K3(i, j, p) k3[(size_t)(i) + (size_t)nx * ((size_t)(j) + (size_t)ny * (size_t)((p) + 2))]
+  /* horizontal (:474-590) */
+  if (modkh == 1) {
+    for (size_t q = 0; q < (size_t)(nx + 4) * ny * nz; ++q) k1[q] = kh0;
+    for (size_t q = 0; q < (size_t)nx * (ny + 4) * nz; ++q) k2[q] = kh0;
+  } else if (modkh == 2 || modkh == 4) {
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          double dx = g->dX1_p[i + 2] * g->Hm1_p[j];
+          double dy = g->dX2_p[j + 2] * g->Hm2_p[j + 2];
+          double dudx = 0.5 * (UC(uc, i + 1, j, k) - UC(uc, i, j, k) + UC(uc, i + 1, j + 1, k) - UC(uc, i, j + 1, k)) / dx;
+          double dvdx = 0.5 * (UC(vc, i + 1, j, k) - UC(vc, i, j, k) + UC(vc, i + 1, j + 1, k) - UC(vc, i, j + 1, k)) / dx;
+          double dudy = 0.5 * (UC(uc, i, j + 1, k) - UC(uc, i, j, k) + UC(uc, i + 1, j + 1, k) - UC(uc, i + 1, j, k)) / dy;
+          double dvdy = 0.5 * (UC(vc, i, j + 1, k) - UC(vc, i, j, k) + UC(vc, i + 1, j + 1, k) - UC(vc, i + 1, j, k)) / dy;
+          double kv;
+          if (modkh == 2) { /* CMAQ :484-499 */
+            double kht = alfa * alfa * dx * dy *
+                         sqrt((dudx - dvdy) * (dudx - dvdy) + (dvdx + dudy) * (dvdx + dudy));
+            double khn = khf * (khn0 / (g->Hm1_p[j] * dlon)) * (khn0 / (g->Hm2_p[j + 2] * dlat));
+            if (kht < 1.0 && khn < 1.0) kv = rkhmin;
+            else kv = fmax(kht * khn / (kht + khn), rkhmin);
+          } else { /* RAMS :528-550 */
+            double kmh = 0.075 * pow(dx * dy, 2.0 / 3.0);
+            kv = rams_cs * rams_cs * dx * dy *
+                 sqrt((dudy + dvdx) * (dudy + dvdx) + 2.0 * (dudx * dudx + dvdy * dvdy));
+            kv = fmax(fmax(kv, kmh), rkhmin);
+          }
+          K1(i, j, k) = kv;
+          K2(i, j, k) = kv;
+        }
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j) {
+        K1(-2, j, k) = K1(0, j, k);
+        K1(-1, j, k) = K1(0, j, k);
+        K1(nx + 1, j, k) = K1(nx - 1, j, k);
+        K1(nx, j, k) = K1(nx - 1, j, k);
+      }
+    for (int k = 0; k < nz; ++k)
+      for (int i = 0; i < nx; ++i) {
+        K2(i, -2, k) = K2(i, 0, k);
+        K2(i, -1, k) = K2(i, 0, k);
+        K2(i, ny + 1, k) = K2(i, ny - 1, k);
+        K2(i, ny, k) = K2(i, ny - 1, k);
+      }
+  } else {
+    return 1;
+  }
+  /* vertical (:592-662) */
+  if (modkv == 1) {
+    for (size_t q = 0; q < (size_t)nx * ny * (nz + 4); ++q) k3[q] = kv0;
+  } else if (modkv == 3) {
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        double hp = (h_c[i + NX1 * j] + h_c[i + 1 + NX1 * j] + h_c[i + NX1 * (j + 1)] +
+                     h_c[i + 1 + NX1 * (j + 1)]) / 4.0;
+        double pb = pblh[i + (size_t)nx * j], L = mon[i + (size_t)nx * j], us = ust[i + (size_t)nx * j];
+        for (int k = 0; k < nz; ++k) {
+          double zp = (UC(z_c, i, j, k) + UC(z_c, i + 1, j, k) + UC(z_c, i, j + 1, k) + UC(z_c, i + 1, j + 1, k) +
+                       UC(z_c, i, j, k + 1) + UC(z_c, i + 1, j, k + 1) + UC(z_c, i, j + 1, k + 1) +
+                       UC(z_c, i + 1, j + 1, k + 1)) / 8.0;
+          double z = fmax(0.0, zp - hp);
+          double kv;
+          if (z < pb) {
+            double zl = z / L, fih; /* phys_get_Fih :1702-1721 */
+            if (zl < 0.0) fih = 1.0 / sqrt(1.0 - 15.0 * zl);
+            else fih = 1.0 + 5.0 * zl;
+            kv = KARMAN * z * us * (1.0 - z / pb) * (1.0 - z / pb) / fih;
+            kv = fmax(0.0, kv);
+          } else {
+            double lc = 1.0 / (KARMAN * z) + 1.0 / landac;
+            lc = 1.0 / lc;
+            double z1 = 0.25 * (UC(z_c, i, j, k) + UC(z_c, i + 1, j, k) + UC(z_c, i, j + 1, k) + UC(z_c, i + 1, j + 1, k));
+            z1 = z1 - hp;
+            double z2 = 0.25 * (UC(z_c, i, j, k + 1) + UC(z_c, i + 1, j, k + 1) + UC(z_c, i, j + 1, k + 1) +
+                                UC(z_c, i + 1, j + 1, k + 1));
+            z2 = z2 - hp;
+            double u1 = 0.25 * (UC(uc, i, j, k) + UC(uc, i + 1, j, k) + UC(uc, i, j + 1, k) + UC(uc, i + 1, j + 1, k));
+            double v1 = 0.25 * (UC(vc, i, j, k) + UC(vc, i + 1, j, k) + UC(vc, i, j + 1, k) + UC(vc, i + 1, j + 1, k));
+            double u2 = 0.25 * (UC(uc, i, j, k + 1) + UC(uc, i + 1, j, k + 1) + UC(uc, i, j + 1, k + 1) +
+                                UC(uc, i + 1, j + 1, k + 1));
+            double v2 = 0.25 * (UC(vc, i, j, k + 1) + UC(vc, i + 1, j, k + 1) + UC(vc, i, j + 1, k + 1) +
+                                UC(vc, i + 1, j + 1, k + 1));
+            double umod1 = sqrt(u1 * u1 + v1 * v1);
+            double umod2 = sqrt(u2 * u2 + v2 * v2);
+            double umod = 0.5 * (umod1 + umod2);
+            double tv1 = 0.25 * (UC(tvc, i, j, k) + UC(tvc, i + 1, j, k) + UC(tvc, i, j + 1, k) + UC(tvc, i + 1, j + 1, k));
+            double tv2 = 0.25 * (UC(tvc, i, j, k + 1) + UC(tvc, i + 1, j, k + 1) + UC(tvc, i, j + 1, k + 1) +
+                                 UC(tvc, i + 1, j + 1, k + 1));
+            /* phys_get_Rib(Tv2, Tv1, umod, z2, z1) :1684-1696 */
+            double um2 = fmax(umod * umod, 1e-18);
+            double Ri = GI * (z2 - z1) * (tv2 - tv1) / (um2 * 0.5 * (tv2 + tv1));
+            double fc; /* phys_get_Fc :1727-1741 */
+            if (Ri > 0.0) {
+              fc = 1.0 + 10.0 * Ri * (1.0 + 8.0 * Ri);
+              fc = 1.0 / fc;
+            } else {
+              fc = sqrt(1.0 - 18.0 * Ri);
+            }
+            kv = lc * lc * fabs((umod2 - umod1) / (z2 - z1)) * fc;
+            kv = fmax(0.0, kv);
+          }
+          K3(i, j, k) = kv;
+        }
+        K3(i, j, -2) = K3(i, j, 0);
+        K3(i, j, -1) = K3(i, j, 0);
+        K3(i, j, nz + 1) = K3(i, j, nz - 1);
+        K3(i, j, nz) = K3(i, j, nz - 1);
+      }
+  } else {
+    return 1;
+  }
+#undef UC
+#undef K1
+#undef K2
+#undef K3
+  return 0;
+}
+
 /* ---- grid_get_time_step: mod_Grid.F90:1026-1141 */
 void or_get_time_step(const or_dims *d, const or_grid *g, int criterion,
                       double cfl, double run_end, const double *u,

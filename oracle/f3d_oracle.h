@@ -122,6 +122,21 @@ void or_add_radial_wind(const or_dims *d, const double p[11],
                         const double *Hm1_c, const double *z_c, double *u,
                         double *v);
 
+/* phys_get_kdiffu (mod_Phys.F90:406-664) with its helpers phys_get_Rib,
+ * phys_get_Fih, phys_get_Fc (:1684-1741) and grid_c2p(_2D)
+ * (mod_Grid.F90:1229-1277).  kdf = {modkh, modkv, map_h} (MOD_CONSTANT 1,
+ * CMAQ 2, SIMILARITY 3, RAMS 4; MAP_H_CARTESIAN 0, SPHERICAL 1); par =
+ * {kh0, kv0, RAMS_CS, dlon, dlat}.  uc, vc, tvc: current corner fields
+ * (ibs:ibe, jbs:jbe, kbs:kbe); pblh, mon, ust (ips:ipe, jps:jpe); z_c
+ * corners; h_c (ibs:ibe, jbs:jbe).  Outputs in the reference layouts
+ * k1(ips-2:ipe+2, jps:jpe, kps:kpe), k2(ips:ipe, jps-2:jpe+2, kps:kpe),
+ * k3(ips:ipe, jps:jpe, kps-2:kpe+2).  Returns MY_ERR%flag. */
+int or_kdiffu(const or_dims *d, const or_grid *g, const int kdf[3],
+              const double par[5], const double *uc, const double *vc,
+              const double *tvc, const double *pblh, const double *mon,
+              const double *ust, const double *z_c, const double *h_c,
+              double *k1, double *k2, double *k3);
+
 /* grid_get_time_step (mod_Grid.F90:1026-1141) for one rank. */
 void or_get_time_step(const or_dims *d, const or_grid *g, int criterion,
                       double cfl, double run_end, const double *u,

@@ -80,6 +80,8 @@ def lib():
                                       dp, dp, dp, dp, dp, C.c_int]
         L.or_current_winds.argtypes = [D, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp]
         L.or_current_winds.restype = C.c_double
+        L.or_kdiffu.argtypes = [D, G, C.POINTER(C.c_int), dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]
+        L.or_kdiffu.restype = C.c_int
         L.or_gc_state.argtypes = [D, dp, C.c_double, dp, dp, dp, dp]
         L.or_gc_state.restype = C.c_int
         L.or_add_radial_wind.argtypes = [D, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]
@@ -148,6 +150,25 @@ class Oracle:
         lib().or_time_step_uv(C.byref(self.dims), C.byref(self.cgrid), dt, s_time, iiter, _p(c), _p(acum),
                               _p(s), _p(u), _p(v), _p(w12), _p(k1), _p(k2), _p(k3), _p(vs), _p(fluxes),
                               self.threads)
+
+    def kdiffu(self, modkh, modkv, map_h, kh0, kv0, rams_cs, dlon, dlat, uc, vc, tvc, pblh, mon, ust):
+        """phys_get_kdiffu on the current corner fields: (flag, k1, k2, k3) in
+        the layouts (nx+4, ny, nz), (nx, ny+4, nz), (nx, ny, nz+4)."""
+        g = self.g
+        nx, ny, nz = g.nx, g.ny, g.nz
+        k1 = np.zeros((nx + 4, ny, nz), order="F")
+        k2 = np.zeros((nx, ny + 4, nz), order="F")
+        k3 = np.zeros((nx, ny, nz + 4), order="F")
+        kdf = (C.c_int * 3)(int(modkh), int(modkv), int(map_h))
+        par = np.array([kh0, kv0, rams_cs, dlon, dlat], np.float64)
+        z = np.zeros((nx, ny))
+        arrs = [np.asfortranarray(a if a is not None else z, dtype=np.float64) for a in (pblh, mon, ust)]
+        tv = np.asfortranarray(tvc if tvc is not None else np.zeros_like(uc), dtype=np.float64)
+        f = lib().or_kdiffu(C.byref(self.dims), C.byref(self.cgrid), kdf, _p(par),
+                            _p(np.asfortranarray(uc)), _p(np.asfortranarray(vc)), _p(tv), *[_p(a) for a in arrs],
+                            _p(np.asfortranarray(g.z_c, dtype=np.float64)),
+                            _p(np.asfortranarray(g.h_c, dtype=np.float64)), _p(k1), _p(k2), _p(k3))
+        return f, k1, k2, k3
 
     def gc_state(self, params, time):
         """(active, [vol_flow_rate, min_radius, radius_grav, c_grav_factor,
