@@ -155,10 +155,9 @@ def sweep_bytes(wl, prec_bytes: int, d: str) -> float:
     nx, ny, nz, nb = g.nx, g.ny, g.nz, wl.nbins
     cells = nx * ny * nz
     c_rw = 2.0 * prec_bytes * cells * nb
-    if prec_bytes == 4:
-        face = 12.0  # two wind snapshots + face diffusion coefficient
-    else:
-        face = 16.0  # current wind + face diffusion
+    # FP32: one float4 per face {two wind snapshots, face diffusion, 1/dxb};
+    # FP64: current wind + face diffusion
+    face = 16.0
     if d == "x":
         return c_rw + face * (nx + 1) * ny * nz
     if d == "y":

@@ -47,6 +47,24 @@ __device__ __forceinline__ float half_phid(float d1, float d0) {
   return 0.5f * pd;
 }
 
+// Prefetch distances (march steps) of the face data and, in y and z, of the
+// concentration: the loads themselves stay one step (faces) or four steps
+// (concentration) ahead in registers, and the prefetch brings the lines into
+// L1 early enough to hide the L2/HBM latency without holding registers.
+#ifndef F3D_FACE_PF
+#define F3D_FACE_PF 8
+#endif
+#ifndef F3D_C_PF
+#define F3D_C_PF 8
+#endif
+#ifndef F3D_PF_L2
+#define F3D_PF_L2 0
+#endif
+__device__ __forceinline__ void prefetch_line(const void* p) {
+  if (F3D_PF_L2) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  else asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // Per-pencil operations of the precision form.  The current wind is
 // interpolated in time on the fly from the two meteo snapshots and scaled by
 // the member's wind factor (ensemble perturbation of u, v).
@@ -54,19 +72,21 @@ template <int LIM, int DIR, int TM>
 struct Ops32 {
   float* cp;
   long long cs;
-  const float* v1;
-  const float* v2;
+  const float4* fd;   // face data {u(its), u(ite), kf, 1/dxb(f-1)} (MemberDev::f4)
   const float* vsub;  // z: settling velocity of the bin
-  const float* kf;    // face diffusion coefficient
   long long vs;
-  const float* rdxb;
+  int nf;  // cells of the pencil (faces 0..nf)
   float s0, s1, wfac;
   float dt, hdt, dt3, dt6;
   XTile<float, (TM == 2) ? 1 : 2> xt;  // x pencils: shared-memory staging of the rows
 
   __device__ __forceinline__ float load_c(int p) const {
-    if constexpr (DIR == DIR_X) return xt.load(p);
-    else return cp[p * cs];
+    if constexpr (DIR == DIR_X) {
+      return xt.load(p);
+    } else {
+      if constexpr (F3D_C_PF > 0) prefetch_line(cp + (long long)min(p + F3D_C_PF, nf - 1) * cs);
+      return cp[p * cs];
+    }
   }
   __device__ __forceinline__ void store_c(int p, float v) {
     if constexpr (DIR == DIR_X) xt.store(p, v);
@@ -77,12 +97,18 @@ struct Ops32 {
   __device__ __forceinline__ void stage_end(int T0) { if constexpr (DIR == DIR_X) xt.block_end(T0); }
   __device__ __forceinline__ void stage_finish() { if constexpr (DIR == DIR_X) xt.finish(); }
   __device__ __forceinline__ FaceV<float> face(int f) const {
+    if constexpr (F3D_FACE_PF > 0) {
+      const long long fp = (long long)min(f + F3D_FACE_PF, nf) * vs;
+      prefetch_line(fd + fp);
+      if constexpr (DIR == DIR_Z) prefetch_line(vsub + fp);
+    }
     FaceV<float> r;
-    float w = fmaf(s0, __ldg(v1 + f * vs), s1 * __ldg(v2 + f * vs));
+    const float4 q = __ldg(fd + f * vs);
+    float w = fmaf(s0, q.x, s1 * q.y);
     if (DIR == DIR_Z) r.u = w - __ldg(vsub + f * vs);
     else r.u = wfac * w;
-    r.k = __ldg(kf + f * vs);
-    r.r = (f >= 1) ? __ldg(rdxb + (f - 1)) : 0.f;
+    r.k = q.z;
+    r.r = q.w;
     return r;
   }
   __device__ __forceinline__ float ghost_l(float c0, float uL) const { return (uL > 0.f) ? -c0 : c0; }
@@ -168,12 +194,9 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
                  threadIdx.x & 31, nx);
       o.cs = 1;
       long long fo = (long long)k * (nx + 1) * ny + j;
-      o.v1 = m.ux32[0] + fo;
-      o.v2 = m.ux32[1] + fo;
-      o.kf = m.kfx + fo;
+      o.fd = (m.gc_cur ? m.gc4[0] : m.f4[0]) + fo;
       o.vs = ny;
       o.vsub = nullptr;
-      o.rdxb = m.rdx1b32;
       area = m.dx3b[k + 1] * m.dx2b[j + 1];
     } else if (DIR == DIR_Y) {
       i = (int)(pen % nx);
@@ -182,12 +205,9 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       o.cp = m.c32 + ((long long)b * nz + k) * ny * (long long)nx + i;
       o.cs = nx;
       long long fo = (long long)k * (ny + 1) * nx + i;
-      o.v1 = m.vy32[0] + fo;
-      o.v2 = m.vy32[1] + fo;
-      o.kf = m.kfy + fo;
+      o.fd = (m.gc_cur ? m.gc4[1] : m.f4[1]) + fo;
       o.vs = nx;
       o.vsub = nullptr;
-      o.rdxb = m.rdx2b32;
       area = m.dx3b[k + 1] * m.dx1b[i + 1];
     } else {
       i = (int)(pen % nx);
@@ -196,27 +216,21 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       o.cp = m.c32 + (long long)b * nz * ny * nx + (long long)j * nx + i;
       o.cs = (long long)nx * ny;
       long long fo = (long long)j * nx + i;
-      o.v1 = m.wz32[0] + fo;
-      o.v2 = m.wz32[1] + fo;
-      o.kf = m.kfz + fo;
+      o.fd = m.f4[2] + fo;
       o.vs = (long long)nx * ny;
       o.vsub = m.vs32 + (long long)b * (nz + 1) * ny * nx + fo;
-      o.rdxb = m.rdx3b32;
       area = m.dx2b[j + 1] * m.dx1b[i + 1];
     }
     const double dt = m.dt;
     o.s1 = (float)m.stime;
     o.s0 = 1.f - o.s1;
     o.wfac = m.wfac;
-    if (DIR != DIR_Z && m.gc_cur) {  // current winds precomputed: u = fmaf(1, u, 0 * u)
-      const float* cur = (DIR == DIR_X) ? m.ucur32 : m.vcur32;
-      const long long fo = o.v1 - ((DIR == DIR_X) ? m.ux32[0] : m.vy32[0]);
-      o.v1 = cur + fo;
-      o.v2 = cur + fo;
+    if (DIR != DIR_Z && m.gc_cur) {  // this step's winds in both slots: u = fmaf(1, u, 0 * u)
       o.s0 = 1.f;
       o.s1 = 0.f;
       o.wfac = 1.f;
     }
+    o.nf = n;
     o.dt = (float)dt;
     o.hdt = 0.5f * o.dt;
     o.dt3 = o.dt * (1.f / 3.f);
@@ -309,24 +323,19 @@ void launch_source32(const MemberDev* members, int nmembers, cudaStream_t st) {
 }
 
 // FP32 field preparation from the FP64 meteo arrays (once per meteo update):
-// winds, settling velocity and the face diffusion coefficients
+// the face data {u(its), u(ite), kf, 1/dxb(f-1)} of each direction with
 //   kf(f) = 0.5 (k(f) + k(f-1)) / dxp(f-1)         (KT_RHS P term, :1111)
+// and the settling velocity.
 __global__ void k_fp32_fields(MemberDev* members, int mi) {
   MemberDev& m = members[mi];
   const int nx = m.nx, ny = m.ny, nz = m.nz, nb = m.nb;
   const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)(ny + 1) * nx * nz,
                   nw = (long long)(nz + 1) * nx * ny;
   const long long nvs = (long long)nb * nw;
-  const long long tot = 2 * nu + 2 * nv + 2 * nw + nu + nv + nw + nvs;
+  const long long tot = nu + nv + nw + nvs;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
     long long q = e;
-    if (q < 2 * nu) { const_cast<float*>(m.ux32[0])[q] = (float)m.ux[0][q]; continue; }
-    q -= 2 * nu;
-    if (q < 2 * nv) { const_cast<float*>(m.vy32[0])[q] = (float)m.vy[0][q]; continue; }
-    q -= 2 * nv;
-    if (q < 2 * nw) { const_cast<float*>(m.wz32[0])[q] = (float)m.wz[0][q]; continue; }
-    q -= 2 * nw;
     if (q < nu) {  // x faces: [k][f][j]
       int j = (int)(q % ny);
       long long t = q / ny;
@@ -334,7 +343,9 @@ __global__ void k_fp32_fields(MemberDev* members, int mi) {
       int k = (int)(t / (nx + 1));
       double kA = m.k1x[((long long)k * (nx + 2) + (f + 1)) * ny + j];
       double kB = m.k1x[((long long)k * (nx + 2) + f) * ny + j];
-      const_cast<float*>(m.kfx)[q] = (float)(0.5 * (kA + kB) / m.dx1p[f + 1]);
+      const_cast<float4*>(m.f4[0])[q] =
+          make_float4((float)m.ux[0][q], (float)m.ux[1][q], (float)(0.5 * (kA + kB) / m.dx1p[f + 1]),
+                      f >= 1 ? m.rdx1b32[f - 1] : 0.f);
       continue;
     }
     q -= nu;
@@ -345,7 +356,9 @@ __global__ void k_fp32_fields(MemberDev* members, int mi) {
       int k = (int)(t / (ny + 1));
       double kA = m.k2y[((long long)k * (ny + 2) + (f + 1)) * nx + i];
       double kB = m.k2y[((long long)k * (ny + 2) + f) * nx + i];
-      const_cast<float*>(m.kfy)[q] = (float)(0.5 * (kA + kB) / m.dx2p[f + 1]);
+      const_cast<float4*>(m.f4[1])[q] =
+          make_float4((float)m.vy[0][q], (float)m.vy[1][q], (float)(0.5 * (kA + kB) / m.dx2p[f + 1]),
+                      f >= 1 ? m.rdx2b32[f - 1] : 0.f);
       continue;
     }
     q -= nv;
@@ -356,7 +369,9 @@ __global__ void k_fp32_fields(MemberDev* members, int mi) {
       int f = (int)(t / ny);
       double kA = m.k3z[((long long)(f + 1) * ny + j) * nx + i];
       double kB = m.k3z[((long long)f * ny + j) * nx + i];
-      const_cast<float*>(m.kfz)[q] = (float)(0.5 * (kA + kB) / m.dx3p[f + 1]);
+      const_cast<float4*>(m.f4[2])[q] =
+          make_float4((float)m.wz[0][q], (float)m.wz[1][q], (float)(0.5 * (kA + kB) / m.dx3p[f + 1]),
+                      f >= 1 ? m.rdx3b32[f - 1] : 0.f);
       continue;
     }
     q -= nw;

@@ -103,10 +103,7 @@ struct EnsClass {
   double* vs = nullptr;
   double* kkf[3] = {nullptr, nullptr, nullptr};
   double4* geo[3] = {nullptr, nullptr, nullptr};
-  float* ux32 = nullptr;
-  float* vy32 = nullptr;
-  float* wz32 = nullptr;
-  float* kf[3] = {nullptr, nullptr, nullptr};
+  float4* f4[3] = {nullptr, nullptr, nullptr};  // FP32 face data (MemberDev::f4)
   float* vs32 = nullptr;
   float* rdx[3] = {nullptr, nullptr, nullptr};
   double* dx[6] = {};   // dx1p dx1b dx2p dx2b dx3p dx3b
@@ -359,12 +356,9 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
       rc |= ealloc(e, &k.geo[1], ny + 1);
       rc |= ealloc(e, &k.geo[2], nz + 1);
     } else {
-      rc |= ealloc(e, &k.ux32, 2 * fu);
-      rc |= ealloc(e, &k.vy32, 2 * fv);
-      rc |= ealloc(e, &k.wz32, 2 * fw);
-      rc |= ealloc(e, &k.kf[0], fu);
-      rc |= ealloc(e, &k.kf[1], fv);
-      rc |= ealloc(e, &k.kf[2], fw);
+      rc |= ealloc(e, &k.f4[0], fu);
+      rc |= ealloc(e, &k.f4[1], fv);
+      rc |= ealloc(e, &k.f4[2], fw);
       rc |= ealloc(e, &k.vs32, nb * fw);
       rc |= ealloc(e, &k.rdx[0], nx);
       rc |= ealloc(e, &k.rdx[1], ny);
@@ -416,10 +410,7 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
       rc |= ealloc(e, &d.wcur, fw);
       for (int q = 0; q < 3; ++q) { d.kkf[q] = k.kkf[q]; d.geo[q] = k.geo[q]; }
     } else {
-      d.ux32[0] = k.ux32; d.ux32[1] = k.ux32 + fu;
-      d.vy32[0] = k.vy32; d.vy32[1] = k.vy32 + fv;
-      d.wz32[0] = k.wz32; d.wz32[1] = k.wz32 + fw;
-      d.kfx = k.kf[0]; d.kfy = k.kf[1]; d.kfz = k.kf[2];
+      for (int q = 0; q < 3; ++q) d.f4[q] = k.f4[q];
       d.vs32 = k.vs32;
       d.rdx1b32 = k.rdx[0]; d.rdx2b32 = k.rdx[1]; d.rdx3b32 = k.rdx[2];
     }

@@ -291,12 +291,10 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
     rc |= dalloc(c, &g4, nz + 1); m.geo[2] = g4;
   } else {
     float* f;
-    rc |= dalloc(c, &f, 2 * (nx + 1) * ny * nz); m.ux32[0] = f; m.ux32[1] = f + (nx + 1) * ny * nz;
-    rc |= dalloc(c, &f, 2 * (ny + 1) * nx * nz); m.vy32[0] = f; m.vy32[1] = f + (ny + 1) * nx * nz;
-    rc |= dalloc(c, &f, 2 * (nz + 1) * nx * ny); m.wz32[0] = f; m.wz32[1] = f + (nz + 1) * nx * ny;
-    rc |= dalloc(c, &f, (nx + 1) * ny * nz); m.kfx = f;
-    rc |= dalloc(c, &f, (ny + 1) * nx * nz); m.kfy = f;
-    rc |= dalloc(c, &f, (nz + 1) * nx * ny); m.kfz = f;
+    float4* f4;
+    rc |= dalloc(c, &f4, (nx + 1) * ny * nz); m.f4[0] = f4;
+    rc |= dalloc(c, &f4, (ny + 1) * nx * nz); m.f4[1] = f4;
+    rc |= dalloc(c, &f4, (nz + 1) * nx * ny); m.f4[2] = f4;
     rc |= dalloc(c, &f, nb * (nz + 1) * nx * ny); m.vs32 = f;
     rc |= dalloc(c, &f, nx); m.rdx1b32 = f;
     rc |= dalloc(c, &f, ny); m.rdx2b32 = f;
@@ -949,10 +947,10 @@ extern "C" int f3d_ads_set_gravity_current(f3d_ctx* c, const double params[11], 
   } else if (c->gc_host.size() != n) {
     return set_err("f3d_ads_set_gravity_current: coordinates not given");
   }
-  if (c->prec == F3D_PREC_FP32 && !c->hm.ucur32) {
+  if (c->prec == F3D_PREC_FP32 && !c->hm.gc4[0]) {
     MemberDev& m = c->hm;
-    if (dalloc(c, &m.ucur32, (size_t)(c->nx + 1) * c->ny * c->nz) ||
-        dalloc(c, &m.vcur32, (size_t)(c->ny + 1) * c->nx * c->nz))
+    if (dalloc(c, &m.gc4[0], (size_t)(c->nx + 1) * c->ny * c->nz) ||
+        dalloc(c, &m.gc4[1], (size_t)(c->ny + 1) * c->nx * c->nz))
       return 1;
     if (upload_member(c)) return 1;
   }

@@ -47,21 +47,19 @@ struct MemberDev {
   //   kkf[d] = 0.5 (k(f) + k(f-1)) at every face, laid out like the winds
   const double4* geo[3];
   const double* kkf[3];
-  // FP32 copies for the precision form (null when unused)
-  const float* ux32[2];
-  const float* vy32[2];
-  const float* wz32[2];
-  const float* kfx;   // [k][f=0..nx][j]  0.5(k(f)+k(f-1))/dxp(f-1)
-  const float* kfy;   // [k][f=0..ny][i]
-  const float* kfz;   // [f=0..nz][j][i]
+  // FP32 face data of the precision form (null when unused), one float4 per
+  // face and direction, laid out like the winds (x [k][f][j], y [k][f][i],
+  // z [f][j][i]): {velocity at its, velocity at ite, 0.5 (k(f) + k(f-1)) /
+  // dxp(f-1), 1/dxb(f-1) (0 at f = 0)}, so that a sweep reads a face with a
+  // single 16-byte load
+  const float4* f4[3];
   const float* vs32;  // [bin][f][j][i]
   // per-step current winds (written by the prep kernel)
   double* ucur;  // [k][f][j]
   double* vcur;  // [k][f][i]
   double* wcur;  // [f][j][i]
-  float* ucur32;
-  float* vcur32;
-  float* wcur32;
+  float4* gc4[2];  // precision form with the gravity current: x and y face
+                   // data with this step's winds in both velocity slots
   float wfac;       // per-member multiplicative factor on u,v (ensemble), FP32 form
   double wfacd;     // the same factor for the FP64 form and the CFL reduction
   // grid metrics (reference arrays with their halos)
@@ -89,9 +87,8 @@ struct MemberDev {
   double time;
   double t_its, t_ite;
   int iiter;
-  int gc_cur;  // precision form: the x and y sweeps read this step's current
-               // winds from ucur32/vcur32 (gravity current) instead of
-               // interpolating the snapshots
+  int gc_cur;  // precision form: the x and y sweeps read gc4 (this step's
+               // winds with the gravity current) instead of f4
   // flux bookkeeping
   double* flux_part;  // per-block partial sums, [slot][2]
   int part_base[3];   // first partial slot of this member for x, y, z

@@ -194,7 +194,8 @@ void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, c
 // (mod_F3D.F90:1437-1445): the exact form adds rvel to the interpolated
 // winds the prep kernel wrote (my_u = my_u + rvel, :1171, :1208); the
 // precision form writes the interpolated FP64 wind plus rvel, rounded to
-// FP32, for the sweeps to read in place of their own interpolation.
+// FP32, into both velocity slots of a copy of its face data (gc4), which the
+// sweeps then read in place of f4.
 __global__ void k_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, int fp32, GcArgs g) {
   MemberDev& m = members[mi];
   const long long nu = (long long)(nx + 1) * ny * nz, nv = (long long)(ny + 1) * nx * nz;
@@ -211,7 +212,9 @@ __global__ void k_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, i
       } else {
         double u = (1.0 - s) * (f * m.ux[0][e]) + s * (f * m.ux[1][e]);
         if (add) u = u + rvel;
-        m.ucur32[e] = (float)u;
+        float4 q = m.f4[0][e];
+        q.x = q.y = (float)u;
+        m.gc4[0][e] = q;
       }
     } else {
       const long long q = e - nu;
@@ -224,7 +227,9 @@ __global__ void k_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, i
       } else {
         double v = (1.0 - s) * (f * m.vy[0][q]) + s * (f * m.vy[1][q]);
         if (add) v = v + rvel;
-        m.vcur32[q] = (float)v;
+        float4 r = m.f4[1][q];
+        r.x = r.y = (float)v;
+        m.gc4[1][q] = r;
       }
     }
   }
