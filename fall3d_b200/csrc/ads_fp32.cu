@@ -111,6 +111,14 @@ struct Ops32 {
     r.r = q.w;
     return r;
   }
+  // face data for the unguarded march: faces outside [0, nf] read the end
+  // face with 1/dxb = 0 (face 0 holds 0 there already), so that the
+  // right-hand side of a ghost cell is 0
+  __device__ __forceinline__ FaceV<float> face_v(int f) const {
+    FaceV<float> r = face(min(max(f, 0), nf));
+    if (f > nf) r.r = 0.f;
+    return r;
+  }
   __device__ __forceinline__ float ghost_l(float c0, float uL) const { return (uL > 0.f) ? -c0 : c0; }
   __device__ __forceinline__ float ghost_r(float cn, float uR) const { return (uR < 0.f) ? -cn : cn; }
   __device__ __forceinline__ float euler(float c, float k) const { return fmaf(dt, k, c); }
@@ -235,7 +243,8 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
     o.hdt = 0.5f * o.dt;
     o.dt3 = o.dt * (1.f / 3.f);
     o.dt6 = o.dt * (1.f / 6.f);
-    March<float, Ops32<LIM, DIR, TM>, TM> M(o, n);
+    // z pencils are short: the unguarded march keeps them in one loop body
+    March<float, Ops32<LIM, DIR, TM>, TM, DIR == DIR_Z> M(o, n);
     M.run();
     if (lane_ok) {
       clo = (double)M.flux_lo * area * dt;
