@@ -102,6 +102,11 @@ SIGNATURES = {
     "f3d_ens_get_fluxes": [_vp, _dp],
     "f3d_ens_mass_volume": [_vp, C.c_int, _dp],
     "f3d_ens_reset_state": [_vp],
+    "f3d_ens_set_class_wet_deposition": [_vp, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _ip, _dp],
+    "f3d_ens_set_radionuclides": [_vp, _ip, _ip],
+    "f3d_ens_get_member_awet": [_vp, C.c_int, _dp],
+    "f3d_ens_set_class_corner_heights": [_vp, C.c_int, _dp],
+    "f3d_ens_output_member_species": [_vp, C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp],
     "f3d_ens_set_profiling": [_vp, C.c_int],
     "f3d_ens_get_profile": [_vp, _dp, _ip],
     "f3d_ens_synchronize": [_vp],

@@ -33,7 +33,8 @@ __global__ void k_wet(WetArgs a) {
     const long long ij = e % ncol;
     const int b = (int)(e / ncol);
     if (!((a.mask >> b) & 1ull)) continue;
-    double lambda = a.dta * a.powpb[ij];
+    const double dta = a.dt_dev ? *a.dt_dev * a.a : a.dta;
+    double lambda = dta * a.powpb[ij];
     if (lambda > 1.0) lambda = 1.0;
     const int kt = a.ktop[ij];
     double aw = a.awet[e];
@@ -56,9 +57,11 @@ __global__ void k_wet(WetArgs a) {
 template <class T>
 __device__ __forceinline__ void decay_cell(const RadioArgs& a, T* c, long long q, long long stride) {
   for (int r = 0; r < a.nr; ++r) {
+    const double f = a.fdev ? a.fdev[r] : a.fact[r];
+    const double pf = a.fdev ? a.fdev[a.nr + r] : a.pfact[r];
     T* p = c + (long long)a.bin[r] * stride + q;
-    *p = (T)((double)*p * a.fact[r]);
-    if (a.parent[r] >= 0) *p = (T)((double)c[(long long)a.parent[r] * stride + q] * (1.0 - a.pfact[r]));
+    *p = (T)((double)*p * f);
+    if (a.parent[r] >= 0) *p = (T)((double)c[(long long)a.parent[r] * stride + q] * (1.0 - pf));
   }
 }
 

@@ -10,12 +10,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
 #include "../../include/fall3d_ads.h"
 #include "f3d_common.cuh"
 #include "phys_dev.cuh"
+#include "phys_host.h"
 #include "step_dev.cuh"
 
 namespace f3d {
@@ -114,6 +116,10 @@ struct EnsClass {
   int map_v = 0;                 // terrain mapping for the on-device meteo term
   double X3max = 1.0;
   double* terrain = nullptr;     // X3_c, X3_p, dhdx_p, dhdy_p
+  double* powpb = nullptr;       // wet deposition: P^b per column
+  int* ktop = nullptr;           // and the cells below the boundary-layer top
+  bool wet_set = false;
+  double* zc = nullptr;          // corner heights (output reductions)
 };
 
 }  // namespace
@@ -159,6 +165,17 @@ struct f3d_ens {
   cudaEvent_t pev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   double prof_ms[5] = {0, 0, 0, 0, 0};  // prep+source, x, y, z, flux+clock
   int prof_steps = 0;
+  // wet deposition and radioactive decay after the sweeps (all members)
+  bool wet_on = false;
+  double wet_a = 0.0;
+  unsigned long long wet_mask = 0;
+  std::vector<double*> awet;           // per member [bin][j][i]
+  bool radio_on = false;
+  RadioSpec radio;
+  double* d_radfact = nullptr;         // per member {fact[nr], pfact[nr]} for its dt
+  size_t radfact_cap = 0;
+  double* d_out = nullptr;             // output reductions: 4 (nx+1)(ny+1) fields
+  size_t out_cap = 0;
 };
 
 namespace {
@@ -181,6 +198,8 @@ void drop_graphs(f3d_ens* e) {
     }
   e->graph_ok = false;
 }
+
+int update_radio_factors(f3d_ens* e, const double* dt);
 
 // The device owns dt, time, stime and iiter once steps have run (device clock,
 // CFL on the device): refresh them in the host mirror before re-uploading it.
@@ -856,8 +875,11 @@ extern "C" int f3d_ens_compute_time_steps(f3d_ens* e, double stime, int criterio
   e->launches += 1;
   ECKL();
   if (pull_dynamic(e)) return 1;
+  std::vector<double> dts(e->nm);
+  for (int m = 0; m < e->nm; ++m) dts[m] = e->hm[m].dt;
+  if (update_radio_factors(e, dts.data())) return 1;
   if (dt)
-    for (int m = 0; m < e->nm; ++m) dt[m] = e->hm[m].dt;
+    for (int m = 0; m < e->nm; ++m) dt[m] = dts[m];
   return 0;
 }
 
@@ -930,6 +952,87 @@ int fused_setup(f3d_ens* e, const void** func, int* smem) {
 // ev[0] before the step, ev[1] after prep/source, ev[2 + q] after the q-th
 // sweep of the step's order, ev[5] at the end; in the persistent mode the
 // whole step lies between ev[0] and ev[5].
+// exp(-kn dt) of every radionuclide bin (and of its Sr90 parent) for each
+// member's dt, with the host C library as the CPU restatement evaluates it
+// (mod_Phys.F90:1276-1297); read by the decay kernel from device memory, so
+// that the captured step graphs pick up a new dt.
+int update_radio_factors(f3d_ens* e, const double* dt) {
+  if (!e->radio_on) return 0;
+  const size_t nr = e->radio.bin.size(), need = 2 * nr * (size_t)e->nm;
+  if (need > e->radfact_cap) {
+    if (ealloc(e, &e->d_radfact, need)) return 1;
+    e->radfact_cap = need;
+    drop_graphs(e);
+  }
+  std::vector<double> f(need);
+  for (int m = 0; m < e->nm; ++m)
+    for (size_t r = 0; r < nr; ++r) {
+      f[2 * nr * m + r] = std::exp(-e->radio.kn[r] * dt[m]);
+      f[2 * nr * m + nr + r] = e->radio.parent[r] >= 0 ? std::exp(-e->radio.pkn[r] * dt[m]) : 1.0;
+    }
+  ECK(cudaMemcpyAsync(e->d_radfact, f.data(), need * 8, cudaMemcpyHostToDevice, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+// Wet deposition and radioactive decay of every member after its sweeps
+// (mod_F3D.F90:1493-1520), one launch each per member.
+int enqueue_wet_radio(f3d_ens* e) {
+  for (int m = 0; m < e->nm; ++m) {
+    const MemberDev& d = e->hm[m];
+    const EnsClass& k = e->cls[e->member_class[m]];
+    const double* dt_dev = reinterpret_cast<const double*>(
+        reinterpret_cast<const char*>(e->dm + m) + offsetof(MemberDev, dt));
+    if (e->wet_on && k.wet_set) {
+      WetArgs a;
+      memset(&a, 0, sizeof(a));
+      a.nx = d.nx;
+      a.ny = d.ny;
+      a.nz = d.nz;
+      a.nb = e->nb;
+      a.dt_dev = dt_dev;
+      a.a = e->wet_a;
+      a.powpb = k.powpb;
+      a.ktop = k.ktop;
+      a.dx3p = d.dx3p;
+      a.awet = e->awet[m];
+      a.c64 = d.c64;
+      a.c32 = d.c32;
+      a.mask = e->wet_mask;
+      launch_wet(a, e->st);
+      e->launches += 1;
+    }
+    if (e->radio_on) {
+      RadioArgs r;
+      memset(&r, 0, sizeof(r));
+      r.nx = d.nx;
+      r.ny = d.ny;
+      r.nz = d.nz;
+      r.nr = (int)e->radio.bin.size();
+      for (int q = 0; q < r.nr; ++q) {
+        r.bin[q] = e->radio.bin[q];
+        r.parent[q] = e->radio.parent[q];
+      }
+      r.fdev = e->d_radfact + 2 * (size_t)r.nr * m;
+      r.c64 = d.c64;
+      r.c32 = d.c32;
+      r.acum = d.acum;
+      r.awet = e->awet.empty() ? nullptr : e->awet[m];
+      launch_radio(r, e->st);
+      e->launches += 1;
+    }
+  }
+  ECKL();
+  return 0;
+}
+
+int wet_radio_launches(const f3d_ens* e) {
+  int n = 0;
+  for (int m = 0; m < e->nm; ++m)
+    if (e->wet_on && e->cls[e->member_class[m]].wet_set) ++n;
+  return n + (e->radio_on ? e->nm : 0);
+}
+
 int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullptr) {
   if (ev) ECK(cudaEventRecord(ev[0], e->st));
   if (e->mode == F3D_ENS_MODE_PERSISTENT) {
@@ -953,6 +1056,7 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullpt
     void* args[] = {&a};
     ECK(cudaLaunchCooperativeKernel(func, dim3(e->fused_grid), dim3(128), args, (size_t)smem, e->st));
     e->launches += 1;
+    if (enqueue_wet_radio(e)) return 1;
     if (ev) ECK(cudaEventRecord(ev[5], e->st));
     return 0;
   }
@@ -976,6 +1080,7 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullpt
   }
   launch_flux_reduce(e->dm, e->nm, 7, e->st);
   e->launches += 1;
+  if (enqueue_wet_radio(e)) return 1;
   if (advance) {
     launch_advance_clock(e->dm, e->nm, e->st);
     e->launches += 1;
@@ -1032,8 +1137,8 @@ int build_graphs(f3d_ens* e) {
 }
 
 int kernels_per_step(const f3d_ens* e) {
-  if (e->mode == F3D_ENS_MODE_PERSISTENT) return 1;
-  return (e->prec == F3D_PREC_FP64 ? 2 : 1) + 3 + 1 + 1;
+  if (e->mode == F3D_ENS_MODE_PERSISTENT) return 1 + wet_radio_launches(e);
+  return (e->prec == F3D_PREC_FP64 ? 2 : 1) + 3 + 1 + 1 + wet_radio_launches(e);
 }
 
 }  // namespace
@@ -1068,6 +1173,7 @@ extern "C" int f3d_ens_step(f3d_ens* e, const double* dt, const double* time, in
   for (const EnsClass& k : e->cls)
     if (k.rep >= 0 && (!k.meteo_set || !k.grid_set)) return set_error_msg("f3d_ens_step: class not ready");
   ECK(cudaSetDevice(e->device));
+  if (update_radio_factors(e, dt)) return 1;
   launch_set_steps(e->dm, e->nm, dt, time, iiter, e->st);
   e->launches += (e->nm + 63) / 64;
   ECKL();
@@ -1123,8 +1229,150 @@ extern "C" int f3d_ens_reset_state(f3d_ens* e) {
     if (d.c64) ECK(cudaMemsetAsync(d.c64, 0, ncell * nb * 8, e->st));
     ECK(cudaMemsetAsync(d.acum, 0, (size_t)d.nx * d.ny * nb * 8, e->st));
   }
+  for (int m = 0; m < (int)e->awet.size(); ++m) {
+    const MemberDev& d = e->hm[m];
+    ECK(cudaMemsetAsync(e->awet[m], 0, (size_t)d.nx * d.ny * e->nb * 8, e->st));
+  }
   ECK(cudaMemsetAsync(e->flux_tot, 0, 12 * (size_t)e->nm * 8, e->st));
   ECK(cudaMemsetAsync(e->flux_step, 0, 6 * (size_t)e->nm * 8, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+// ---- wet deposition, radioactive decay, output reductions -----------------
+extern "C" int f3d_ens_set_class_wet_deposition(f3d_ens* e, int ci, double a, double b, const double* pre,
+                                                const double* pblh, const double* h_c, const double* z_c,
+                                                const int* bin_cat, const double* bin_diam) {
+  if (!e || ci < 0 || ci >= e->ncls) return set_error_msg("f3d_ens_set_class_wet_deposition: bad class");
+  if (!bin_cat) {
+    e->wet_on = false;
+    drop_graphs(e);
+    return 0;
+  }
+  if (!pre || !pblh || !h_c || !z_c || !bin_diam)
+    return set_error_msg("f3d_ens_set_class_wet_deposition: null array");
+  EnsClass& k = e->cls[ci];
+  if (!k.grid_set) return set_error_msg("f3d_ens_set_class_wet_deposition: class grid not set");
+  if (e->nb > 64) return set_error_msg("f3d_ens_set_class_wet_deposition: at most 64 bins");
+  ECK(cudaSetDevice(e->device));
+  std::vector<double> powpb;
+  std::vector<int> ktop;
+  if (!wet_tables(k.nx, k.ny, k.nz, b, pre, pblh, h_c, z_c, powpb, ktop))
+    return set_error_msg("f3d_ens_set_class_wet_deposition: heights not increasing with k");
+  const size_t ncol = (size_t)k.nx * k.ny;
+  if (!k.powpb && (ealloc(e, &k.powpb, ncol) || ealloc(e, &k.ktop, ncol))) return 1;
+  ECK(cudaMemcpy(k.powpb, powpb.data(), ncol * 8, cudaMemcpyHostToDevice));
+  ECK(cudaMemcpy(k.ktop, ktop.data(), ncol * 4, cudaMemcpyHostToDevice));
+  if (e->awet.empty()) {
+    e->awet.assign(e->nm, nullptr);
+    for (int m = 0; m < e->nm; ++m) {
+      const MemberDev& d = e->hm[m];
+      if (ealloc(e, &e->awet[m], (size_t)d.nx * d.ny * e->nb)) return 1;
+      ECK(cudaMemset(e->awet[m], 0, (size_t)d.nx * d.ny * e->nb * 8));
+    }
+  }
+  k.wet_set = true;
+  e->wet_mask = wet_bin_mask(e->nb, bin_cat, bin_diam);
+  e->wet_a = a;
+  e->wet_on = true;
+  drop_graphs(e);
+  return 0;
+}
+
+extern "C" int f3d_ens_set_radionuclides(f3d_ens* e, const int* bin_cat, const int* bin_spe) {
+  if (!e) return set_error_msg("f3d_ens_set_radionuclides: null ensemble");
+  drop_graphs(e);
+  e->radio_on = false;
+  e->radio = RadioSpec();
+  if (!bin_cat || !bin_spe) return 0;
+  if (e->nb > 64) return set_error_msg("f3d_ens_set_radionuclides: at most 64 bins");
+  int bad = 0;
+  const int rc = radio_spec(e->nb, bin_cat, bin_spe, e->radio, &bad);
+  if (rc == 1) return set_error_msg("The number of SR90 and Y90 classes must be equal.");
+  if (rc == 2) return set_error_msg("Invalid radionuclide type: species %d", bad);
+  e->radio_on = !e->radio.bin.empty();
+  if (!e->radio_on) return 0;
+  ECK(cudaSetDevice(e->device));
+  if (pull_dynamic(e)) return 1;
+  std::vector<double> dts(e->nm);
+  for (int m = 0; m < e->nm; ++m) dts[m] = e->hm[m].dt;
+  return update_radio_factors(e, dts.data());
+}
+
+extern "C" int f3d_ens_get_member_awet(f3d_ens* e, int mi, double* my_awet) {
+  if (!e || !my_awet || mi < 0 || mi >= e->nm) return set_error_msg("f3d_ens_get_member_awet: bad arguments");
+  const EnsClass& k = e->cls[e->member_class[mi]];
+  const size_t nx = k.nx, ny = k.ny, nb = e->nb;
+  std::vector<double> d(nx * ny * nb, 0.0);
+  if (!e->awet.empty()) {
+    ECK(cudaSetDevice(e->device));
+    ECK(cudaStreamSynchronize(e->st));
+    ECK(cudaMemcpy(d.data(), e->awet[mi], d.size() * 8, cudaMemcpyDeviceToHost));
+  }
+  std::fill(my_awet, my_awet + (nx + 4) * (ny + 4) * nb, 0.0);
+  for (size_t b = 0; b < nb; ++b)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i)
+        my_awet[(i + 2) + (nx + 4) * ((j + 2) + (ny + 4) * b)] = d[(b * ny + j) * nx + i];
+  return 0;
+}
+
+extern "C" int f3d_ens_set_class_corner_heights(f3d_ens* e, int ci, const double* z_c) {
+  if (!e || ci < 0 || ci >= e->ncls || !z_c) return set_error_msg("f3d_ens_set_class_corner_heights: bad arguments");
+  EnsClass& k = e->cls[ci];
+  if (!k.grid_set) return set_error_msg("f3d_ens_set_class_corner_heights: class grid not set");
+  ECK(cudaSetDevice(e->device));
+  const size_t n = (size_t)(k.nx + 1) * (k.ny + 1) * (k.nz + 1);
+  if (!k.zc && ealloc(e, &k.zc, n)) return 1;
+  ECK(cudaMemcpy(k.zc, z_c, n * 8, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+extern "C" int f3d_ens_output_member_species(f3d_ens* e, int mi, const int* bin_in, int col_du,
+                                             double* con_sur, double* col_mass, double* cloud_top,
+                                             double* grn_load) {
+  if (!e || !bin_in || mi < 0 || mi >= e->nm)
+    return set_error_msg("f3d_ens_output_member_species: bad arguments");
+  if (e->nb > 64) return set_error_msg("f3d_ens_output_member_species: at most 64 bins");
+  const EnsClass& k = e->cls[e->member_class[mi]];
+  if ((con_sur || col_mass || cloud_top) && !k.zc)
+    return set_error_msg("f3d_ens_output_member_species: corner heights not set (f3d_ens_set_class_corner_heights)");
+  ECK(cudaSetDevice(e->device));
+  const size_t ncol = (size_t)(k.nx + 1) * (k.ny + 1);
+  if (4 * ncol > e->out_cap) {
+    if (ealloc(e, &e->d_out, 4 * ncol)) return 1;
+    e->out_cap = 4 * ncol;
+  }
+  const MemberDev& d = e->hm[mi];
+  OutArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nx = k.nx;
+  a.ny = k.ny;
+  a.nz = k.nz;
+  a.nb = e->nb;
+  for (int q = 0; q < e->nb; ++q)
+    if (bin_in[q]) a.mask |= 1ull << q;
+  a.col_du = col_du;
+  a.c64 = d.c64;
+  a.c32 = d.c32;
+  a.acum = d.acum;
+  a.awet = e->awet.empty() ? nullptr : e->awet[mi];
+  a.hm1 = d.hm1;
+  a.hm2 = d.hm2;
+  a.hm3 = d.hm3;
+  a.zc = k.zc;
+  double* outs[4] = {con_sur, col_mass, cloud_top, grn_load};
+  double* dev[4];
+  for (int q = 0; q < 4; ++q) dev[q] = outs[q] ? e->d_out + q * ncol : nullptr;
+  a.con_sur = dev[0];
+  a.col_mass = dev[1];
+  a.cloud_top = dev[2];
+  a.grn_load = dev[3];
+  launch_out_columns(a, e->st);
+  e->launches += 1;
+  ECKL();
+  for (int q = 0; q < 4; ++q)
+    if (outs[q]) ECK(cudaMemcpyAsync(outs[q], dev[q], ncol * 8, cudaMemcpyDeviceToHost, e->st));
   ECK(cudaStreamSynchronize(e->st));
   return 0;
 }

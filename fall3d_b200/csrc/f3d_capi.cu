@@ -14,6 +14,7 @@
 #include "../../include/fall3d_ads.h"
 #include "f3d_common.cuh"
 #include "phys_dev.cuh"
+#include "phys_host.h"
 
 namespace f3d {
 // ads_fp64.cu
@@ -668,33 +669,11 @@ extern "C" int f3d_ads_set_wet_deposition(f3d_ctx* c, double a, double b, const 
   if (!c->grid_set) return set_err("f3d_ads_set_wet_deposition: grid not set");
   if (c->nb > 64) return set_err("f3d_ads_set_wet_deposition: at most 64 bins");
   CK(cudaSetDevice(c->device));
-  const int nx = c->nx, ny = c->ny, nz = c->nz;
-  const size_t ncol = (size_t)nx * ny;
-  std::vector<double> powpb(ncol);
-  std::vector<int> ktop(ncol);
-#define HC(i, j) h_c[(i) + (size_t)(nx + 1) * (j)]
-#define ZC(i, j, k) z_c[(i) + (size_t)(nx + 1) * ((j) + (size_t)(ny + 1) * (k))]
-  for (int j = 0; j < ny; ++j)
-    for (int i = 0; i < nx; ++i) {
-      const size_t ij = i + (size_t)nx * j;
-      powpb[ij] = pow(pre[ij], b);
-      // cells below the boundary-layer top (mod_Phys.F90:1404-1414); heights
-      // grow with k, so they are the first ktop levels of the column
-      const double ho = 0.25 * (HC(i, j) + HC(i + 1, j) + HC(i, j + 1) + HC(i + 1, j + 1));
-      int kt = 0;
-      for (int k = 0; k < nz; ++k) {
-        const double zp1 = 0.25 * (ZC(i, j, k) + ZC(i + 1, j, k) + ZC(i, j + 1, k) + ZC(i + 1, j + 1, k));
-        const double zp2 = 0.25 * (ZC(i, j, k + 1) + ZC(i + 1, j, k + 1) + ZC(i, j + 1, k + 1) +
-                                   ZC(i + 1, j + 1, k + 1));
-        const double zp = 0.5 * (zp1 + zp2);
-        const bool below = ho + zp <= pblh[ij];
-        if (below && kt != k) return set_err("f3d_ads_set_wet_deposition: heights not increasing with k");
-        if (below) kt = k + 1;
-      }
-      ktop[ij] = kt;
-    }
-#undef HC
-#undef ZC
+  const size_t ncol = (size_t)c->nx * c->ny;
+  std::vector<double> powpb;
+  std::vector<int> ktop;
+  if (!wet_tables(c->nx, c->ny, c->nz, b, pre, pblh, h_c, z_c, powpb, ktop))
+    return set_err("f3d_ads_set_wet_deposition: heights not increasing with k");
   if (!c->d_powpb) {
     if (dalloc(c, &c->d_powpb, ncol) || dalloc(c, &c->d_ktop, ncol) ||
         dalloc(c, &c->d_awet, ncol * c->nb))
@@ -703,10 +682,7 @@ extern "C" int f3d_ads_set_wet_deposition(f3d_ctx* c, double a, double b, const 
   }
   CK(cudaMemcpy(c->d_powpb, powpb.data(), ncol * 8, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_ktop, ktop.data(), ncol * 4, cudaMemcpyHostToDevice));
-  unsigned long long mask = 0;
-  for (int q = 0; q < c->nb; ++q)  // particles and radionuclides below 100 um (mod_F3D.F90:1499-1506)
-    if ((bin_cat[q] == 1 || bin_cat[q] == 3) && bin_diam[q] <= 1e-4) mask |= 1ull << q;
-  c->wet_mask = mask;
+  c->wet_mask = wet_bin_mask(c->nb, bin_cat, bin_diam);
   c->wet_a = a;
   c->wet_on = true;
   return 0;
@@ -721,32 +697,15 @@ extern "C" int f3d_ads_set_radionuclides(f3d_ctx* c, const int* bin_cat, const i
   c->rad_pkn.clear();
   if (!bin_cat || !bin_spe) return 0;
   if (c->nb > 64) return set_err("f3d_ads_set_radionuclides: at most 64 bins");
-  auto rate = [](int spe) {  // mod_Phys.F90:79-83
-    switch (spe) {
-      case 5: return 1.06e-8;
-      case 6: return 9.29e-10;
-      case 7: return 1.00e-6;
-      case 8: return 7.63e-10;
-      case 9: return 2.98e-6;
-    }
-    return -1.0;
-  };
-  int ny90 = 0, nsr90 = 0, shift = 0;
-  for (int q = 0; q < c->nb; ++q) {
-    if (bin_cat[q] == 3 && bin_spe[q] == 9 && ++ny90 == 1) shift -= q;
-    if (bin_cat[q] == 3 && bin_spe[q] == 8 && ++nsr90 == 1) shift += q;
-  }
-  if (ny90 != nsr90) return set_err("The number of SR90 and Y90 classes must be equal.");
-  for (int q = 0; q < c->nb; ++q) {
-    if (bin_cat[q] != 3) continue;
-    const double kn = rate(bin_spe[q]);
-    if (kn < 0.0) return set_err("Invalid radionuclide type: species %d", bin_spe[q]);
-    const int par = (bin_spe[q] == 9) ? q + shift : -1;
-    c->rad_bin.push_back(q);
-    c->rad_parent.push_back(par);
-    c->rad_kn.push_back(kn);
-    c->rad_pkn.push_back(par >= 0 ? rate(bin_spe[par]) : 0.0);
-  }
+  RadioSpec r;
+  int bad = 0;
+  const int rc = radio_spec(c->nb, bin_cat, bin_spe, r, &bad);
+  if (rc == 1) return set_err("The number of SR90 and Y90 classes must be equal.");
+  if (rc == 2) return set_err("Invalid radionuclide type: species %d", bad);
+  c->rad_bin = r.bin;
+  c->rad_parent = r.parent;
+  c->rad_kn = r.kn;
+  c->rad_pkn = r.pkn;
   c->radio_on = !c->rad_bin.empty();
   return 0;
 }
@@ -1243,6 +1202,7 @@ static int enqueue_wet_radio(f3d_ctx* c, double dt) {
   MemberDev& m = c->hm;
   if (c->wet_on) {
     WetArgs a;
+    memset(&a, 0, sizeof(a));
     a.nx = c->nx;
     a.ny = c->ny;
     a.nz = c->nz;

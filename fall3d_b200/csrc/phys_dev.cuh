@@ -19,6 +19,8 @@ struct WetArgs {
   double* c64;             // exact form state (or null)
   float* c32;              // precision form state (or null)
   unsigned long long mask; // bins that take wet deposition
+  const double* dt_dev;    // ensemble: the member's device time step (dta = dt * a), or null
+  double a;
 };
 
 // radioactive decay, phys_radionuclides (mod_Phys.F90:1216-1342)
@@ -35,6 +37,7 @@ struct RadioArgs {
   double* gh64;             // boundary halo layers (or null): the reference
   float* gh32;              // decays the halo cells of the state as well
   long long ngh;            // halo layer elements per bin
+  const double* fdev;       // ensemble: the member's {fact[nr], pfact[nr]} in device memory, or null
 };
 
 // per-species output reductions of nc_IO_out_res (mod_nc_IO.F90:3206-4335)

@@ -199,6 +199,48 @@ class Ensemble:
         """Zero every member's concentration, deposit and flux totals."""
         check(lib().f3d_ens_reset_state(self._h), "f3d_ens_reset_state")
 
+    def set_class_wet_deposition(self, ci, a, b, pre, pblh, bin_cat, bin_diam):
+        """Wet deposition of the members of class ci (precipitation rate and
+        boundary-layer height per column of the class grid); bin_cat=None
+        switches it off for the ensemble."""
+        g = self.grids[ci]
+        if bin_cat is None:
+            check(lib().f3d_ens_set_class_wet_deposition(self._h, ci, 0.0, 0.0, None, None, None, None, None,
+                                                         None), "f3d_ens_set_class_wet_deposition")
+            return
+        arr = [np.asfortranarray(x, dtype=np.float64) for x in (pre, pblh, g.h_c, g.z_c)]
+        cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
+        check(lib().f3d_ens_set_class_wet_deposition(self._h, ci, float(a), float(b), *[_p(x) for x in arr],
+                                                     _ip(cat), _p(np.ascontiguousarray(bin_diam, np.float64))),
+              "f3d_ens_set_class_wet_deposition")
+
+    def set_radionuclides(self, bin_cat, bin_spe):
+        cat = np.ascontiguousarray(bin_cat, dtype=np.int32)
+        spe = np.ascontiguousarray(bin_spe, dtype=np.int32)
+        check(lib().f3d_ens_set_radionuclides(self._h, _ip(cat), _ip(spe)), "f3d_ens_set_radionuclides")
+
+    def get_member_awet(self, m):
+        g = self.grids[self.member_classes[m]]
+        out = np.zeros((g.nx + 4, g.ny + 4, self.nbins), order="F")
+        check(lib().f3d_ens_get_member_awet(self._h, int(m), _p(out)), "f3d_ens_get_member_awet")
+        return out
+
+    def output_member_species(self, m, bins, col_du=False):
+        """nc_IO_out_res's per-species fields of member m at the corners."""
+        ci = self.member_classes[m]
+        g = self.grids[ci]
+        if ci not in getattr(self, "_zc_set", set()):
+            check(lib().f3d_ens_set_class_corner_heights(self._h, ci, _p(np.asfortranarray(g.z_c, np.float64))),
+                  "f3d_ens_set_class_corner_heights")
+            self._zc_set = getattr(self, "_zc_set", set()) | {ci}
+        sel = np.zeros(self.nbins, np.int32)
+        sel[list(bins)] = 1
+        keys = ("con_sur", "col_mass", "cloud_top", "grn_load")
+        out = {k: np.zeros((g.nx + 1, g.ny + 1), order="F") for k in keys}
+        check(lib().f3d_ens_output_member_species(self._h, int(m), _ip(sel), int(bool(col_du)),
+                                                  *[_p(out[k]) for k in keys]), "f3d_ens_output_member_species")
+        return out
+
     def set_profiling(self, on=True):
         check(lib().f3d_ens_set_profiling(self._h, int(bool(on))), "f3d_ens_set_profiling")
 

@@ -441,6 +441,32 @@ int f3d_ens_mass_volume(f3d_ens *ens, int member, double *mass);
  * (a fresh start without host transfers; the clocks are left to
  * f3d_ens_set_clock). */
 int f3d_ens_reset_state(f3d_ens *ens);
+/* Wet deposition and radioactive decay for every member after its sweeps,
+ * as f3d_ads_set_wet_deposition / f3d_ads_set_radionuclides do for one
+ * domain (mod_F3D.F90:1493-1520).  The precipitation, boundary layer,
+ * terrain and heights are per grid class; a, bin_cat and bin_diam are the
+ * ensemble's (bin_cat NULL switches wet deposition off).  Each member's
+ * lambda uses its own dt on the device; the decay factors exp(-kn dt) are
+ * evaluated on the host for each member's dt whenever the time steps change
+ * (f3d_ens_compute_time_steps, f3d_ens_step). */
+int f3d_ens_set_class_wet_deposition(f3d_ens *ens, int grid_class, double a,
+                                     double b, const double *pre,
+                                     const double *pblh, const double *h_c,
+                                     const double *z_c, const int *bin_cat,
+                                     const double *bin_diam);
+int f3d_ens_set_radionuclides(f3d_ens *ens, const int *bin_cat,
+                              const int *bin_spe);
+/* A member's wet deposit MY_TRA%my_awet(ips-2:ipe+2, jps-2:jpe+2, nbins). */
+int f3d_ens_get_member_awet(f3d_ens *ens, int member, double *my_awet);
+/* Corner heights of a grid class, and the per-species output reductions of
+ * nc_IO_out_res for one member (f3d_ads_output_species; the halo reads as
+ * zero). */
+int f3d_ens_set_class_corner_heights(f3d_ens *ens, int grid_class,
+                                     const double *z_c);
+int f3d_ens_output_member_species(f3d_ens *ens, int member, const int *bin_in,
+                                  int col_du, double *con_sur,
+                                  double *col_mass, double *cloud_top,
+                                  double *grn_load);
 /* Per-phase device timing: while on, f3d_ens_run enqueues steps without the
  * graph and records events between phases; ms[5] accumulates
  * {prep+source, x sweep, y sweep, z sweep, flux+clock} (persistent mode: the
