@@ -279,7 +279,8 @@ struct March {
     }
   }
 
-  // one step of the V march (RK4)
+  // one step of the V march (RK4); the steps of the last block past
+  // t = n + 7 run on ghosts and store nothing (cheaper than a branch per step)
   template <int U>
   __device__ __forceinline__ void iter_v(int t) {
     constexpr int m1 = (U + 7) & 7, m2 = (U + 6) & 7, m3 = (U + 5) & 7, m4 = (U + 4) & 7,
@@ -320,15 +321,23 @@ struct March {
     }
   }
 
+  // The march starts at t = 0 in the state the steps t < 0 would leave: every
+  // position below 0 has arrived in every stage as gL (a ghost's right-hand
+  // side is 0), the faces below 0 carry 1/dxb = 0, and the queue holds
+  // positions 0..3.  The limiter and flux values of those steps feed only
+  // ghost right-hand sides, which are multiplied by 1/dxb = 0.
   __device__ __forceinline__ void run_v() {
     o.stage_init();
     const T c0 = o.load_c(0);
     gL = o.ghost_l(c0, o.face(0).u);
     uR = o.face(n).u;
     gR = o.ghost_r(o.load_c(n - 1), uR);
-    // positions -4..-1 are already in the queue as ghosts
-    cn1 = cn2 = cn3 = cn4 = gL;
-    fq = o.face_v(-8);
+    cn1 = c0;
+    cn2 = (n > 1) ? o.load_c(1) : gR;
+    cn3 = (n > 2) ? o.load_c(2) : gR;
+    cn4 = (n > 3) ? o.load_c(3) : gR;
+    const FaceV<T> fm = o.face_v(-1);  // face 0's data with 1/dxb = 0
+    fq = o.face_v(0);
     flux_lo = flux_hi = T(0);
     S1 = StageS<T>{gL, gL, T(0), T(0), T(0), T(0)};
     S2 = S1;
@@ -338,11 +347,11 @@ struct March {
     for (int u = 0; u < 8; ++u) {
       ch[u] = gL;
       nh[u] = gL;
-      fw[u] = fq;
+      fw[u] = fm;
     }
     const int t_last = n + 7;
 #pragma unroll 1
-    for (int T0 = -8; T0 <= t_last; T0 += 8) {
+    for (int T0 = 0; T0 <= t_last; T0 += 8) {
       o.stage_begin(T0);
       if (T0 >= 8 && T0 + 7 <= n - 2) {
         block8<false>(T0);  // interior: the steady body
