@@ -323,6 +323,47 @@ struct March {
     }
   }
 
+  // The first block (t = 0..7, known at compile time): a stage's arrivals at
+  // q <= -1 only shape ghost right-hand sides (x 1/dxb = 0), so each stage
+  // starts at its arrival q = 0 (t = 2(s-1)) from the state the ghosts leave
+  // (a1 = a2 = gL, d1 = 0); nothing is stored before t = 8.
+  template <int U>
+  __device__ __forceinline__ void iter_head() {
+    constexpr int t = U;
+    constexpr int m1 = (U + 7) & 7, m2 = (U + 6) & 7, m3 = (U + 5) & 7, m4 = (U + 4) & 7,
+                  m5 = (U + 3) & 7, m6 = (U + 2) & 7, m7 = (U + 1) & 7;
+    T k1, k2, k3, k4, ff;
+    {
+      const T a = cn1;
+      cn1 = cn2;
+      cn2 = cn3;
+      cn3 = cn4;
+      const int p = t + 4;
+      const T c = o.load_c(min(p, n - 1));
+      cn4 = (p < n) ? c : gR;
+      fw[U] = fq;
+      fq = o.face_v(t + 1);
+      ch[U] = (t < n) ? a : gR;
+      o.template arrive<false>(S1, t, ch[U], fw[m1], t - 2, k1, ff);
+    }
+    if constexpr (t >= 2) {
+      const T a = o.rk_half(ch[m2], k1);
+      nh[m2] = o.rk_new1(ch[m2], k1);
+      o.template arrive<false>(S2, t - 2, a, fw[m3], t - 4, k2, ff);
+    }
+    if constexpr (t >= 4) {
+      const T a = o.rk_half(ch[m4], k2);
+      nh[m4] = o.rk_add3(nh[m4], k2);
+      o.template arrive<false>(S3, t - 4, a, fw[m5], t - 6, k3, ff);
+    }
+    if constexpr (t >= 6) {
+      const T a = o.rk_full(ch[m6], k3);
+      nh[m6] = o.rk_add3(nh[m6], k3);
+      o.template arrive<false>(S4, t - 6, a, fw[m7], t - 8, k4, ff);
+      if constexpr (t == 7) flux_lo = ff;  // face 0 of the last stage
+    }
+  }
+
   // The march starts at t = 0 in the state the steps t < 0 would leave: every
   // position below 0 has arrived in every stage as gL (a ghost's right-hand
   // side is 0), the faces below 0 carry 1/dxb = 0, and the queue holds
@@ -352,10 +393,20 @@ struct March {
       fw[u] = fm;
     }
     const int t_last = n + 7;
+    o.stage_begin(0);
+    iter_head<0>();
+    iter_head<1>();
+    iter_head<2>();
+    iter_head<3>();
+    iter_head<4>();
+    iter_head<5>();
+    iter_head<6>();
+    iter_head<7>();
+    o.stage_end(0);
 #pragma unroll 1
-    for (int T0 = 0; T0 <= t_last; T0 += 8) {
+    for (int T0 = 8; T0 <= t_last; T0 += 8) {
       o.stage_begin(T0);
-      if (T0 >= 8 && T0 + 7 <= n - 2) {
+      if (T0 + 7 <= n - 2) {
         block8<false>(T0);  // interior: the steady body
       } else {
         iter_v<0>(T0);
