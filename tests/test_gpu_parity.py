@@ -185,6 +185,29 @@ def test_fp32_form_error_vs_fp64_oracle(oracle_mod, built_lib):
     assert abs(dep_g - dep_o) <= 1e-4 * abs(dep_o)
 
 
+# nz >= 2: with one level the grid's dX3_p is 0 (no neighbour level), which
+# the reference's grid cannot be either
+@pytest.mark.parametrize("shape", [(1, 1, 2, 1), (1, 9, 2, 1), (2, 3, 2, 2), (3, 1, 5, 2), (7, 4, 3, 1),
+                                   (5, 6, 7, 2), (9, 8, 10, 3), (17, 2, 15, 2)])
+@pytest.mark.parametrize("limiter", [1, 2, 3])
+def test_fp32_form_short_pencils(oracle_mod, built_lib, shape, limiter):
+    """The precision form on pencils of 1..17 cells in every direction, where
+    the march's compile-time head block overlaps the pencil end and the edge
+    blocks carry ghost cells: FP32 bar against the FP64 oracle, boundary
+    fluxes and deposit included."""
+    nx, ny, nz, nb = shape
+    wl = W.small_case(nx, ny, nz, nb, seed=3 * nx + ny + nz, limiter=limiter)
+    c0, a0 = W.random_state(wl, seed=nx + 2 * ny + 5 * nz)
+    c0 = np.asfortranarray(c0.astype(np.float32).astype(np.float64))
+    (c_o, a_o, f_o), (c_g, a_g, f_g), _ = run_pair(oracle_mod, wl, nsteps=3, dt=2.5, c0=c0, acum0=a0,
+                                                     precision=PREC_FP32)
+    ci_o, ci_g = interior(c_o), interior(c_g)
+    assert np.linalg.norm(ci_g - ci_o) <= 1e-5 * np.linalg.norm(ci_o), shape
+    dep_o, dep_g = acum_interior(a_o).sum(), acum_interior(a_g).sum()
+    assert abs(dep_g - dep_o) <= 1e-5 * abs(dep_o) + 1e-30, (dep_o, dep_g)
+    assert np.all(np.abs(f_g - f_o) <= 1e-5 * np.abs(f_o).max() + 1e-30), (f_o, f_g)
+
+
 def test_async_steps_match_sync(oracle_mod, built_lib):
     wl = W.small_case(seed=31)
     vs = oracle_vs(oracle_mod, wl)
