@@ -44,6 +44,7 @@ SIGNATURES = {
     "f3d_ads_set_wet_deposition": [_vp, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _ip, _dp],
     "f3d_ads_set_radionuclides": [_vp, _ip, _ip],
     "f3d_ads_get_awet": [_vp, _dp],
+    "f3d_ads_mass_sink": [_vp, _dp],
     "f3d_ads_set_corner_heights": [_vp, _dp],
     "f3d_ads_keep_boundary_halo": [_vp, C.c_int],
     "f3d_ads_set_gravity_current": [_vp, _dp, _dp, _dp, _dp, _dp, _dp],
@@ -102,6 +103,7 @@ SIGNATURES = {
     "f3d_ens_get_fluxes": [_vp, _dp],
     "f3d_ens_mass_volume": [_vp, C.c_int, _dp],
     "f3d_ens_reset_state": [_vp],
+    "f3d_ens_mass_sink": [_vp, C.c_int, _dp],
     "f3d_ens_set_class_wet_deposition": [_vp, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _ip, _dp],
     "f3d_ens_set_radionuclides": [_vp, _ip, _ip],
     "f3d_ens_get_member_awet": [_vp, C.c_int, _dp],

@@ -309,6 +309,12 @@ class Domain:
               "f3d_ads_get_time_step")
         return a.value, b.value
 
+    def grid_get_mass_sink(self):
+        """grid_get_mass_sink (mod_Grid.F90:1400-1450): mass removed by wet deposition."""
+        m = C.c_double()
+        check(lib().f3d_ads_mass_sink(self._h, C.byref(m)), "f3d_ads_mass_sink")
+        return m.value
+
     def grid_get_mass_volume(self, per_bin=False):
         m = C.c_double()
         pb = np.zeros(self.nbins)

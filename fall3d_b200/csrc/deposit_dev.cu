@@ -85,6 +85,26 @@ __global__ void k_radio(RadioArgs a) {
   }
 }
 
+// Column terms of grid_get_mass_sink (mod_Grid.F90:1400-1450): the bins'
+// wet deposit summed in bin order, times dX times dY; the host adds the
+// columns in the reference's serial order (j outer, i inner).
+__global__ void k_sink_cols(int nx, int ny, int nb, const double* awet, const double* dx1p,
+                            const double* dx2p, double* col) {
+  const long long ncol = (long long)nx * ny;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < ncol;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % nx), j = (int)(e / nx);
+    double aw = 0.0;
+    for (int b = 0; b < nb; ++b) aw = aw + awet[(long long)b * ncol + e];
+    col[e] = aw * dx1p[i + 2] * dx2p[j + 2];
+  }
+}
+
+void launch_sink_cols(int nx, int ny, int nb, const double* awet, const double* dx1p,
+                      const double* dx2p, double* col, cudaStream_t st) {
+  k_sink_cols<<<296, 256, 0, st>>>(nx, ny, nb, awet, dx1p, dx2p, col);
+}
+
 void launch_wet(const WetArgs& a, cudaStream_t st) { k_wet<<<592, 256, 0, st>>>(a); }
 void launch_radio(const RadioArgs& a, cudaStream_t st) { k_radio<<<592, 256, 0, st>>>(a); }
 

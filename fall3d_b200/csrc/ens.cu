@@ -1317,6 +1317,29 @@ extern "C" int f3d_ens_get_member_awet(f3d_ens* e, int mi, double* my_awet) {
   return 0;
 }
 
+extern "C" int f3d_ens_mass_sink(f3d_ens* e, int mi, double* mass) {
+  if (!e || !mass || mi < 0 || mi >= e->nm) return set_error_msg("f3d_ens_mass_sink: bad arguments");
+  if (e->awet.empty()) {
+    *mass = 0.0 + 0.0;
+    return 0;
+  }
+  const EnsClass& k = e->cls[e->member_class[mi]];
+  ECK(cudaSetDevice(e->device));
+  const size_t ncol = (size_t)k.nx * k.ny, need = 4 * (size_t)(k.nx + 1) * (k.ny + 1);
+  if (need > e->out_cap) {
+    if (ealloc(e, &e->d_out, need)) return 1;
+    e->out_cap = need;
+  }
+  launch_sink_cols(k.nx, k.ny, e->nb, e->awet[mi], e->hm[mi].dx1p, e->hm[mi].dx2p, e->d_out, e->st);
+  e->launches += 1;
+  ECKL();
+  std::vector<double> col(ncol);
+  ECK(cudaMemcpyAsync(col.data(), e->d_out, ncol * 8, cudaMemcpyDeviceToHost, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  *mass = mass_sink_sum(k.nx, k.ny, col.data());
+  return 0;
+}
+
 extern "C" int f3d_ens_set_class_corner_heights(f3d_ens* e, int ci, const double* z_c) {
   if (!e || ci < 0 || ci >= e->ncls || !z_c) return set_error_msg("f3d_ens_set_class_corner_heights: bad arguments");
   EnsClass& k = e->cls[ci];

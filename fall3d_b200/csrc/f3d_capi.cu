@@ -1466,6 +1466,26 @@ extern "C" int f3d_ads_mass_volume(f3d_ctx* c, double* mass, double* per_bin) {
   return 0;
 }
 
+extern "C" int f3d_ads_mass_sink(f3d_ctx* c, double* mass) {
+  if (!c || !mass) return set_err("f3d_ads_mass_sink: null argument");
+  if (!c->grid_set) return set_err("f3d_ads_mass_sink: grid not set");
+  if (!c->d_awet) {  // no wet deposition: the sink is 0
+    *mass = 0.0 + 0.0;
+    return 0;
+  }
+  CK(cudaSetDevice(c->device));
+  const size_t ncol = (size_t)c->nx * c->ny;
+  if (!c->d_out && dalloc(c, &c->d_out, 4 * (size_t)(c->nx + 1) * (c->ny + 1))) return 1;
+  launch_sink_cols(c->nx, c->ny, c->nb, c->d_awet, c->hm.dx1p, c->hm.dx2p, c->d_out, c->st);
+  c->launches += 1;
+  CKL();
+  std::vector<double> col(ncol);
+  CK(cudaMemcpyAsync(col.data(), c->d_out, ncol * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *mass = mass_sink_sum(c->nx, c->ny, col.data());
+  return 0;
+}
+
 extern "C" int f3d_ads_mass_boundaries(const double fluxes[6], double* ground, double* lateral) {
   if (!fluxes || !ground || !lateral) return set_err("f3d_ads_mass_boundaries: null argument");
   *ground = std::fabs(fluxes[5]);

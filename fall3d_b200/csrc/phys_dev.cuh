@@ -144,6 +144,8 @@ struct KdArgs {
 void launch_kdiffu(const KdArgs& a, cudaStream_t st);
 
 void launch_wet(const WetArgs& a, cudaStream_t st);
+void launch_sink_cols(int nx, int ny, int nb, const double* awet, const double* dx1p,
+                      const double* dx2p, double* col, cudaStream_t st);
 void launch_radio(const RadioArgs& a, cudaStream_t st);
 void launch_out_columns(const OutArgs& a, cudaStream_t st);
 // current winds of the step with the radial wind (meteo_dev.cu)

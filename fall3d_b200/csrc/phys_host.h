@@ -93,4 +93,13 @@ inline int radio_spec(int nb, const int* bin_cat, const int* bin_spe, RadioSpec&
   return 0;
 }
 
+// grid_get_mass_sink's serial sum (mod_Grid.F90:1426-1447) over the column
+// terms, j outer, i inner, then gl_mass = 0 + the (single) rank's sum.
+inline double mass_sink_sum(int nx, int ny, const double* col) {
+  double my_mass = 0.0;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) my_mass = my_mass + col[i + (size_t)nx * j];
+  return 0.0 + my_mass;
+}
+
 }  // namespace f3d

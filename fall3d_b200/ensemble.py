@@ -219,6 +219,12 @@ class Ensemble:
         spe = np.ascontiguousarray(bin_spe, dtype=np.int32)
         check(lib().f3d_ens_set_radionuclides(self._h, _ip(cat), _ip(spe)), "f3d_ens_set_radionuclides")
 
+    def mass_sink(self, m):
+        """grid_get_mass_sink of member m."""
+        v = C.c_double()
+        check(lib().f3d_ens_mass_sink(self._h, int(m), C.byref(v)), "f3d_ens_mass_sink")
+        return v.value
+
     def get_member_awet(self, m):
         g = self.grids[self.member_classes[m]]
         out = np.zeros((g.nx + 4, g.ny + 4, self.nbins), order="F")

@@ -313,6 +313,11 @@ int f3d_mass_volume_noalloc(int nx, int ny, int nz, int nbins, const double *c,
                             const double *dX3_p, double *per_bin,
                             double *total, void *stream);
 
+/* grid_get_mass_sink (mod_Grid.F90:1400-1450): the mass removed by wet
+ * deposition, sum over columns of (sum over bins of awet) dX dY, added in the
+ * reference's serial order (the column terms are formed on the device). 0
+ * without wet deposition. */
+int f3d_ads_mass_sink(f3d_ctx *ctx, double *mass);
 /* grid_get_mass_boundaries (mod_Grid.F90:1461-1511) from fluxes {W,E,S,N,U,D}. */
 int f3d_ads_mass_boundaries(const double fluxes[6], double *ground,
                             double *lateral);
@@ -441,6 +446,8 @@ int f3d_ens_mass_volume(f3d_ens *ens, int member, double *mass);
  * (a fresh start without host transfers; the clocks are left to
  * f3d_ens_set_clock). */
 int f3d_ens_reset_state(f3d_ens *ens);
+/* grid_get_mass_sink (mod_Grid.F90:1400-1450) of one member. */
+int f3d_ens_mass_sink(f3d_ens *ens, int member, double *mass);
 /* Wet deposition and radioactive decay for every member after its sweeps,
  * as f3d_ads_set_wet_deposition / f3d_ads_set_radionuclides do for one
  * domain (mod_F3D.F90:1493-1520).  The precipitation, boundary layer,

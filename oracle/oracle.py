@@ -283,3 +283,19 @@ def mass_boundaries(fluxes):
 
 def perturb(var_id, ptype, var, random, range_):
     return lib().or_perturb(var_id, ptype, var, random, range_)
+
+
+def mass_sink(awet, grid):
+    """grid_get_mass_sink (mod_Grid.F90:1400-1450) in its serial order:
+    awet(ips-2:ipe+2, jps-2:jpe+2, nbins); a plain loop, for small grids."""
+    nx, ny, nb = awet.shape[0] - 4, awet.shape[1] - 4, awet.shape[2]
+    my_mass = 0.0
+    for j in range(ny):
+        dY = float(grid.dX2_p[j + 2])
+        for i in range(nx):
+            dX = float(grid.dX1_p[i + 2])
+            aw = 0.0
+            for b in range(nb):
+                aw = aw + float(awet[i + 2, j + 2, b])
+            my_mass = my_mass + aw * dX * dY
+    return 0.0 + my_mass

@@ -86,6 +86,7 @@ def test_ensemble_wet_decay_bitexact_to_oracle(oracle_mod, built_lib, mode):
         assert np.array_equal(acum_interior(a_o), acum_interior(a_g)), f"member {m}"
         assert np.array_equal(acum_interior(w_o), acum_interior(w_g)), f"member {m}"
         assert acum_interior(w_g)[..., 0].sum() > 0
+        assert ens.mass_sink(m) == oracle_mod.mass_sink(w_o, cls[ci].grid), f"member {m}"
     ens.close()
 
 

@@ -87,6 +87,34 @@ def test_wet_deposition_and_decay_fp32(oracle_mod, built_lib):
     assert np.abs(wb.sum() / wa.sum() - 1.0) <= 1e-5
 
 
+def test_mass_sink_bitexact(oracle_mod, built_lib):
+    """grid_get_mass_sink from the device column terms and the reference's
+    serial order: the oracle's bits."""
+    wl, pre, pblh = _case()
+    g = wl.grid
+    vs = oracle_vs(oracle_mod, wl)
+    c0, a0 = W.random_state(wl, seed=5)
+    orc = oracle_mod.Oracle(g, NB, wl.limiter, wl.time_marching, threads=4)
+    s = dense_source(g, wl.src_ijk, wl.src_vals, NB)
+    c_o, a_o = np.asfortranarray(c0.copy()), np.asfortranarray(a0.copy())
+    w_o = np.zeros((g.nx + 4, g.ny + 4, NB), order="F")
+    wet_bins = [b for b in range(NB) if CAT[b] in (1, 3) and DIAM[b] <= 1e-4]
+    dom = Domain(g, NB, wl.limiter, wl.time_marching, PREC_FP64)
+    assert dom.grid_get_mass_sink() == 0.0
+    dom.set_meteo(wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3, vs, wl.t_its, wl.t_ite)
+    dom.set_source(wl.src_ijk, wl.src_vals)
+    dom.phys_wet_deposition(A, B, pre, pblh, CAT, DIAM)
+    dom.upload_state(c0, a0)
+    for it in range(3):
+        orc.time_step(40.0, 40.0 * it, wl.t_its, wl.t_ite, it, c_o, a_o, s, wl.u12, wl.v12, wl.w12, wl.k1,
+                      wl.k2, wl.k3, vs, np.zeros(6))
+        orc.wet_deposition(40.0, A, B, pre, pblh, g.h_c, g.z_c, c_o, w_o, wet_bins)
+        dom.F3D_time_step(40.0, 40.0 * it, it)
+    ref = oracle_mod.mass_sink(w_o, g)
+    assert ref > 0 and dom.grid_get_mass_sink() == ref
+    dom.close()
+
+
 def test_radionuclide_species_checks(built_lib):
     wl, pre, pblh = _case()
     dom = Domain(wl.grid, NB)
