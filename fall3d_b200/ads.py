@@ -19,6 +19,7 @@ F3DNoConvergence (the reference's MY_ERR%flag = 2).
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -374,3 +375,54 @@ def phys_get_vset_point(diam, rhop, psi, rhoa, visc, model=2, want_iters=False):
     if rc not in (0, 2):
         check(rc, "f3d_vset_points")
     return (out, flags, iters) if want_iters else (out, flags)
+
+
+# ---- particle shape factor (per-bin setup, host) ----------------------------
+_PI = 4.0 * math.atan(1.0)  # mod_KindType.F90:43
+
+
+def phys_get_gama(diam):
+    """phys_get_gama (mod_Phys.F90:1820-1863): a/c of the prolate spheroid
+    with the surface of the sphere of diameter diam, by bisection on
+    gama in [1e-3, 1] (diam scaled by 1e3).  Returns (gama, ierr); ierr = 1
+    without convergence in 1000 iterations."""
+    d = diam * 1e3
+    toler, gmin, gmax = 1e-8, 1e-3, 1.0
+    ap = 4.0 * _PI * ((0.5 * d) * (0.5 * d))
+    gama = 0.0
+    for it in range(1, 1001):
+        gama = 0.5 * (gmin + gmax)
+        e = math.acos(gama)
+        ao = 0.5 * _PI * d * d * (gama ** (-4.0 / 3.0)) * (gama * gama + (e / math.tan(e)))
+        if ao < ap:
+            gmax = gama
+        else:
+            gmin = gama
+        if it > 1 and abs(ao - ap) < toler:
+            return gama, 0
+    return gama, 1
+
+
+def phys_get_psi(sphe, diam, modv):
+    """phys_get_psi (mod_Phys.F90:971-1069): the shape factor psi of each bin
+    for settling-velocity model modv (1 Arastopour, 2 Ganser, 3 Wilson,
+    4 Dellino, 5 Pfeiffer, 6/7 Dioguardi)."""
+    sphe = [float(x) for x in sphe]
+    diam = [float(x) for x in diam]
+    if modv == 1:
+        return np.ones(len(sphe))
+    if modv in (2, 6, 7):
+        return np.array(sphe)
+    if modv not in (3, 4, 5):
+        raise F3DError("setling velocity model not found ")
+    psi = np.zeros(len(sphe))
+    for ic, d in enumerate(diam):
+        gama, ierr = phys_get_gama(d)
+        if ierr:
+            raise F3DError("No convergence in phys_get_gama")
+        if modv == 4:  # Dellino: sphericity / circularity (Riley 1941 for prolate)
+            circula = 1.0 if gama >= 1.0 else math.sqrt(gama)
+            psi[ic] = sphe[ic] / circula
+        else:          # Wilson, Pfeiffer: (b + c) / 2a
+            psi[ic] = 0.5 * (1.0 + 1.0 / gama) if gama >= 1.0 else gama
+    return psi
