@@ -750,15 +750,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    ws, rank, local, pg = dist_setup()
     if args.impl == "reference":
+        # CPU only: rank 0 runs the reference path on the host cores, the other
+        # ranks exit at once; no process group (nor GPU) is needed
+        ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
         if args.workload == "ensemble":
             run_reference_ensemble(args, ws, rank)
         else:
             run_reference_c2(args, ws, rank)
-        if pg is not None:
-            pg.destroy_process_group()
         return
+    ws, rank, local, pg = dist_setup()
     if args.workload == "ensemble":
         res = run_ensemble(args, ws, rank, local, pg)
         res["roofline"] = ens_roofline(res, args.steps)
