@@ -147,6 +147,88 @@ def cuda_events(stream_ptr: int, device: int):
 
 
 # ---------------------------------------------------------------------------
+def run_aux(args, local):
+    """The kernels around the step on the 400x300x60x20 domain (FP32 form):
+    the meteo term from corner fields with CMAQ horizontal and similarity
+    vertical K, wet deposition, radioactive decay, the gravity current,
+    kept boundary halos, the output reductions and the mass sink.  Prints
+    event-timed costs (ms) per call or per step; the per-kernel launch list
+    comes from ncu on this workload."""
+    import torch
+    from fall3d_b200 import workloads as W
+    from fall3d_b200.ads import PREC_FP32, Domain
+    torch.cuda.set_device(local)
+    wl = W.random_c2(seed=0)
+    g = wl.grid
+    nb = wl.nbins
+    rng = np.random.default_rng(7)
+    shp = (g.nx + 1, g.ny + 1, g.nz + 1)
+    zz = (np.arange(g.nz + 1) / g.nz)[None, None, :]
+    uc = [np.asfortranarray(rng.uniform(-20.0, 20.0, shp)) for _ in range(2)]
+    vc = [np.asfortranarray(rng.uniform(-20.0, 20.0, shp)) for _ in range(2)]
+    wc = [np.asfortranarray(rng.uniform(-0.3, 0.3, shp)) for _ in range(2)]
+    tvc = [np.asfortranarray(290.0 - 40.0 * zz + rng.uniform(-2.0, 2.0, shp)) for _ in range(2)]
+    n2 = (g.nx, g.ny)
+    pblh = np.asfortranarray(rng.uniform(300.0, 2500.0, n2))
+    mon = np.asfortranarray(rng.choice([-1.0, 1.0], n2) * rng.uniform(10.0, 500.0, n2))
+    ust = np.asfortranarray(rng.uniform(0.05, 0.8, n2))
+    pre = np.asfortranarray(rng.uniform(0.0, 20.0, n2))
+    cat = np.ones(nb, np.int32)
+    spe = np.ones(nb, np.int32)
+    cat[-4:], spe[-4:] = 3, [8, 9, 6, 7]  # Sr90, Y90, Cs137, I131
+    dom = Domain(g, nb, wl.limiter, wl.time_marching, PREC_FP32, device=local)
+    st, e0, e1 = cuda_events(dom.stream_ptr, local)
+    ms = {}
+
+    def timed(name, fn, reps=1):
+        torch.cuda.synchronize(local)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(local)
+        ms[name] = round(e0.elapsed_time(e1) / reps, 4)
+
+    dom.set_terrain()
+    timed("meteo_term_cmaq_similarity_incl_h2d", lambda: dom.set_meteo_corners_kdiffu(
+        uc, vc, wc, 2, 3, 0.5, tvc_pair=tvc, pblh=pblh, mon=mon, ust=ust, t_its=0.0, t_ite=3600.0))
+    dom.phys_get_vset(wl.vset_model, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi, wl.bin_cat)
+    dom.set_source(wl.src_ijk, wl.src_vals)
+    _, dt = dom.grid_get_time_step(0.5, wl.criterion, wl.cfl, wl.run_end)
+    c0, a0 = W.random_state(wl, seed=3)
+    dom.upload_state(c0, a0)
+    K = max(args.steps, 1)
+    t = [0.0]
+
+    def steps():
+        for _ in range(K):
+            dom.step_async(dt, t[0], 0)
+            t[0] += dt
+    for _ in range(args.warmup):
+        dom.step_async(dt, t[0], 0)
+    timed("step_plain", steps)
+    ms["step_plain"] = round(ms["step_plain"] / K, 4)
+    dom.phys_wet_deposition(8.4e-5, 0.79, pre, pblh, cat, wl.diam)
+    dom.phys_radionuclides(cat, spe)
+    timed("step_wet_decay", steps)
+    ms["step_wet_decay"] = round(ms["step_wet_decay"] / K, 4)
+    dom.set_gravity_current(g.lon_p[g.nx // 2], g.lat_p[g.ny // 2], -3600.0, 1e9, 430.0, 0.1, 0.02, 0.2, 1e6,
+                            0.8 * g.z_c.max(), 0.0)
+    timed("step_wet_decay_gravity_current", steps)
+    ms["step_wet_decay_gravity_current"] = round(ms["step_wet_decay_gravity_current"] / K, 4)
+    dom.keep_boundary_halo()
+    timed("step_all_kept_halo", steps)
+    ms["step_all_kept_halo"] = round(ms["step_all_kept_halo"] / K, 4)
+    dom.nc_IO_out_res(range(nb - 4))  # first call: scratch allocation
+    dom.grid_get_mass_sink()
+    timed("output_species_incl_d2h", lambda: dom.nc_IO_out_res(range(nb - 4)), reps=3)
+    timed("mass_sink_incl_d2h", lambda: dom.grid_get_mass_sink(), reps=3)
+    dom.close()
+    print(json.dumps({"workload": f"aux: {g.nx}x{g.ny}x{g.nz} grid, {nb} bins, FP32 form",
+                      "ms": ms, "steps": K}), flush=True)
+
+
+# ---------------------------------------------------------------------------
 def sweep_bytes(wl, prec_bytes: int, d: str) -> float:
     """Algorithmic HBM bytes of one sweep launch (per the roofline model):
     c read+write per cell*bin, the per-face fields once, and for z the
@@ -746,7 +828,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c2"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c2", "aux"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -760,6 +842,9 @@ def main():
             run_reference_c2(args, ws, rank)
         return
     ws, rank, local, pg = dist_setup()
+    if args.workload == "aux":
+        run_aux(args, local)
+        return
     if args.workload == "ensemble":
         res = run_ensemble(args, ws, rank, local, pg)
         res["roofline"] = ens_roofline(res, args.steps)

@@ -176,6 +176,8 @@ struct f3d_ens {
   size_t radfact_cap = 0;
   double* d_out = nullptr;             // output reductions: 4 (nx+1)(ny+1) fields
   size_t out_cap = 0;
+  double* d_cs = nullptr;              // and the cs of the selected bins
+  size_t cs_cap = 0;
 };
 
 namespace {
@@ -1384,6 +1386,14 @@ extern "C" int f3d_ens_output_member_species(f3d_ens* e, int mi, const int* bin_
   a.hm2 = d.hm2;
   a.hm3 = d.hm3;
   a.zc = k.zc;
+  if (con_sur || col_mass || cloud_top) {
+    const size_t need = (size_t)__builtin_popcountll(a.mask) * k.nx * k.ny * k.nz;
+    if (need > e->cs_cap) {
+      if (ealloc(e, &e->d_cs, need)) return 1;
+      e->cs_cap = need;
+    }
+    a.cs = e->d_cs;
+  }
   double* outs[4] = {con_sur, col_mass, cloud_top, grn_load};
   double* dev[4];
   for (int q = 0; q < 4; ++q) dev[q] = outs[q] ? e->d_out + q * ncol : nullptr;

@@ -170,6 +170,8 @@ struct f3d_ctx {
   double gc_p[11] = {};
   std::vector<double> gc_host;  // lon_c, lat_c, lon_p, lat_p, Hm1_c
   double* d_gc_xy = nullptr;    // the same on the device
+  double* d_cs = nullptr;       // output reductions: cs of the selected bins
+  size_t cs_cap = 0;
   double* d_gh64 = nullptr;     // boundary halo layers (f3d_ads_keep_boundary_halo)
   float* d_gh32 = nullptr;
   double* d_out = nullptr;      // four (nx+1)(ny+1) output fields
@@ -986,6 +988,14 @@ extern "C" int f3d_ads_output_species(f3d_ctx* c, const int* bin_in, int col_du,
   a.zc = c->d_zc;
   a.gh64 = m.gh64;
   a.gh32 = m.gh32;
+  if (con_sur || col_mass || cloud_top) {
+    const size_t need = (size_t)__builtin_popcountll(a.mask) * c->nx * c->ny * c->nz;
+    if (need > c->cs_cap) {
+      if (dalloc(c, &c->d_cs, need)) return 1;  // the old buffer stays in the allocation list
+      c->cs_cap = need;
+    }
+    a.cs = c->d_cs;
+  }
   double* outs[4] = {con_sur, col_mass, cloud_top, grn_load};
   double* dev[4];
   for (int q = 0; q < 4; ++q) dev[q] = outs[q] ? c->d_out + q * ncol : nullptr;

@@ -32,13 +32,41 @@ namespace f3d {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// cs at mass point (i, j, k) of bin b, i in [-1, nx] and likewise j, k
-__device__ __forceinline__ double cs_at(const OutArgs& a, int b, int i, int j, int k) {
+// cs = max(0, 1e3 c / (Hm1 Hm2 Hm3)) at an interior mass point
+__device__ __forceinline__ double cs_interior(const OutArgs& a, int b, int i, int j, int k) {
+  const long long q = (((long long)b * a.nz + k) * a.ny + j) * a.nx + i;
+  const double c = a.c64 ? a.c64[q] : (double)a.c32[q];
+  const double v = 1e3 * c / (a.hm1[j] * a.hm2[j + 2] * a.hm3[i + (long long)a.nx * j]);
+  return v > 0.0 ? v : 0.0;
+}
+
+// The interior cs of the selected bins, once per mass point (every value is
+// read by the eight corners around it).
+__global__ void k_out_cs(OutArgs a) {
+  const long long ncell = (long long)a.nx * a.ny * a.nz;
+  int nsel = 0;
+  for (int b = 0; b < a.nb; ++b) nsel += (int)((a.mask >> b) & 1ull);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < ncell * nsel;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(e / ncell);
+    const long long q = e - (long long)s * ncell;
+    int b = 0;
+    for (int r = -1; b < a.nb; ++b)  // the s-th selected bin
+      if (((a.mask >> b) & 1ull) && ++r == s) break;
+    const int i = (int)(q % a.nx);
+    const long long t = q / a.nx;
+    const int j = (int)(t % a.ny), k = (int)(t / a.ny);
+    a.cs[e] = cs_interior(a, b, i, j, k);
+  }
+}
+
+// cs at mass point (i, j, k) of bin b (its index s among the selected bins),
+// i in [-1, nx] and likewise j, k
+__device__ __forceinline__ double cs_at(const OutArgs& a, int b, int s, int i, int j, int k) {
   const bool ox = i < 0 || i >= a.nx, oy = j < 0 || j >= a.ny, oz = k < 0 || k >= a.nz;
   double c;
   if (!ox && !oy && !oz) {
-    const long long q = (((long long)b * a.nz + k) * a.ny + j) * a.nx + i;
-    c = a.c64 ? a.c64[q] : (double)a.c32[q];
+    return a.cs[(((long long)s * a.nz + k) * a.ny + j) * a.nx + i];
   } else {
     if ((int)ox + (int)oy + (int)oz > 1 || (!a.gh64 && !a.gh32)) return 0.0;
     long long g;
@@ -57,13 +85,16 @@ __device__ __forceinline__ double cs_at(const OutArgs& a, int b, int i, int j, i
 // species sum of the corner means at corner (i, j, k)
 __device__ __forceinline__ double w_at(const OutArgs& a, int i, int j, int k) {
   double w = 0.0;
+  int s = 0;
   for (int b = 0; b < a.nb; ++b) {
     if (!((a.mask >> b) & 1ull)) continue;
-    const double cc = (cs_at(a, b, i, j, k) + cs_at(a, b, i - 1, j, k) + cs_at(a, b, i, j - 1, k) +
-                       cs_at(a, b, i - 1, j - 1, k) + cs_at(a, b, i, j, k - 1) + cs_at(a, b, i - 1, j, k - 1) +
-                       cs_at(a, b, i, j - 1, k - 1) + cs_at(a, b, i - 1, j - 1, k - 1)) /
+    const double cc = (cs_at(a, b, s, i, j, k) + cs_at(a, b, s, i - 1, j, k) + cs_at(a, b, s, i, j - 1, k) +
+                       cs_at(a, b, s, i - 1, j - 1, k) + cs_at(a, b, s, i, j, k - 1) +
+                       cs_at(a, b, s, i - 1, j, k - 1) + cs_at(a, b, s, i, j - 1, k - 1) +
+                       cs_at(a, b, s, i - 1, j - 1, k - 1)) /
                       8.0;
     w = w + cc;
+    ++s;
   }
   return w;
 }
@@ -117,6 +148,9 @@ __global__ void k_out_columns(OutArgs a) {
   }
 }
 
-void launch_out_columns(const OutArgs& a, cudaStream_t st) { k_out_columns<<<592, 128, 0, st>>>(a); }
+void launch_out_columns(const OutArgs& a, cudaStream_t st) {
+  if (a.con_sur || a.col_mass || a.cloud_top) k_out_cs<<<1184, 256, 0, st>>>(a);
+  k_out_columns<<<592, 128, 0, st>>>(a);
+}
 
 }  // namespace f3d

@@ -59,6 +59,8 @@ struct OutArgs {
   double* col_mass;
   double* cloud_top;
   double* grn_load;
+  double* cs;               // scratch: cs of the selected bins at the interior mass points,
+                            // [selected bin][k][j][i], formed once per call
 };
 
 // gravity current, F3D_add_radial_wind (mod_F3D.F90:978-1226): the radial
