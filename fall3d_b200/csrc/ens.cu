@@ -1387,12 +1387,14 @@ extern "C" int f3d_ens_output_member_species(f3d_ens* e, int mi, const int* bin_
   a.hm3 = d.hm3;
   a.zc = k.zc;
   if (con_sur || col_mass || cloud_top) {
-    const size_t need = (size_t)__builtin_popcountll(a.mask) * k.nx * k.ny * k.nz;
+    const size_t ncs = (size_t)__builtin_popcountll(a.mask) * k.nx * k.ny * k.nz;
+    const size_t need = ncs + (size_t)(k.nz + 1) * ncol;
     if (need > e->cs_cap) {
       if (ealloc(e, &e->d_cs, need)) return 1;
       e->cs_cap = need;
     }
     a.cs = e->d_cs;
+    a.wbuf = e->d_cs + ncs;
   }
   double* outs[4] = {con_sur, col_mass, cloud_top, grn_load};
   double* dev[4];

@@ -989,12 +989,14 @@ extern "C" int f3d_ads_output_species(f3d_ctx* c, const int* bin_in, int col_du,
   a.gh64 = m.gh64;
   a.gh32 = m.gh32;
   if (con_sur || col_mass || cloud_top) {
-    const size_t need = (size_t)__builtin_popcountll(a.mask) * c->nx * c->ny * c->nz;
+    const size_t ncs = (size_t)__builtin_popcountll(a.mask) * c->nx * c->ny * c->nz;
+    const size_t need = ncs + (size_t)(c->nz + 1) * ncol;
     if (need > c->cs_cap) {
       if (dalloc(c, &c->d_cs, need)) return 1;  // the old buffer stays in the allocation list
       c->cs_cap = need;
     }
     a.cs = c->d_cs;
+    a.wbuf = c->d_cs + ncs;
   }
   double* outs[4] = {con_sur, col_mass, cloud_top, grn_load};
   double* dev[4];

@@ -82,23 +82,6 @@ __device__ __forceinline__ double cs_at(const OutArgs& a, int b, int s, int i, i
   return v > 0.0 ? v : 0.0;
 }
 
-// species sum of the corner means at corner (i, j, k)
-__device__ __forceinline__ double w_at(const OutArgs& a, int i, int j, int k) {
-  double w = 0.0;
-  int s = 0;
-  for (int b = 0; b < a.nb; ++b) {
-    if (!((a.mask >> b) & 1ull)) continue;
-    const double cc = (cs_at(a, b, s, i, j, k) + cs_at(a, b, s, i - 1, j, k) + cs_at(a, b, s, i, j - 1, k) +
-                       cs_at(a, b, s, i - 1, j - 1, k) + cs_at(a, b, s, i, j, k - 1) +
-                       cs_at(a, b, s, i - 1, j, k - 1) + cs_at(a, b, s, i, j - 1, k - 1) +
-                       cs_at(a, b, s, i - 1, j - 1, k - 1)) /
-                      8.0;
-    w = w + cc;
-    ++s;
-  }
-  return w;
-}
-
 __device__ __forceinline__ double g_at(const double* f, const OutArgs& a, int b, int i, int j) {
   i = clampi(i, 0, a.nx - 1);
   j = clampi(j, 0, a.ny - 1);
@@ -111,12 +94,35 @@ __global__ void k_out_columns(OutArgs a) {
        e += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(e % (a.nx + 1)), j = (int)(e / (a.nx + 1));
     if (a.con_sur || a.col_mass || a.cloud_top) {
-      double wk = w_at(a, i, j, 0);
+      // species sum at every corner level, bins in order (the reference adds
+      // whole bins: my_work3d = my_work3d + my_cc(:,:,:,ib)); per bin the
+      // levels slide a window, so that level k-1's four mass points are
+      // reused from level k's step before
+      double* w = a.wbuf + e;
+      for (int k = 0; k <= a.nz; ++k) w[ncol * k] = 0.0;
+      int s = 0;
+      for (int b = 0; b < a.nb; ++b) {
+        if (!((a.mask >> b) & 1ull)) continue;
+        double p0 = cs_at(a, b, s, i, j, -1), p1 = cs_at(a, b, s, i - 1, j, -1);
+        double p2 = cs_at(a, b, s, i, j - 1, -1), p3 = cs_at(a, b, s, i - 1, j - 1, -1);
+        for (int k = 0; k <= a.nz; ++k) {
+          const double q0 = cs_at(a, b, s, i, j, k), q1 = cs_at(a, b, s, i - 1, j, k);
+          const double q2 = cs_at(a, b, s, i, j - 1, k), q3 = cs_at(a, b, s, i - 1, j - 1, k);
+          const double cc = (q0 + q1 + q2 + q3 + p0 + p1 + p2 + p3) / 8.0;
+          w[ncol * k] = w[ncol * k] + cc;
+          p0 = q0;
+          p1 = q1;
+          p2 = q2;
+          p3 = q3;
+        }
+        ++s;
+      }
+      double wk = w[0];
       if (a.con_sur) a.con_sur[e] = wk;
       double col = 0.0, top = 0.0;
       if (wk > 50e-6) top = a.zc[e];
       for (int k = 0; k < a.nz; ++k) {
-        const double wk1 = w_at(a, i, j, k + 1);
+        const double wk1 = w[ncol * (k + 1)];
         const double dz = a.zc[e + ncol * (k + 1)] - a.zc[e + ncol * k];
         col = col + 0.5 * (wk + wk1) * dz;
         if (wk1 > 50e-6) top = a.zc[e + ncol * (k + 1)];

@@ -61,6 +61,7 @@ struct OutArgs {
   double* grn_load;
   double* cs;               // scratch: cs of the selected bins at the interior mass points,
                             // [selected bin][k][j][i], formed once per call
+  double* wbuf;             // scratch: species sum at the corners, [k][corner column]
 };
 
 // gravity current, F3D_add_radial_wind (mod_F3D.F90:978-1226): the radial
