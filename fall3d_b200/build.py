@@ -66,7 +66,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
     tmp = LIB + ".tmp"
-    cmd = [nv, "-shared", "-o", tmp] + objs + ARCH + ["-lcudart_static" if False else "-cudart=static"]
+    cmd = [nv, "-shared", "-o", tmp] + objs + ARCH + ["-cudart=static"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

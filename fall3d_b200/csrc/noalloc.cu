@@ -6,8 +6,12 @@
 // framework that forbids allocation once its time loop runs.  This entry
 // point computes the mass in the volume straight from the caller's device
 // arrays and allocates nothing: the per-block partial sums it needs live in
-// a fixed file-scope __device__ array (kMaxBins x kBlocks doubles, 148 KiB),
-// which every GPU that loads the library holds until the process exits.
+// a fixed file-scope __device__ array (kMaxBins x kBlocks doubles, 148 KiB).
+// The CUDA runtime commits that array on a device when it loads this
+// library's device code there: at the first call on that device under the
+// default lazy module loading (CUDA_MODULE_LOADING=LAZY), or when the
+// context is created with eager loading.  From then on the device holds it
+// until the context ends.
 //
 // The array is shared by every call on a device and keeps the last call's
 // partials; every call overwrites all the slots it reads, so nothing has to
@@ -16,7 +20,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
 namespace f3d {
 int set_error_msg(const char* fmt, ...);  // f3d_capi.cu
@@ -25,15 +28,8 @@ namespace {
 constexpr int kMaxBins = 64;
 constexpr int kBlocks = 296;  // 2 x 148 SMs, the same grid as the context path
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) double g_mass_partials[kMaxBins * kBlocks];
-
-// Host-side cache of the array's device address, one per device.  In host
-// code the symbol g_mass_partials is only a stand-in for the device copy; the
-// address a kernel may use comes from cudaGetSymbolAddress.
-double* g_partials_addr[kMaxDevices] = {};
-std::mutex g_setup_mutex;
 
 // Same cell order and Neumaier accumulation as the context path's
 // k_mass_partial, reading the reference layout with its two-cell halos.
@@ -112,27 +108,17 @@ extern "C" int f3d_mass_volume_noalloc(int nx, int ny, int nz, int nbins, const 
                          "bins", nbins, kMaxBins);
   if (!c || !dX1_p || !dX2_p || !dX3_p || (!per_bin && !total))
     return set_error_msg("f3d_mass_volume_noalloc: null device pointer");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess)
-    return set_error_msg("f3d_mass_volume_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices)
-    return set_error_msg("f3d_mass_volume_noalloc: device %d beyond %d", dev, kMaxDevices);
-  double* partials = nullptr;
-  {
-    // one-time set-up per device, with that device current: the kernel needs
-    // the device address of the scratch array, not the host-side symbol
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_addr[dev]) {
-      void* p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_mass_partials);
-      if (e != cudaSuccess || !p)
-        return set_error_msg("f3d_mass_volume_noalloc: cudaGetSymbolAddress failed: %s",
-                             cudaGetErrorString(e));
-      g_partials_addr[dev] = static_cast<double*>(p);
-    }
-    partials = g_partials_addr[dev];
-  }
+  // In host code the symbol g_mass_partials is only a stand-in for the
+  // device copy; the address a kernel may use comes from
+  // cudaGetSymbolAddress, for the current device and its current context.
+  // It is looked up on every call (cheap once the module is loaded), so a
+  // context that was reset and created again gets its own array's address.
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_mass_partials);
+  if (e != cudaSuccess || !p)
+    return set_error_msg("f3d_mass_volume_noalloc: cudaGetSymbolAddress failed: %s",
+                         cudaGetErrorString(e));
+  double* partials = static_cast<double*>(p);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   dim3 g(kBlocks, nbins);
   k_mass_ref_partial<<<g, kThreads, 0, st>>>(c, nx, ny, nz, dX1_p, dX2_p, dX3_p, partials);

@@ -296,18 +296,22 @@ int f3d_ads_mass_volume(f3d_ctx *ctx, double *mass, double *per_bin);
  * counterpart in the reference: a variant of f3d_ads_mass_volume for code
  * whose device memory is owned by its own runtime (an OpenACC or CUDA
  * Fortran port holding my_c on the device, a pool reserved at start-up, a
- * framework that forbids allocation in its time loop).  It allocates
- * nothing and calls no allocating routine: the per-block partial sums use a
- * fixed device array of 64 bins x 296 blocks (148 KiB) that every GPU
- * loading the library keeps until exit.  All pointers are DEVICE pointers:
+ * framework that forbids allocation in its time loop).  It calls no
+ * allocating routine: the per-block partial sums use a fixed device array
+ * of 64 bins x 296 blocks (148 KiB).  The CUDA runtime commits that array
+ * when it loads this library's device code on a device, which under the
+ * default lazy module loading is the FIRST call on that device; the device
+ * then keeps it until its context ends.  So make the first call on each
+ * device before any region where allocation is forbidden and before any
+ * stream capture.  All pointers are DEVICE pointers:
  *   c      my_c (ips-2:ipe+2, jps-2:jpe+2, kps-2:kpe+2, nbins), FP64
  *   dX1_p, dX2_p, dX3_p   the grid arrays with their halos (as in set_grid)
  *   per_bin (nbins) and/or total (1): outputs, either may be NULL
  * nbins above 64 is rejected.  Work is enqueued on `stream` (a
- * cudaStream_t, NULL = default stream) and not waited for.  The first call
- * on a device looks up the scratch array's device address; make that first
- * call before any stream capture.  Calls share the array, so calls that
- * overlap on the GPU race; order them on one stream. */
+ * cudaStream_t, NULL = default stream) and not waited for.  The array's
+ * device address is looked up on every call, for the current device.
+ * Calls share the array, so calls that overlap on the GPU race; order them
+ * on one stream. */
 int f3d_mass_volume_noalloc(int nx, int ny, int nz, int nbins, const double *c,
                             const double *dX1_p, const double *dX2_p,
                             const double *dX3_p, double *per_bin,

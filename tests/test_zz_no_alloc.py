@@ -5,10 +5,12 @@ f3d_mass_volume_noalloc serves callers that cannot allocate device memory
 start-up), so it takes only device pointers the caller already holds and
 keeps its partial sums in a fixed device array.  The test allocates the
 device copies itself (the entry point never does), calls the entry point
-twice in a row on the same stream and compares both results with
-f3d_ads_mass_volume on the same state, within the 1e-13 relative tolerance
-of the mass-volume parity test.  It runs last in the suite so that a
-failure here never hides another test.
+twice in a row on the same stream and requires both results to equal
+f3d_ads_mass_volume on the same state bit for bit (both paths add the same
+cells in the same order with the same compensation).  Around the second
+call it checks the property the entry point exists for: the device's free
+memory and torch's allocated bytes do not change.  It runs last in the
+suite so that a failure here never hides another test.
 """
 import ctypes as C
 
@@ -45,14 +47,20 @@ def test_mass_volume_noalloc_matches_context_path(built_lib):
     for call in range(2):
         pb_d.fill_(-1.0)
         tot_d.fill_(-1.0)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        alloc0 = torch.cuda.memory_allocated()
         rc = lib().f3d_mass_volume_noalloc(g.nx, g.ny, g.nz, wl.nbins, vp(c_d), vp(d1), vp(d2),
                                            vp(d3), vp(pb_d), vp(tot_d), C.c_void_p(stream.cuda_stream))
         assert rc == 0, last_error()
         torch.cuda.synchronize()
+        if call == 1:  # the first call may load the module (and commit its array)
+            assert torch.cuda.mem_get_info()[0] == free0, "device memory changed across the call"
+            assert torch.cuda.memory_allocated() == alloc0
         total = float(tot_d.cpu()[0])
         pb = pb_d.cpu().numpy()
-        assert abs(total - ref_total) <= 1e-13 * abs(ref_total), (call, total, ref_total)
-        assert np.all(np.abs(pb - ref_pb) <= 1e-13 * np.abs(ref_pb)), (call, pb, ref_pb)
+        assert total == ref_total, (call, total, ref_total)
+        assert np.array_equal(pb, ref_pb), (call, pb, ref_pb)
 
 
 def test_mass_volume_noalloc_rejects_too_many_bins(built_lib):
