@@ -36,6 +36,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell·bin·steps/s on 1 B200: FP32+ensemble+MLP vs plain FP64, ≤1e-5 rel L2"
+# precision forms of the timed ensemble: FP32 stencil on the compensated
+# hi + lo state (conservative, the default), or on a plain FP32 state
+PRECISIONS = {"fp32c": 2, "fp32": 1}
+FORMS = {"fp32c": "FP32 stencils on a compensated FP32 hi + lo state with a conservative FP64 "
+                  "final update per cell (FP64 deposit, flux sums, CFL)",
+         "fp32": "FP32 state and stencils (FP64 deposit, flux sums, CFL)"}
 UNIT = "cell*bin*steps/s"
 L2_BYTES = 126 * 2**20
 
@@ -520,7 +526,7 @@ def run_ensemble(args, ws, rank, local, pg):
     ew = ensemble_workload(seed=rank)
     nm, nb = len(ew.member_class), ew.nbins
     cbs = float(ew.cell_bins())
-    out = {"workload": ew}
+    out = {"workload": ew, "state_bytes": 8 if args.precision == "fp32c" else 4}
     # ---- learned settling velocity (trained once, outside the timed region)
     t0 = time.perf_counter()
     sur = trained_surrogate(device=local)
@@ -528,7 +534,8 @@ def run_ensemble(args, ws, rank, local, pg):
     out["mlp_train_ms_device"] = round(sur.train_ms, 1)
     # ---- FP32 batched ensemble; class settling velocity by the iteration
     # (timed, for the plain arm) and then by the surrogate (kept)
-    ens = Ensemble([c.grid for c in ew.classes], nb, ew.member_class, ew.wind_factor, 2, 2, 1, local)
+    ens = Ensemble([c.grid for c in ew.classes], nb, ew.member_class, ew.wind_factor, 2, 2,
+                   PRECISIONS[args.precision], local)
     vinfo = {"iter_ms": [], "mlp_ms": [], "fallback_faces": [], "faces": []}
     for ci, wl in enumerate(ew.classes):
         ens.set_class_meteo(ci, wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3, None, wl.t_its, wl.t_ite)
@@ -548,7 +555,7 @@ def run_ensemble(args, ws, rank, local, pg):
     reps = class_reps(ew)
     steps_per_meteo = [max(1.0, METEO_INTERVAL_S / dts[m]) for m in reps]
     # ---- autotune (tile shapes / mode), then a fresh start
-    key = f"ens64-{nb}-fp32-{torch.cuda.get_device_name(local)}"
+    key = f"ens64-{nb}-{args.precision}-{torch.cuda.get_device_name(local)}"
     tune = autotune(ens, key, steps=2)
     out["tuning"] = {"mode": ["kernels+graphs", "persistent"][tune["tuning"][0]],
                      "bins_per_block": tune["tuning"][1], "ctas_per_sm": tune["tuning"][2],
@@ -585,6 +592,7 @@ def run_ensemble(args, ws, rank, local, pg):
     fp64_ms = []
     errs = []
     iter_amort = 0.0
+    flux_tot = ens.get_fluxes()  # boundary-flux totals of the W + K steps
     for ci, m in enumerate(reps):
         dom = fp64_member_domain(ew, m, local)
         g = ew.classes[ci].grid
@@ -592,9 +600,11 @@ def run_ensemble(args, ws, rank, local, pg):
         fp64_ms.append(max_over_ranks(pg, ms64))
         c64, a64 = dom.download_state()
         mv64 = dom.grid_get_mass_volume()
+        out64 = float(np.abs(dom.get_fluxes(np.zeros(6))[:5]).sum())
         dom.close()
         c32, a32 = ens.download_member_state(m)
         mv32 = ens.mass_volume(m)
+        out32 = float(np.abs(flux_tot[m, :5]).sum())
         i64, i32 = c64[2:-2, 2:-2, 2:-2, :], c32[2:-2, 2:-2, 2:-2, :]
         d64, d32 = deposit_mass(g, a64), deposit_mass(g, a32)
         errs.append({"member": m, "grid": f"{g.nx}x{g.ny}x{g.nz}",
@@ -603,7 +613,9 @@ def run_ensemble(args, ws, rank, local, pg):
                                                         max(np.linalg.norm(i64[..., q]), 1e-300)
                                                         for q in range(nb))),
                      "deposit_rel": abs(d32 / d64 - 1.0) if d64 else 0.0,
-                     "mass_rel": abs((mv32 + d32) / (mv64 + d64) - 1.0)})
+                     # mass budget: in the volume + ground deposit + out through
+                     # the lateral and top boundaries (mod_Grid.F90:1340-1511)
+                     "mass_rel": abs((mv32 + d32 + out32) / (mv64 + d64 + out64) - 1.0)})
         del c64, a64, c32, a32, i64, i32
         n_c = ew.member_class.count(ci)
         # every plain member job recomputes its own settling velocity by the iteration
@@ -620,9 +632,9 @@ def run_ensemble(args, ws, rank, local, pg):
 
 def ens_roofline(r, K):
     """Dominant kernel of the ensemble step, from event-timed profiled steps
-    in the tuned mode; algorithmic bytes: every member's concentration read
-    and written once per sweep, the class fields (shared by the members of a
-    class) once."""
+    in the tuned mode; algorithmic bytes: every member's concentration (the
+    compensated form: its hi and lo parts) read and written once per sweep,
+    the class fields (shared by the members of a class) once."""
     ens, ew = r["ens"], r["workload"]
     ens.set_profiling(True)
     ens.run(3)
@@ -638,7 +650,8 @@ def ens_roofline(r, K):
             g = wl.grid
             nmem = ew.member_class.count(ci)
             cells = g.nx * g.ny * g.nz
-            tot += nmem * 2.0 * 4 * cells * nb                 # c read + write, FP32
+            # c read + write: FP32 (4 B), or the compensated pair hi + lo (8 B)
+            tot += nmem * 2.0 * r["state_bytes"] * cells * nb
             tot += sweep_bytes(wl, 4, d) - 2.0 * 4 * cells * nb  # class fields once
         return tot
 
@@ -802,9 +815,9 @@ def line_ensemble(args, ws, res):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": "ensemble: " + ENS_CONFIG,
-                   "form": "FP32 state and stencils (FP64 deposit, flux sums, CFL), batched "
-                           "ensemble step, learned settling velocity (surrogate + one Steffensen "
-                           "correction; iteration outside the envelope), once per 1 h meteo interval",
+                   "form": FORMS[args.precision] + ", batched ensemble step, learned settling "
+                           "velocity (surrogate + one Steffensen correction; iteration outside the "
+                           "envelope), once per 1 h meteo interval",
                    "parallelism": f"replicas x{ws} (one 64-member ensemble per GPU)",
                    "l2": f"inputs larger than L2: member concentrations total "
                          f"{ew.cell_bins() * 4 / 2**30:.1f} GiB vs {L2_BYTES / 2**20:.0f} MiB L2"},
@@ -838,6 +851,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c2", "aux"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp32c", choices=sorted(PRECISIONS))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -115,6 +115,13 @@ SIGNATURES = {
     "f3d_ens_get_stream": [_vp, C.POINTER(_vp)],
     "f3d_ens_launch_count": [_vp, C.POINTER(C.c_longlong)],
     "f3d_ens_status": [_vp, _ip],
+    "f3d_ens_clear_status": [_vp],
+    "f3d_ens_autotune": [_vp, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(C.c_int), _dp, _dp],
+    "f3d_ens_check_finite": [_vp, C.c_int, _ip],
+    "f3d_ads_check_finite": [_vp, _ip],
+    "f3d_ads_solve_1d": [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp, _dp, _ip, C.c_int],
+    "f3d_set_wait_limit": [C.c_longlong],
+    "f3d_set_vset_maxit": [C.c_int],
     "f3d_mlp_create": [C.c_int, _dp, C.c_double, C.c_ulonglong, C.c_int, C.POINTER(_vp)],
     "f3d_mlp_destroy": [_vp],
     "f3d_mlp_generate": [_vp, C.c_longlong, C.c_ulonglong, C.POINTER(C.c_longlong)],

@@ -26,7 +26,7 @@ import numpy as np
 from ._lib import F3DDims, F3DError, F3DKdiffu, F3DNoConvergence, check, lib
 from .grid import ArakawaCGrid
 
-PREC_FP64, PREC_FP32 = 0, 1
+PREC_FP64, PREC_FP32, PREC_FP32C = 0, 1, 2  # FP32C: FP32 stencil, compensated hi + lo state
 _dp = C.POINTER(C.c_double)
 
 
@@ -322,6 +322,14 @@ class Domain:
         check(lib().f3d_ads_mass_volume(self._h, C.byref(m), _p(pb)), "f3d_ads_mass_volume")
         return (m.value, pb) if per_bin else m.value
 
+    def check_finite(self) -> int:
+        """On-device finite scan of the resident inputs and state: 0 when all
+        values are finite, else the bit mask of f3d_ads_check_finite
+        (1 state, 2 deposit, 4 u, 8 v, 16 w, 32 k1, 64 k2, 128 k3, 256 vs)."""
+        m = C.c_int()
+        check(lib().f3d_ads_check_finite(self._h, C.byref(m)), "f3d_ads_check_finite")
+        return m.value
+
     def phys_get_vset(self, model, rhoc, tc, diam, rhop, psi, bin_cat, is_aggregate=None,
                       vset_fac=1.0, want_host=False):
         g = self.grid
@@ -375,6 +383,38 @@ def phys_get_vset_point(diam, rhop, psi, rhoa, visc, model=2, want_iters=False):
     if rc not in (0, 2):
         check(rc, "f3d_vset_points")
     return (out, flags, iters) if want_iters else (out, flags)
+
+
+def ADS_solve_1D(c, dxp, dxb, u, k, dt, bvalue=(0.0, 0.0), flux=None, bcode=(2, 2), limiter=2,
+                 device=0):
+    """ADS_solve_1D (mod_ADS.F90:820-1053) on the GPU: RK4 of one pencil with
+    boundary codes (-1 periodic, 0 given ghosts, 1 Dirichlet, 2 free flow).
+    c (n+4, with the two ghost cells each side) is advanced in place;
+    returns (c, flux[2])."""
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    f = np.zeros(2) if flux is None else np.ascontiguousarray(flux, dtype=np.float64)
+    arr = [np.ascontiguousarray(a, dtype=np.float64) for a in (dxp, dxb, u, k)]
+    n = c.size - 4
+    if arr[0].size != n + 4 or arr[3].size != n + 4 or arr[1].size != n + 3 or arr[2].size != n + 3:
+        raise F3DError("ADS_solve_1D: c, dxp, k need n+4 values, dxb and u n+3")
+    bv = np.ascontiguousarray(bvalue, dtype=np.float64)
+    bc = np.ascontiguousarray(bcode, dtype=np.int32)
+    check(lib().f3d_ads_solve_1d(n, int(limiter), _p(c), _p(arr[0]), _p(arr[1]), _p(arr[2]),
+                                 _p(arr[3]), float(dt), _p(bv), _p(f), _ip(bc), int(device)),
+          "f3d_ads_solve_1d")
+    return c, f
+
+
+def set_wait_limit(polls: int):
+    """Poll limit of the bounded device waits (f3d_set_wait_limit); negative
+    restores the default."""
+    check(lib().f3d_set_wait_limit(int(polls)), "f3d_set_wait_limit")
+
+
+def set_vset_maxit(maxit: int):
+    """Iteration limit of the settling-velocity fixed point (maxit of
+    phys_get_vset_point, mod_Phys.F90:794); -1 restores 1000."""
+    check(lib().f3d_set_vset_maxit(int(maxit)), "f3d_set_vset_maxit")
 
 
 # ---- particle shape factor (per-bin setup, host) ----------------------------

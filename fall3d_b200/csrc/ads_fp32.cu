@@ -21,30 +21,63 @@ namespace f3d {
 
 constexpr float kEpsF = 1e-12f;
 
-// 0.5 * phi(r) * d0 with r = d1/d0  (d1 = c(i)-c(i-1), d0 = c(i+1)-c(i))
+// Three-input max (one instruction on sm_100).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ unsigned int sign_bit(float x) { return __float_as_uint(x) & 0x80000000u; }
+__device__ __forceinline__ float xor_sign(float x, unsigned int s) {
+  return __uint_as_float(__float_as_uint(x) ^ s);
+}
+
+#ifndef F3D_LIM_EPS
+#define F3D_LIM_EPS 1
+#endif
+#ifndef F3D_CMP_EFT
+#define F3D_CMP_EFT 1
+#endif
+#ifndef F3D_FFORM
+#define F3D_FFORM 0
+#endif
+
+// 0.5 * phi(r) * d0 with r = d1/d0  (d1 = c(i)-c(i-1), d0 = c(i+1)-c(i)).
+// Superbee and minmod are evaluated division-free on x = d1 sign(d0) and
+// y = |d0|, so that the sign test of r costs nothing:
+//   superbee  0.5 phi d0 = sign(d0) max(0, min(x, y/2), min(x/2, y))
+//   minmod    0.5 phi d0 = sign(d0) max(0, min(x, y)) / 2
+// (mod_ADS.F90:1124-1187).  The reference's |d0| < 1e-12 branches are kept
+// by feeding the general formula a substitute x there: x = 1e30 gives the
+// largest slope, y = |d0| (superbee phi = 2; minmod phi = 1, :1139-1140), and
+// x = -1 gives 0 (superbee with |d1| < 1e-12 too, :1171-1173).  They decide
+// the fluxes in the dilute fringe of the plume, which dominates the early
+// ground deposit.  (F3D_LIM_EPS=0 drops them: a half-slope change below
+// 1e-12 there, about 8% fewer instructions.)
 template <int LIM>
 __device__ __forceinline__ float half_phid(float d1, float d0) {
-  float pd;
-  if (LIM == 1) {  // minmod, mod_ADS.F90:1139-1147
-    float lo = fminf(d0, d1), hi = fmaxf(d0, d1);
-    pd = (d0 > 0.f) ? fmaxf(0.f, lo) : fminf(0.f, hi);
-    if (fabsf(d0) < kEpsF) pd = d0;
-  } else if (LIM == 2) {  // superbee, mod_ADS.F90:1170-1183
-    // 0.5 phi(r) d0 = sign(d0) max(min(|d1|, |d0|/2), min(|d1|/2, |d0|)) when
-    // d1 has the sign of d0, else 0 (the halving is exact, so these are the
-    // values of the two-sided form times 0.5)
-    const float a = fabsf(d0), b = fabsf(d1);
-    const float m = fmaxf(fminf(b, 0.5f * a), fminf(0.5f * b, a));
-    float h = (d0 * d1 > 0.f) ? copysignf(m, d0) : 0.f;
-    if (a < kEpsF) h = (b < kEpsF) ? 0.f : d0;
-    return h;
-  } else {  // ospre, mod_ADS.F90:1206-1219: 1.5 (r^2+r)/(r^2+r+1) * d0
+  const unsigned int sg = sign_bit(d0);
+  float x = xor_sign(d1, sg);
+  const float y = fabsf(d0);
+#if F3D_LIM_EPS
+  if (LIM == 2) {
+    const float xs = (fabsf(d1) < kEpsF) ? -1.f : 1e30f;
+    x = (y < kEpsF) ? xs : x;
+  } else if (LIM == 1) {
+    x = (y < kEpsF) ? 1e30f : x;
+  }
+#endif
+  if (LIM == 1) {  // minmod
+    return xor_sign(0.5f * fmaxf(0.f, fminf(x, y)), sg);
+  } else if (LIM == 2) {  // superbee
+    return xor_sign(max3f(0.f, fminf(x, 0.5f * y), fminf(0.5f * x, y)), sg);
+  } else {  // ospre, mod_ADS.F90:1191-1223: 1.5 (r^2+r)/(r^2+r+1) * d0
     float num = d1 * (d1 + d0);
     float den = fmaf(d1, d1 + d0, d0 * d0);
-    pd = 1.5f * num * __frcp_rn(den) * d0;
+    float pd = 1.5f * num * __frcp_rn(den) * d0;
     if (fabsf(d0) < kEpsF) pd = (fabsf(d1) < kEpsF) ? 0.f : 1.5f * d0;
+    return 0.5f * pd;
   }
-  return 0.5f * pd;
 }
 
 // Prefetch distances (march steps) of the face data and, in y and z, of the
@@ -68,10 +101,15 @@ __device__ __forceinline__ void prefetch_line(const void* p) {
 // Per-pencil operations of the precision form.  The current wind is
 // interpolated in time on the fly from the two meteo snapshots and scaled by
 // the member's wind factor (ensemble perturbation of u, v).
-template <int LIM, int DIR, int TM>
+template <int LIM, int DIR, int TM, bool CMP = false>
 struct Ops32 {
   float* cp;
   long long cs;
+  float* lop;          // CMP: low part of the state, same layout and stride as cp
+  const double* r64;   // CMP: 1/dxb of the pencil's cells, FP64
+  const float2* r2;    // CMP: the same as FP32 pairs {hi, lo}
+  double dtf;          // CMP: weight of the face sums (dt/6 for RK4, dt for Euler), FP64
+  float dtf_hi, dtf_lo;  // CMP: dtf as an FP32 pair
   const float4* fd;   // face data {u(its), u(ite), kf, 1/dxb(f-1)} (MemberDev::f4)
   const float* vsub;  // z: settling velocity of the bin
   long long vs;
@@ -106,8 +144,13 @@ struct Ops32 {
     FaceV<float> r;
     const float4 q = __ldg(fd + f * vs);
     float w = fmaf(s0, q.x, s1 * q.y);
+#if F3D_FFORM == 1
+    if (DIR == DIR_Z) r.u = fmaf(-0.5f, __ldg(vsub + f * vs), w);  // s0, s1 carry the 0.5
+    else r.u = wfac * w;                                           // wfac carries the 0.5
+#else
     if (DIR == DIR_Z) r.u = w - __ldg(vsub + f * vs);
     else r.u = wfac * w;
+#endif
     r.k = q.z;
     r.r = q.w;
     return r;
@@ -129,6 +172,50 @@ struct Ops32 {
   __device__ __forceinline__ float rk_full(float c, float k) const { return fmaf(dt, k, c); }
   __device__ __forceinline__ float rk_final(float nw, float k) const { return fmaf(dt6, k, nw); }
 
+  // Compensated final update of cell p (CMP): c(p) = hi + lo advanced by
+  // dtf (H(p+1) - H(p)) / dxb(p) in FP64 and split back into hi + lo.  The
+  // difference of two FP32 face sums is exact in FP64 and 1/dxb is FP64, so
+  // the cell's change times its volume is the two shared face sums to FP64
+  // rounding: the sweep conserves mass to ~1e-16 of the transported mass,
+  // and the state carries ~48 bits.
+  __device__ __forceinline__ float final_cmp(float chi, float hl, float hr, int p) {
+    float* lp = lop + (long long)p * cs;
+    prefetch_line(lop + (long long)min(p + 16, nf - 1) * cs);  // a later cell's low part
+    const float clo = *lp;
+#if F3D_CMP_EFT
+    // The same in FP32 pair arithmetic (error-free transformations; every
+    // operation explicitly rounded, none contracted):
+    //   hr - hl = s + e exactly (Knuth's TwoSum),
+    //   X = (s + e) (1/dxb as hi + lo), D = X (dtf as hi + lo), each to ~2^-48,
+    //   (chi + clo) + D summed with TwoSum and renormalised to hi + lo.
+    const float s = __fsub_rn(hr, hl);
+    const float sb = __fsub_rn(s, hr);
+    const float e = __fadd_rn(__fsub_rn(hr, __fsub_rn(s, sb)), __fsub_rn(-hl, sb));
+    const float2 rr = __ldg(r2 + p);
+    const float x = __fmul_rn(s, rr.x);
+    float xe = __fmaf_rn(s, rr.x, -x);
+    xe = __fmaf_rn(s, rr.y, xe);
+    xe = __fmaf_rn(e, rr.x, xe);
+    const float d = __fmul_rn(x, dtf_hi);
+    float de = __fmaf_rn(x, dtf_hi, -d);
+    de = __fmaf_rn(x, dtf_lo, de);
+    de = __fmaf_rn(xe, dtf_hi, de);
+    const float t = __fadd_rn(chi, d);
+    const float tb = __fsub_rn(t, chi);
+    float te = __fadd_rn(__fsub_rn(chi, __fsub_rn(t, tb)), __fsub_rn(d, tb));
+    te = __fadd_rn(te, __fadd_rn(clo, de));
+    const float nhi = __fadd_rn(t, te);
+    *lp = __fsub_rn(te, __fsub_rn(nhi, t));
+    return nhi;
+#else
+    const double dlt = ((double)hr - (double)hl) * (dtf * __ldg(r64 + p));
+    const double c64 = ((double)chi + (double)clo) + dlt;
+    const float nhi = __double2float_rn(c64);
+    *lp = __double2float_rn(c64 - (double)nhi);
+    return nhi;
+#endif
+  }
+
   // KT right-hand side with G = P - F per face; h = 0.5 phi(r) dc
   template <bool G>
   __device__ __forceinline__ void arrive(StageS<float>& s, int q, float a0, FaceV<float> fv, int p,
@@ -139,11 +226,15 @@ struct Ops32 {
       const float u = fv.u;
       const float cl = s.a2 + s.h2;
       const float cr = s.a1 - h1;
+#if F3D_FFORM == 1
+      // fv.u holds 0.5 u: F = 0.5 u (cl + cr) - 0.5 |u| (cr - cl)
+      const float F = fmaf(u, cl + cr, -fabsf(u) * (cr - cl));
+#else
       // 0.5 u (cl + cr) - 0.5 |u| (cr - cl) in upwind form: u+ cl + u- cr
       const float F = fmaf(fmaxf(u, 0.f), cl, fminf(u, 0.f) * cr);
-      const float Pd = fv.k * s.d1;
-      flux = F + Pd;
-      const float G0 = Pd - F;
+#endif
+      flux = fmaf(fv.k, s.d1, F);        // F + P, the boundary flux
+      const float G0 = fmaf(fv.k, s.d1, -F);  // P - F
       if (!G || q >= 2) rhs = (G0 - s.F1) * fv.r;  // fv is face q-1: r = 1/dxb(q-2)
       s.F1 = G0;
     }
@@ -175,7 +266,7 @@ __device__ __forceinline__ void block_reduce2_f64(double a, double b, double* ou
 
 // One work item (32 pencils x bpb bins of one member) of a sweep; called by
 // the per-sweep kernels and by the persistent fused step kernel.
-template <int DIR, int LIM, int TM>
+template <int DIR, int LIM, int TM, bool CMP = false>
 __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ members,
                                              const WorkItem w, int bpb, unsigned char* f3d_smem) {
   const MemberDev& m = members[w.member];
@@ -191,7 +282,7 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
   const long long pen = pen_raw < nsp ? pen_raw : nsp - 1;
   double clo = 0.0, chi = 0.0;
   if (run_it) {
-    Ops32<LIM, DIR, TM> o;
+    Ops32<LIM, DIR, TM, CMP> o;
     double area;
     int n, i = 0, j = 0;
     if (DIR == DIR_X) {
@@ -199,6 +290,11 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       int k = (int)(pen / ny);
       n = nx;
       o.cp = m.c32 + (((long long)b * nz + k) * ny + j) * nx;
+      if constexpr (CMP) {
+        o.lop = m.c32lo + (((long long)b * nz + k) * ny + j) * nx;
+        o.r64 = m.rdxb64[0];
+        o.r2 = m.rdxb2[0];
+      }
       o.xt.setup(f3d_smem + warp * decltype(o.xt)::BYTES, lane_ok ? o.cp : nullptr,
                  threadIdx.x & 31, nx);
       o.cs = 1;
@@ -212,6 +308,11 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       int k = (int)(pen / nx);
       n = ny;
       o.cp = m.c32 + ((long long)b * nz + k) * ny * (long long)nx + i;
+      if constexpr (CMP) {
+        o.lop = m.c32lo + ((long long)b * nz + k) * ny * (long long)nx + i;
+        o.r64 = m.rdxb64[1];
+        o.r2 = m.rdxb2[1];
+      }
       o.cs = nx;
       long long fo = (long long)k * (ny + 1) * nx + i;
       o.fd = (m.gc_cur ? m.gc4[1] : m.f4[1]) + fo;
@@ -223,6 +324,11 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       j = (int)(pen / nx);
       n = nz;
       o.cp = m.c32 + (long long)b * nz * ny * nx + (long long)j * nx + i;
+      if constexpr (CMP) {
+        o.lop = m.c32lo + (long long)b * nz * ny * nx + (long long)j * nx + i;
+        o.r64 = m.rdxb64[2];
+        o.r2 = m.rdxb2[2];
+      }
       o.cs = (long long)nx * ny;
       long long fo = (long long)j * nx + i;
       o.fd = m.f4[2] + fo;
@@ -239,13 +345,26 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       o.s1 = 0.f;
       o.wfac = 1.f;
     }
+#if F3D_FFORM == 1
+    if (DIR == DIR_Z) {  // the face velocity enters as 0.5 u (exact scaling)
+      o.s0 *= 0.5f;
+      o.s1 *= 0.5f;
+    } else {
+      o.wfac *= 0.5f;
+    }
+#endif
     o.nf = n;
     o.dt = (float)dt;
     o.hdt = 0.5f * o.dt;
     o.dt3 = o.dt * (1.f / 3.f);
     o.dt6 = o.dt * (1.f / 6.f);
+    if constexpr (CMP) {
+      o.dtf = (TM == 2) ? dt / 6.0 : dt;
+      o.dtf_hi = __double2float_rn(o.dtf);
+      o.dtf_lo = __double2float_rn(o.dtf - (double)o.dtf_hi);
+    }
     // the edge blocks run the unguarded body (cheaper than the guarded one)
-    March<float, Ops32<LIM, DIR, TM>, TM, true> M(o, n);
+    March<float, Ops32<LIM, DIR, TM, CMP>, TM, true, CMP> M(o, n);
     M.run();
     if (lane_ok) {
       clo = (double)M.flux_lo * area * dt;
@@ -264,16 +383,23 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
   block_reduce2_f64(clo, chi, m.flux_part + 2 * (long long)w.slot);
 }
 
-template <int DIR, int LIM, int TM>
+#ifndef F3D_CMP_BLOCKS
+#define F3D_CMP_BLOCKS 3
+#endif
+#ifndef F3D_CMP_YZ_BLOCKS
+#define F3D_CMP_YZ_BLOCKS 4
+#endif
+template <int DIR, int LIM, int TM, bool CMP>
 // 4 blocks of 128 threads per SM (128 registers); with one output buffer the
-// RK4 x tiles (4 x 12.6 KB per block) fit 4 blocks as well.
-__global__ void __launch_bounds__(128, 4) k_sweep32(const MemberDev* __restrict__ members,
-                                                 const WorkItem* __restrict__ work, int bpb) {
+// RK4 x tiles (4 x 12.6 KB per block) fit 4 blocks as well.  The compensated
+// x sweep runs 3 blocks (170 registers): at 128 it spills.
+__global__ void __launch_bounds__(128, CMP ? (DIR == DIR_X ? F3D_CMP_BLOCKS : F3D_CMP_YZ_BLOCKS) : 4)
+    k_sweep32(const MemberDev* __restrict__ members, const WorkItem* __restrict__ work, int bpb) {
   extern __shared__ __align__(16) unsigned char f3d_smem[];
-  sweep32_item<DIR, LIM, TM>(members, work[blockIdx.x], bpb, f3d_smem);
+  sweep32_item<DIR, LIM, TM, CMP>(members, work[blockIdx.x], bpb, f3d_smem);
 }
 
-template <int DIR>
+template <int DIR, bool CMP>
 static void launch_dir32(int lim, int tm, const MemberDev* members, const WorkItem* work,
                          int nblocks, int bpb, cudaStream_t st) {
   dim3 g(nblocks), b(128);
@@ -282,15 +408,15 @@ static void launch_dir32(int lim, int tm, const MemberDev* members, const WorkIt
   const int smem = (DIR == DIR_X) ? 4 * ((tm == 2) ? XTile<float, 1>::BYTES : XTile<float, 2>::BYTES) : 0;
   static bool attr_set = false;
   if (!attr_set && smem_max > 0) {
-    cudaFuncSetAttribute(k_sweep32<DIR, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(k_sweep32<DIR, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(k_sweep32<DIR, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(k_sweep32<DIR, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(k_sweep32<DIR, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(k_sweep32<DIR, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 1, 1, CMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 2, 1, CMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 3, 1, CMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 1, 2, CMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 2, 2, CMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(k_sweep32<DIR, 3, 2, CMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     attr_set = true;
   }
-#define F3D_L(L, T) k_sweep32<DIR, L, T><<<g, b, smem, st>>>(members, work, bpb)
+#define F3D_L(L, T) k_sweep32<DIR, L, T, CMP><<<g, b, smem, st>>>(members, work, bpb)
   if (tm == 1) {
     if (lim == 1) F3D_L(1, 1); else if (lim == 2) F3D_L(2, 1); else F3D_L(3, 1);
   } else {
@@ -299,12 +425,18 @@ static void launch_dir32(int lim, int tm, const MemberDev* members, const WorkIt
 #undef F3D_L
 }
 
-void launch_sweep32(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
-                    int nblocks, int bpb, cudaStream_t st) {
+void launch_sweep32(int dir, int lim, int tm, int cmp, const MemberDev* members,
+                    const WorkItem* work, int nblocks, int bpb, cudaStream_t st) {
   if (nblocks <= 0) return;
-  if (dir == DIR_X) launch_dir32<DIR_X>(lim, tm, members, work, nblocks, bpb, st);
-  else if (dir == DIR_Y) launch_dir32<DIR_Y>(lim, tm, members, work, nblocks, bpb, st);
-  else launch_dir32<DIR_Z>(lim, tm, members, work, nblocks, bpb, st);
+  if (cmp) {
+    if (dir == DIR_X) launch_dir32<DIR_X, true>(lim, tm, members, work, nblocks, bpb, st);
+    else if (dir == DIR_Y) launch_dir32<DIR_Y, true>(lim, tm, members, work, nblocks, bpb, st);
+    else launch_dir32<DIR_Z, true>(lim, tm, members, work, nblocks, bpb, st);
+  } else {
+    if (dir == DIR_X) launch_dir32<DIR_X, false>(lim, tm, members, work, nblocks, bpb, st);
+    else if (dir == DIR_Y) launch_dir32<DIR_Y, false>(lim, tm, members, work, nblocks, bpb, st);
+    else launch_dir32<DIR_Z, false>(lim, tm, members, work, nblocks, bpb, st);
+  }
 }
 
 void launch_prep32(const MemberDev* members, const int* blk_member, const int* blk_first,
@@ -321,8 +453,8 @@ __global__ void k_source32(const MemberDev* __restrict__ members, int nmembers) 
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
          e += (long long)gridDim.x * blockDim.x) {
       int q = (int)(e / m.nb), b = (int)(e % m.nb);
-      float* cc = m.c32 + (long long)b * ncell + m.src_cell[q];
-      *cc = (float)((double)*cc + m.dt * m.src_s[(long long)q * m.nb + b] / m.src_vol[q]);
+      const long long at = (long long)b * ncell + m.src_cell[q];
+      add_to_state32(m, at, m.dt * m.src_s[(long long)q * m.nb + b] / m.src_vol[q]);
     }
   }
 }
@@ -406,18 +538,18 @@ __device__ __forceinline__ void source32_all(MemberDev* members, int nmembers) {
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot;
          e += (long long)gridDim.x * blockDim.x) {
       int q = (int)(e / m.nb), b = (int)(e % m.nb);
-      float* cc = m.c32 + (long long)b * ncell + m.src_cell[q];
-      *cc = (float)((double)*cc + m.dt * m.src_s[(long long)q * m.nb + b] / m.src_vol[q]);
+      const long long at = (long long)b * ncell + m.src_cell[q];
+      add_to_state32(m, at, m.dt * m.src_s[(long long)q * m.nb + b] / m.src_vol[q]);
     }
   }
 }
 
 // Out-of-line sweep items for the persistent kernel: each direction keeps its
 // own register allocation instead of one inlined union of all three.
-template <int DIR, int LIM, int TM>
+template <int DIR, int LIM, int TM, bool CMP>
 __device__ __noinline__ void sweep32_item_call(MemberDev* members, WorkItem w, int bpb,
                                                unsigned char* smem) {
-  sweep32_item<DIR, LIM, TM>(members, w, bpb, smem);
+  sweep32_item<DIR, LIM, TM, CMP>(members, w, bpb, smem);
 }
 
 // One whole time step of every member in one persistent kernel: source,
@@ -426,13 +558,13 @@ __device__ __noinline__ void sweep32_item_call(MemberDev* members, WorkItem w, i
 // work items from per-phase atomic counters (members of uneven size balance
 // themselves) and meet at bounded grid barriers between phases.  Launched
 // cooperatively so that every block is resident.
-template <int LIM, int TM>
+template <int LIM, int TM, bool CMP>
 __global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
   extern __shared__ __align__(16) unsigned char f3d_smem[];
   __shared__ int slot;
   __shared__ double sa[128], sb[128];
   source32_all(a.members, a.nmembers);
-  grid_barrier(a.counters + 6, a.err);
+  grid_barrier(a.counters + 6, a.err, a.wait_limit);
   const bool xfirst = (a.members[0].iiter % 2) == 0;
   for (int ph = 0; ph < 3; ++ph) {
     const int dir = (ph == 2) ? 2 : (((ph == 0) == xfirst) ? 0 : 1);
@@ -440,11 +572,11 @@ __global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
       const int it = grab_item(a.counters + ph, &slot);
       if (it >= a.nwork[dir]) break;
       const WorkItem w = a.work[dir][it];
-      if (dir == 0) sweep32_item_call<0, LIM, TM>(a.members, w, a.bpb, f3d_smem);
-      else if (dir == 1) sweep32_item_call<1, LIM, TM>(a.members, w, a.bpb, f3d_smem);
-      else sweep32_item_call<2, LIM, TM>(a.members, w, a.bpb, f3d_smem);
+      if (dir == 0) sweep32_item_call<0, LIM, TM, CMP>(a.members, w, a.bpb, f3d_smem);
+      else if (dir == 1) sweep32_item_call<1, LIM, TM, CMP>(a.members, w, a.bpb, f3d_smem);
+      else sweep32_item_call<2, LIM, TM, CMP>(a.members, w, a.bpb, f3d_smem);
     }
-    grid_barrier(a.counters + 6, a.err);
+    grid_barrier(a.counters + 6, a.err, a.wait_limit);
   }
   for (int mi = blockIdx.x; mi < a.nmembers; mi += gridDim.x) {
     member_flux_reduce(a.members[mi], 7, sa, sb);
@@ -455,15 +587,20 @@ __global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
 
 int fused32_smem() { return 4 * XTile<float, 2>::BYTES; }
 
-const void* fused32_func(int lim, int tm) {
+template <bool CMP>
+static const void* fused32_func_t(int lim, int tm) {
   if (tm == 1) {
-    if (lim == 1) return (const void*)k_fused32<1, 1>;
-    if (lim == 2) return (const void*)k_fused32<2, 1>;
-    return (const void*)k_fused32<3, 1>;
+    if (lim == 1) return (const void*)k_fused32<1, 1, CMP>;
+    if (lim == 2) return (const void*)k_fused32<2, 1, CMP>;
+    return (const void*)k_fused32<3, 1, CMP>;
   }
-  if (lim == 1) return (const void*)k_fused32<1, 2>;
-  if (lim == 2) return (const void*)k_fused32<2, 2>;
-  return (const void*)k_fused32<3, 2>;
+  if (lim == 1) return (const void*)k_fused32<1, 2, CMP>;
+  if (lim == 2) return (const void*)k_fused32<2, 2, CMP>;
+  return (const void*)k_fused32<3, 2, CMP>;
+}
+
+const void* fused32_func(int lim, int tm, int cmp) {
+  return cmp ? fused32_func_t<true>(lim, tm) : fused32_func_t<false>(lim, tm);
 }
 
 }  // namespace f3d

@@ -47,13 +47,20 @@ struct Ops64 {
   long long vs;
   const double* kk;    // 0.5 (k(f) + k(f-1)) at face f, same stride
   const double4* geo;  // {dxp(p), 1/dxp(p), dxb(p), 1/dxb(p)} at geo[p + 1]
+  int nf;              // cells of the pencil (faces 0..nf)
   double dt, hdt;
   XTile<double> xt;    // x pencils: shared-memory staging of the rows
 
   __device__ __forceinline__ double load_c(int p) const {
-    if constexpr (DIR == DIR_X) return xt.load(p);
-    else return cp[p * cs];
+    if constexpr (DIR == DIR_X) {
+      return xt.load(p);
+    } else {
+      // the line of a later position into L1 ahead of its load
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(cp + (long long)min(p + 8, nf - 1) * cs));
+      return cp[p * cs];
+    }
   }
+  __device__ __forceinline__ double load_last() const { return cp[(long long)(nf - 1) * cs]; }
   __device__ __forceinline__ void store_c(int p, double v) {
     if constexpr (DIR == DIR_X) xt.store(p, v);
     else cp[p * cs] = v;
@@ -63,6 +70,12 @@ struct Ops64 {
   __device__ __forceinline__ void stage_end(int T0) { if constexpr (DIR == DIR_X) xt.block_end(T0); }
   __device__ __forceinline__ void stage_finish() { if constexpr (DIR == DIR_X) xt.finish(); }
   __device__ __forceinline__ FaceV<double> face(int f) const {
+    {
+      const long long fp = (long long)min(f + 8, nf) * vs;
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(vel + fp));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(kk + fp));
+      if (DIR == DIR_Z) asm volatile("prefetch.global.L1 [%0];" ::"l"(vsub + fp));
+    }
     FaceV<double> r;
     r.u = vel[f * vs];
     if (DIR == DIR_Z) r.u = r.u - vsub[f * vs];  // CB%w - my_vs  (mod_ADS.F90:670)
@@ -70,6 +83,10 @@ struct Ops64 {
     r.r = 0.0;  // the exact form reads its metrics from geo
     return r;
   }
+  // face data for the unguarded march (faces outside [0, nf] read the end
+  // faces; the right-hand side of a cell outside the pencil is set to 0 in
+  // arrive, so its stage values stay the frozen ghost value exactly)
+  __device__ __forceinline__ FaceV<double> face_v(int f) const { return face(min(max(f, 0), nf)); }
   // free flow (mod_ADS.F90:1227-1326) with bvalue = 0
   __device__ __forceinline__ double ghost_l(double c0, double uL) const {
     return (uL > 0.0) ? 2.0 * 0.0 - c0 : c0;
@@ -104,10 +121,11 @@ struct Ops64 {
       const double F_l = cl * u;
       const double F_r = cr * u;
       const double F0 = 0.5 * (F_l + F_r) - 0.5 * fabs(u) * (cr - cl);
-      const double4 g = geo[p + 1];
+      const double4 g = geo[min(max(p + 1, 0), nf)];
       const double P0 = div_rn_recip(fv.k * s.d1, g.x, g.y);
       flux = F0 + P0;
       if (!G || q >= 2) rhs = div_rn_recip(P0 - s.P1, g.z, g.w) - div_rn_recip(F0 - s.F1, g.z, g.w);
+      if (!G) rhs = (p >= 0 && p < nf) ? rhs : 0.0;  // ghost cells of the unguarded march
       s.F1 = F0;
       s.P1 = P0;
     }
@@ -200,9 +218,11 @@ __device__ __forceinline__ void sweep64_item(const MemberDev* __restrict__ membe
       area = m.dx2b[j + 1] * m.dx1b[i + 1];
     }
     o.geo = m.geo[DIR];
+    o.nf = n;
     o.dt = m.dt;
     o.hdt = 0.5 * m.dt;
-    March<double, Ops64<LIM, DIR>, TM> M(o, n);
+    // RK4: the edge blocks run the unguarded body (cheaper than the guarded one)
+    March<double, Ops64<LIM, DIR>, TM, true> M(o, n);
     M.run();
     const double dt = m.dt;
     if (lane_ok) {
@@ -360,7 +380,7 @@ __global__ void __launch_bounds__(128) k_fused64(FusedArgs a) {
     prep64_range(a.members[mi], (long long)(it - a.prep_first[mi]) * 256, 256, 7);
   }
   source64_all(a.members, a.nmembers);
-  grid_barrier(a.counters + 6, a.err);
+  grid_barrier(a.counters + 6, a.err, a.wait_limit);
   const bool xfirst = (a.members[0].iiter % 2) == 0;
   for (int ph = 0; ph < 3; ++ph) {
     const int dir = (ph == 2) ? 2 : (((ph == 0) == xfirst) ? 0 : 1);
@@ -372,7 +392,7 @@ __global__ void __launch_bounds__(128) k_fused64(FusedArgs a) {
       else if (dir == 1) sweep64_item_call<1, LIM, TM>(a.members, w, a.bpb, f3d_smem);
       else sweep64_item_call<2, LIM, TM>(a.members, w, a.bpb, f3d_smem);
     }
-    grid_barrier(a.counters + 6, a.err);
+    grid_barrier(a.counters + 6, a.err, a.wait_limit);
   }
   for (int mi = blockIdx.x; mi < a.nmembers; mi += gridDim.x) {
     member_flux_reduce(a.members[mi], 7, sa, sb);

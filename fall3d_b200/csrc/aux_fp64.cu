@@ -396,7 +396,7 @@ __global__ void k_mass_partial(const MemberDev* __restrict__ members, int mi, in
     long long t = e / nx;
     int j = (int)(t % ny);
     int k = (int)(t / ny);
-    double c = fp32 ? (double)m.c32[(long long)b * ncell + e] : m.c64[(long long)b * ncell + e];
+    double c = fp32 ? state32(m, (long long)b * ncell + e) : m.c64[(long long)b * ncell + e];
     double x = c * m.dx1p[i + 2] * m.dx2p[j + 2] * m.dx3p[k + 2];
     double tt = acc + x;
     if (fabs(acc) >= fabs(x)) comp += (acc - tt) + x; else comp += (x - tt) + acc;
@@ -440,11 +440,11 @@ void launch_mass(const MemberDev* members, int mi, int nb, int fp32, double* par
 // ---- settling velocity: phys_get_vset_point, see vset.cuh --------------------
 __global__ void k_vset_points(int model, int n, const double* diam, const double* rhop,
                               const double* psi, const double* rhoa, const double* visc,
-                              double* vset, int* flags, int* iters, int* nfail) {
+                              double* vset, int* flags, int* iters, int* nfail, int maxit) {
   GRID_STRIDE(q, (long long)n) {
     int it;
     double v;
-    int fl = vset_point_dev(diam[q], rhop[q], psi[q], rhoa[q], visc[q], model, &v, &it);
+    int fl = vset_point_dev(diam[q], rhop[q], psi[q], rhoa[q], visc[q], model, &v, &it, maxit);
     vset[q] = v;
     flags[q] = fl;
     if (iters) iters[q] = it;
@@ -455,7 +455,7 @@ void launch_vset_points(int model, int n, const double* diam, const double* rhop
                         const double* psi, const double* rhoa, const double* visc, double* vset,
                         int* flags, int* iters, int* nfail, cudaStream_t st) {
   k_vset_points<<<592, 128, 0, st>>>(model, n, diam, rhop, psi, rhoa, visc, vset, flags, iters,
-                                      nfail);
+                                      nfail, vset_maxit());
 }
 
 // phys_get_vset (mod_Phys.F90:673-740) + vs/Hm3 (mod_Grid.F90:996-1005).
@@ -463,7 +463,7 @@ void launch_vset_points(int model, int n, const double* diam, const double* rhop
 // in bin_par[3*b..], bin_flags[b] = cat | (aggregate << 8).
 __global__ void k_vset_field(MemberDev* members, int mi, int model, const double* rhoc,
                              const double* tc, const double* bin_par, const int* bin_flags,
-                             double vset_fac, int* nfail) {
+                             double vset_fac, int* nfail, int maxit) {
   const MemberDev& m = members[mi];
   const int nx = m.nx, ny = m.ny, nz = m.nz, nb = m.nb;
   const long long cx = nx + 1, cy = ny + 1;
@@ -486,7 +486,7 @@ __global__ void k_vset_field(MemberDev* members, int mi, int model, const double
     if ((fl & 0xff) != 2) {
       int it;
       int f = vset_point_dev(bin_par[3 * b], bin_par[3 * b + 1], bin_par[3 * b + 2], rhoa, visa,
-                             model, &v, &it);
+                             model, &v, &it, maxit);
       if (f) atomicAdd(nfail, 1);
     }
     if (fl >> 8) v = vset_fac * v;
@@ -498,7 +498,131 @@ void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc
                        const double* tc, const double* bin_par, const int* bin_flags,
                        double vset_fac, int* nfail, cudaStream_t st) {
   k_vset_field<<<1184, 128, 0, st>>>(members, mi, model, rhoc, tc, bin_par, bin_flags, vset_fac,
-                                     nfail);
+                                     nfail, vset_maxit());
 }
 
+// ---- finite scan: diagnostics of NaN/Inf-poisoned inputs --------------------
+// Sets bit `bit` of *mask when any of the n values is NaN or infinite.
+template <class T>
+__global__ void k_nonfinite(const T* __restrict__ p, long long n, int bit, unsigned int* mask) {
+  bool bad = false;
+  GRID_STRIDE(e, n) {
+    if (!isfinite(p[e])) bad = true;
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(mask, 1u << bit);
+}
+void launch_nonfinite(const double* p, long long n, int bit, unsigned int* mask, cudaStream_t st) {
+  if (p && n > 0) k_nonfinite<<<592, 256, 0, st>>>(p, n, bit, mask);
+}
+void launch_nonfinite(const float* p, long long n, int bit, unsigned int* mask, cudaStream_t st) {
+  if (p && n > 0) k_nonfinite<<<592, 256, 0, st>>>(p, n, bit, mask);
+}
+
+}  // namespace f3d
+
+namespace f3d {
+// ---- ADS_solve_1D (mod_ADS.F90:820-1053) -----------------------------------
+// One pencil of n cells in one block: the boundary codes set the ghost cells
+// (-1 periodic when the face velocity enters, 0 as given, 1 Dirichlet, 2
+// free flow: Dirichlet on inflow, zero gradient on outflow), then RK4 with
+// four KT_RHS evaluations (:1057-1120) whose limiter, reconstruction and
+// fluxes are computed cell-parallel between block barriers, in the
+// reference's operation order (this file is compiled with --fmad=false; the
+// divisions are IEEE divisions).  The serial reference's halo swaps are
+// no-ops, so the ghosts stay as set.  Arrays (device) with the reference
+// offsets: c, dxp, k from ips-2; dxb, u from ibs-1; w (scratch) holds
+// c0 (n+4), r (n+4), cl and cr (n+3 each) and k1..k4 (n each).
+__device__ void kt_rhs_block(int n, int lim, const double* c, const double* dxp, const double* dxb,
+                             const double* u, const double* k, double* r, double* cl, double* cr,
+                             double* rhs, double* flux) {
+  for (int p = -1 + (int)threadIdx.x; p <= n; p += blockDim.x) {
+    const double cm = c[p + 1], c0 = c[p + 2], cp = c[p + 3];
+    double rv;
+    if (fabs(cp - c0) < kEps) {
+      rv = (lim == 1) ? 1.0 : ((fabs(c0 - cm) < kEps) ? 0.0 : (lim == 2 ? 2.0 : 1.5));
+    } else {
+      const double rr = (c0 - cm) / (cp - c0);
+      if (lim == 1) rv = fmax(0.0, fmin(1.0, rr));
+      else if (lim == 2) rv = fmax(fmax(0.0, fmin(2.0 * rr, 1.0)), fmin(rr, 2.0));
+      else rv = 1.5 * (rr * rr + rr) / (rr * rr + rr + 1.0);
+    }
+    r[p + 2] = rv;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    r[0] = r[1];          // r(ips-2) = r(ips-1)
+    r[n + 3] = r[n + 2];  // r(ipe+2) = r(ipe+1)
+  }
+  __syncthreads();
+  for (int p = -1 + (int)threadIdx.x; p <= n; p += blockDim.x) {
+    cr[p + 1] = c[p + 2] - 0.5 * r[p + 2] * (c[p + 3] - c[p + 2]);
+    cl[p + 1] = c[p + 1] + 0.5 * r[p + 1] * (c[p + 2] - c[p + 1]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double ui = u[i + 1], up = u[i + 2];
+    const double F_m = 0.5 * (cl[i + 1] * ui + cr[i + 1] * ui) - 0.5 * fabs(ui) * (cr[i + 1] - cl[i + 1]);
+    const double F_p = 0.5 * (cl[i + 2] * up + cr[i + 2] * up) - 0.5 * fabs(up) * (cr[i + 2] - cl[i + 2]);
+    const double P_m = 0.5 * (k[i + 2] + k[i + 1]) * (c[i + 2] - c[i + 1]) / dxp[i + 1];
+    const double P_p = 0.5 * (k[i + 3] + k[i + 2]) * (c[i + 3] - c[i + 2]) / dxp[i + 2];
+    rhs[i] = -1.0 * (F_p - F_m) / dxb[i + 1] + (P_p - P_m) / dxb[i + 1];
+    if (i == 0) flux[0] = F_m + P_m;
+    if (i == n - 1) flux[1] = F_p + P_p;
+  }
+  __syncthreads();
+}
+
+__global__ void k_ads_solve_1d(int n, int lim, double* c, const double* dxp, const double* dxb,
+                               const double* u, const double* k, double dt, double bv0, double bv1,
+                               int bc0, int bc1, double* flux, double* w) {
+  double* c0 = w;
+  double* r = c0 + (n + 4);
+  double* cl = r + (n + 4);
+  double* cr = cl + (n + 3);
+  double* k1 = cr + (n + 3);
+  double* k2 = k1 + n;
+  double* k3 = k2 + n;
+  double* k4 = k3 + n;
+  if (threadIdx.x == 0) {  // boundary conditions (:880-942)
+    const double uL = u[1], uR = u[n + 1];
+    if (bc0 == -1) {
+      if (uL > 0.0) { c[1] = c[n + 1]; c[0] = c[n]; c[n + 2] = c[2]; c[n + 3] = c[3]; }
+    } else if (bc0 == 1) {
+      c[1] = 2.0 * bv0 - c[2]; c[0] = c[1];
+    } else if (bc0 == 2) {
+      if (uL > 0.0) c[1] = 2.0 * bv0 - c[2]; else c[1] = c[2];
+      c[0] = c[1];
+    }
+    if (bc1 == -1) {
+      if (uR < 0.0) { c[1] = c[n + 1]; c[0] = c[n]; c[n + 2] = c[2]; c[n + 3] = c[3]; }
+    } else if (bc1 == 1) {
+      c[n + 2] = 2.0 * bv1 - c[n + 1]; c[n + 3] = c[n + 2];
+    } else if (bc1 == 2) {
+      if (uR < 0.0) c[n + 2] = 2.0 * bv1 - c[n + 1]; else c[n + 2] = c[n + 1];
+      c[n + 3] = c[n + 2];
+    }
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < n + 4; p += blockDim.x) c0[p] = c[p];  // with the halos (:946)
+  __syncthreads();
+  kt_rhs_block(n, lim, c0, dxp, dxb, u, k, r, cl, cr, k1, flux);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) c0[i + 2] = c[i + 2] + 0.5 * dt * k1[i];
+  __syncthreads();
+  kt_rhs_block(n, lim, c0, dxp, dxb, u, k, r, cl, cr, k2, flux);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) c0[i + 2] = c[i + 2] + 0.5 * dt * k2[i];
+  __syncthreads();
+  kt_rhs_block(n, lim, c0, dxp, dxb, u, k, r, cl, cr, k3, flux);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) c0[i + 2] = c[i + 2] + dt * k3[i];
+  __syncthreads();
+  kt_rhs_block(n, lim, c0, dxp, dxb, u, k, r, cl, cr, k4, flux);
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    c[i + 2] = c[i + 2] + dt * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]) / 6.0;
+}
+
+void launch_ads_solve_1d(int n, int lim, double* c, const double* dxp, const double* dxb,
+                         const double* u, const double* k, double dt, const double bvalue[2],
+                         const int bcode[2], double* flux, double* work, cudaStream_t st) {
+  k_ads_solve_1d<<<1, 256, 0, st>>>(n, lim, c, dxp, dxb, u, k, dt, bvalue[0], bvalue[1], bcode[0],
+                                    bcode[1], flux, work);
+}
 }  // namespace f3d

@@ -44,6 +44,13 @@ __global__ void k_wet(WetArgs a) {
         const double cv = a.c64[q];
         aw = aw + a.dx3p[k + 2] * lambda * cv;
         a.c64[q] = cv * (1.0 - lambda);
+      } else if (a.c32lo) {  // compensated pair: FP64 value, split back
+        const double cv = (double)a.c32[q] + (double)a.c32lo[q];
+        aw = aw + a.dx3p[k + 2] * lambda * cv;
+        const double nv = cv * (1.0 - lambda);
+        const float hi = __double2float_rn(nv);
+        a.c32[q] = hi;
+        a.c32lo[q] = __double2float_rn(nv - (double)hi);
       } else {
         const double cv = (double)a.c32[q];
         aw = aw + a.dx3p[k + 2] * lambda * cv;
@@ -65,6 +72,24 @@ __device__ __forceinline__ void decay_cell(const RadioArgs& a, T* c, long long q
   }
 }
 
+// The same on the compensated pair hi + lo of the precision form.
+__device__ __forceinline__ void decay_cell_pair(const RadioArgs& a, float* hi, float* lo, long long q,
+                                                long long stride) {
+  for (int r = 0; r < a.nr; ++r) {
+    const double f = a.fdev ? a.fdev[r] : a.fact[r];
+    const double pf = a.fdev ? a.fdev[a.nr + r] : a.pfact[r];
+    const long long at = (long long)a.bin[r] * stride + q;
+    double v = ((double)hi[at] + (double)lo[at]) * f;
+    if (a.parent[r] >= 0) {
+      const long long pa = (long long)a.parent[r] * stride + q;
+      v = ((double)hi[pa] + (double)lo[pa]) * (1.0 - pf);
+    }
+    const float h = __double2float_rn(v);
+    hi[at] = h;
+    lo[at] = __double2float_rn(v - (double)h);
+  }
+}
+
 __global__ void k_radio(RadioArgs a) {
   const long long n2 = (long long)a.nx * a.ny, n3 = n2 * a.nz;
   const long long ng = (a.gh64 || a.gh32) ? a.ngh : 0;
@@ -72,6 +97,7 @@ __global__ void k_radio(RadioArgs a) {
        e += (long long)gridDim.x * blockDim.x) {
     if (e < n3) {
       if (a.c64) decay_cell(a, a.c64, e, n3);
+      else if (a.c32lo) decay_cell_pair(a, a.c32, a.c32lo, e, n3);
       else decay_cell(a, a.c32, e, n3);
     } else if (e < n3 + n2) {
       const long long q = e - n3;

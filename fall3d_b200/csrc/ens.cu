@@ -11,7 +11,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/fall3d_ads.h"
@@ -24,8 +26,8 @@ namespace f3d {
 int set_error_msg(const char* fmt, ...);
 void launch_sweep64(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
                     int nblocks, int bpb, cudaStream_t st);
-void launch_sweep32(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
-                    int nblocks, int bpb, cudaStream_t st);
+void launch_sweep32(int dir, int lim, int tm, int cmp, const MemberDev* members,
+                    const WorkItem* work, int nblocks, int bpb, cudaStream_t st);
 void launch_prep64(const MemberDev* members, const int* blk_member, const int* blk_first,
                    int nblocks, int mask, cudaStream_t st);
 void launch_source64(const MemberDev* members, int nmembers, cudaStream_t st);
@@ -62,6 +64,8 @@ void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, c
 void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
                          double* k3, cudaStream_t st);
 void launch_face_kk(MemberDev* members, int mi, cudaStream_t st);
+void launch_nonfinite(const double* p, long long n, int bit, unsigned int* mask, cudaStream_t st);
+void launch_nonfinite(const float* p, long long n, int bit, unsigned int* mask, cudaStream_t st);
 void launch_fp32_fields(MemberDev* members, int mi, cudaStream_t st);
 void launch_set_steps(MemberDev* members, int n, const double* dt, const double* time, int iiter,
                       cudaStream_t st);
@@ -70,7 +74,7 @@ void launch_finalize_dt(MemberDev* members, int n, const double* red, double cfl
                         cudaStream_t st);
 int fused32_smem();
 int fused64_smem();
-const void* fused32_func(int lim, int tm);
+const void* fused32_func(int lim, int tm, int cmp);
 const void* fused64_func(int lim, int tm);
 }  // namespace f3d
 
@@ -108,6 +112,8 @@ struct EnsClass {
   float4* f4[3] = {nullptr, nullptr, nullptr};  // FP32 face data (MemberDev::f4)
   float* vs32 = nullptr;
   float* rdx[3] = {nullptr, nullptr, nullptr};
+  double* rdx64[3] = {nullptr, nullptr, nullptr};  // compensated form: 1/dxb in FP64
+  float2* rdx2[3] = {nullptr, nullptr, nullptr};   // and as FP32 pairs {hi, lo}
   double* dx[6] = {};   // dx1p dx1b dx2p dx2b dx3p dx3b
   double* hm[3] = {};   // hm1 hm2 hm3
   std::vector<double> dX1_p, dX2_p, dX3_p, Hm1_p, Hm2_p, Hm3_p;
@@ -126,6 +132,7 @@ struct EnsClass {
 
 struct f3d_ens {
   int ncls = 0, nm = 0, nb = 0, lim = 2, tm = 2, prec = 0, device = 0;
+  int cmp = 0;  // precision form with the compensated (hi + lo) state
   int mode = F3D_ENS_MODE_KERNELS, bpb = 4, ctas_per_sm = 0;
   cudaStream_t st = nullptr;
   std::vector<EnsClass> cls;
@@ -326,8 +333,10 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
   if (limiter < 1 || limiter > 3) return set_error_msg("f3d_ens_create: limiter %d not in 1..3", limiter);
   if (time_marching < 1 || time_marching > 2)
     return set_error_msg("f3d_ens_create: time_marching %d not in 1..2", time_marching);
-  if (precision != F3D_PREC_FP64 && precision != F3D_PREC_FP32)
+  if (precision != F3D_PREC_FP64 && precision != F3D_PREC_FP32 && precision != F3D_PREC_FP32C)
     return set_error_msg("f3d_ens_create: precision %d unknown", precision);
+  const int cmp = precision == F3D_PREC_FP32C;
+  if (cmp) precision = F3D_PREC_FP32;
   const int nb = dims[0].nbins;
   for (int c = 0; c < nclasses; ++c)
     if (dims[c].nx < 1 || dims[c].ny < 1 || dims[c].nz < 1 || dims[c].nbins != nb)
@@ -344,6 +353,7 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
   e->lim = limiter;
   e->tm = time_marching;
   e->prec = precision;
+  e->cmp = cmp;
   e->device = device;
   e->cls.resize(nclasses);
   e->member_class.resize(nmembers);
@@ -384,6 +394,14 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
       rc |= ealloc(e, &k.rdx[0], nx);
       rc |= ealloc(e, &k.rdx[1], ny);
       rc |= ealloc(e, &k.rdx[2], nz);
+      if (cmp) {
+        rc |= ealloc(e, &k.rdx64[0], nx);
+        rc |= ealloc(e, &k.rdx64[1], ny);
+        rc |= ealloc(e, &k.rdx64[2], nz);
+        rc |= ealloc(e, &k.rdx2[0], nx);
+        rc |= ealloc(e, &k.rdx2[1], ny);
+        rc |= ealloc(e, &k.rdx2[2], nz);
+      }
     }
     const size_t dn[6] = {nx + 4, nx + 3, ny + 4, ny + 3, nz + 4, nz + 3};
     for (int q = 0; q < 6; ++q) rc |= ealloc(e, &k.dx[q], dn[q]);
@@ -420,6 +438,7 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
     const size_t fu = (nx + 1) * ny * nz, fv = (ny + 1) * nx * nz, fw = (nz + 1) * nx * ny;
     if (f32) rc |= ealloc(e, &d.c32, ncell * nb);
     else rc |= ealloc(e, &d.c64, ncell * nb);
+    if (cmp) rc |= ealloc(e, &d.c32lo, ncell * nb);
     rc |= ealloc(e, &d.acum, nx * ny * nb);
     d.ux[0] = k.ux; d.ux[1] = k.ux + fu;
     d.vy[0] = k.vy; d.vy[1] = k.vy + fv;
@@ -434,6 +453,10 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
       for (int q = 0; q < 3; ++q) d.f4[q] = k.f4[q];
       d.vs32 = k.vs32;
       d.rdx1b32 = k.rdx[0]; d.rdx2b32 = k.rdx[1]; d.rdx3b32 = k.rdx[2];
+      for (int q = 0; q < 3; ++q) {
+        d.rdxb64[q] = k.rdx64[q];
+        d.rdxb2[q] = k.rdx2[q];
+      }
     }
     d.dx1p = k.dx[0]; d.dx1b = k.dx[1]; d.dx2p = k.dx[2];
     d.dx2b = k.dx[3]; d.dx3p = k.dx[4]; d.dx3b = k.dx[5];
@@ -444,6 +467,7 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
     if (!rc) {
       if (f32) rc |= cudaMemsetAsync(d.c32, 0, ncell * nb * 4, e->st) != cudaSuccess;
       else rc |= cudaMemsetAsync(d.c64, 0, ncell * nb * 8, e->st) != cudaSuccess;
+      if (cmp) rc |= cudaMemsetAsync(d.c32lo, 0, ncell * nb * 4, e->st) != cudaSuccess;
       rc |= cudaMemsetAsync(d.acum, 0, nx * ny * nb * 8, e->st) != cudaSuccess;
     }
   }
@@ -505,6 +529,17 @@ extern "C" int f3d_ens_set_class_grid(f3d_ens* e, int ci, const double* dX1_p, c
       std::vector<float> r(nn[d]);
       for (size_t q = 0; q < nn[d]; ++q) r[q] = (float)(1.0 / db[d][q + 1]);
       ECK(cudaMemcpy(k.rdx[d], r.data(), nn[d] * 4, cudaMemcpyHostToDevice));
+      if (k.rdx64[d]) {
+        std::vector<double> r64(nn[d]);
+        for (size_t q = 0; q < nn[d]; ++q) r64[q] = 1.0 / db[d][q + 1];
+        ECK(cudaMemcpy(k.rdx64[d], r64.data(), nn[d] * 8, cudaMemcpyHostToDevice));
+        std::vector<float2> r2(nn[d]);
+        for (size_t q = 0; q < nn[d]; ++q) {
+          const float h = (float)r64[q];
+          r2[q] = make_float2(h, (float)(r64[q] - (double)h));
+        }
+        ECK(cudaMemcpy(k.rdx2[d], r2.data(), nn[d] * sizeof(float2), cudaMemcpyHostToDevice));
+      }
     }
   }
   k.grid_set = true;
@@ -813,14 +848,18 @@ extern "C" int f3d_ens_upload_member_state(f3d_ens* e, int mi, const double* my_
     if (e->prec == F3D_PREC_FP64) {
       if (ens_upload_conv(e, k, 7, my_c, (nx + 4) * (ny + 4) * (nz + 4) * nb, m.c64)) return 1;
     } else {
-      std::vector<float> tmp(nx * ny * nz * nb);
+      std::vector<float> tmp(nx * ny * nz * nb), tlo(m.c32lo ? tmp.size() : 0);
       for (size_t b = 0; b < nb; ++b)
         for (size_t kk = 0; kk < nz; ++kk)
           for (size_t j = 0; j < ny; ++j)
-            for (size_t i = 0; i < nx; ++i)
-              tmp[((b * nz + kk) * ny + j) * nx + i] = (float)my_c[(i + 2) + (nx + 4) *
-                  ((j + 2) + (ny + 4) * ((kk + 2) + (nz + 4) * b))];
+            for (size_t i = 0; i < nx; ++i) {
+              const size_t q = ((b * nz + kk) * ny + j) * nx + i;
+              const double v = my_c[(i + 2) + (nx + 4) * ((j + 2) + (ny + 4) * ((kk + 2) + (nz + 4) * b))];
+              tmp[q] = (float)v;
+              if (m.c32lo) tlo[q] = (float)(v - (double)tmp[q]);
+            }
       ECK(cudaMemcpy(m.c32, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice));
+      if (m.c32lo) ECK(cudaMemcpy(m.c32lo, tlo.data(), tlo.size() * 4, cudaMemcpyHostToDevice));
     }
   }
   if (my_acum && ens_upload_conv(e, k, 8, my_acum, (nx + 4) * (ny + 4) * nb, m.acum)) return 1;
@@ -842,6 +881,10 @@ extern "C" int f3d_ens_download_member_state(f3d_ens* e, int mi, double* my_c, d
       std::vector<float> t32(tmp.size());
       ECK(cudaMemcpy(t32.data(), m.c32, t32.size() * 4, cudaMemcpyDeviceToHost));
       for (size_t q = 0; q < t32.size(); ++q) tmp[q] = t32[q];
+      if (m.c32lo) {
+        ECK(cudaMemcpy(t32.data(), m.c32lo, t32.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < t32.size(); ++q) tmp[q] = tmp[q] + (double)t32[q];
+      }
     }
     for (size_t b = 0; b < nb; ++b)
       for (size_t kk = 0; kk < nz; ++kk)
@@ -936,7 +979,7 @@ namespace {
 
 int fused_setup(f3d_ens* e, const void** func, int* smem) {
   const bool f32 = e->prec == F3D_PREC_FP32;
-  *func = f32 ? fused32_func(e->lim, e->tm) : fused64_func(e->lim, e->tm);
+  *func = f32 ? fused32_func(e->lim, e->tm, e->cmp) : fused64_func(e->lim, e->tm);
   *smem = f32 ? fused32_smem() : fused64_smem();
   ECK(cudaFuncSetAttribute(*func, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
   int per_sm = 0;
@@ -1000,6 +1043,7 @@ int enqueue_wet_radio(f3d_ens* e) {
       a.awet = e->awet[m];
       a.c64 = d.c64;
       a.c32 = d.c32;
+      a.c32lo = d.c32lo;
       a.mask = e->wet_mask;
       launch_wet(a, e->st);
       e->launches += 1;
@@ -1018,6 +1062,7 @@ int enqueue_wet_radio(f3d_ens* e) {
       r.fdev = e->d_radfact + 2 * (size_t)r.nr * m;
       r.c64 = d.c64;
       r.c32 = d.c32;
+      r.c32lo = d.c32lo;
       r.acum = d.acum;
       r.awet = e->awet.empty() ? nullptr : e->awet[m];
       launch_radio(r, e->st);
@@ -1055,6 +1100,7 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullpt
     a.counters = e->counters;
     a.err = e->d_err;
     a.bpb = e->bpb;
+    a.wait_limit = wait_limit();
     void* args[] = {&a};
     ECK(cudaLaunchCooperativeKernel(func, dim3(e->fused_grid), dim3(128), args, (size_t)smem, e->st));
     e->launches += 1;
@@ -1076,7 +1122,7 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullpt
     if (e->prec == F3D_PREC_FP64)
       launch_sweep64(d, e->lim, e->tm, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
     else
-      launch_sweep32(d, e->lim, e->tm, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
+      launch_sweep32(d, e->lim, e->tm, e->cmp, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
     e->launches += 1;
     if (ev) ECK(cudaEventRecord(ev[2 + q], e->st));
   }
@@ -1169,6 +1215,109 @@ extern "C" int f3d_ens_run(f3d_ens* e, int nsteps) {
   return 0;
 }
 
+// ---- autotuner --------------------------------------------------------------
+namespace {
+// The candidates: per-phase kernels replayed from CUDA graphs with 4, 2 or 1
+// bins per block, and the persistent step kernel with 4 or 2.
+const int kTuneCand[F3D_ENS_TUNE_CANDIDATES][3] = {
+    {F3D_ENS_MODE_KERNELS, 4, 0},    {F3D_ENS_MODE_KERNELS, 2, 0},
+    {F3D_ENS_MODE_KERNELS, 1, 0},    {F3D_ENS_MODE_PERSISTENT, 4, 0},
+    {F3D_ENS_MODE_PERSISTENT, 2, 0}};
+
+// Cache file: one line per key, "key mode bpb ctas ms c0 c1 c2 c3 c4"
+// (keys are single tokens; later lines of a key win).
+bool tune_cache_read(const char* path, const char* key, int tuning[3], double* ms, double* cand) {
+  FILE* f = fopen(path, "r");
+  if (!f) return false;
+  char line[1024];
+  bool found = false;
+  while (fgets(line, sizeof line, f)) {
+    char k[512];
+    int t0, t1, t2;
+    double m, c[F3D_ENS_TUNE_CANDIDATES];
+    if (sscanf(line, "%511s %d %d %d %lf %lf %lf %lf %lf %lf", k, &t0, &t1, &t2, &m, &c[0], &c[1],
+               &c[2], &c[3], &c[4]) == 10 &&
+        strcmp(k, key) == 0) {
+      tuning[0] = t0;
+      tuning[1] = t1;
+      tuning[2] = t2;
+      *ms = m;
+      if (cand) memcpy(cand, c, sizeof c);
+      found = true;
+    }
+  }
+  fclose(f);
+  return found;
+}
+
+void tune_cache_write(const char* path, const char* key, const int tuning[3], double ms,
+                      const double* cand) {
+  std::vector<std::string> keep;
+  if (FILE* f = fopen(path, "r")) {
+    char line[1024], k[512];
+    while (fgets(line, sizeof line, f))
+      if (sscanf(line, "%511s", k) == 1 && strcmp(k, key) != 0) keep.push_back(line);
+    fclose(f);
+  }
+  const std::string tmp = std::string(path) + ".tmp";
+  FILE* f = fopen(tmp.c_str(), "w");
+  if (!f) return;  // an unwritable cache only costs a re-tune
+  for (const std::string& l : keep) fputs(l.c_str(), f);
+  fprintf(f, "%s %d %d %d %.6f", key, tuning[0], tuning[1], tuning[2], ms);
+  for (int q = 0; q < F3D_ENS_TUNE_CANDIDATES; ++q) fprintf(f, " %.6f", cand[q]);
+  fputc('\n', f);
+  fclose(f);
+  rename(tmp.c_str(), path);
+}
+}  // namespace
+
+extern "C" int f3d_ens_autotune(f3d_ens* e, int steps, const char* cache_file, const char* key,
+                                int tuning[3], double* ms_per_step, double* cand_ms) {
+  if (!e || !tuning || !ms_per_step || steps < 1)
+    return set_error_msg("f3d_ens_autotune: bad arguments");
+  if (key && strpbrk(key, " \t\n"))
+    return set_error_msg("f3d_ens_autotune: the cache key must be a single token");
+  const bool cached = cache_file && key;
+  if (cached && tune_cache_read(cache_file, key, tuning, ms_per_step, cand_ms))
+    return f3d_ens_set_tuning(e, tuning[0], tuning[1], tuning[2]);
+  ECK(cudaSetDevice(e->device));
+  cudaEvent_t ev[2];
+  ECK(cudaEventCreate(&ev[0]));
+  ECK(cudaEventCreate(&ev[1]));
+  double ms[F3D_ENS_TUNE_CANDIDATES];
+  int best = -1;
+  for (int q = 0; q < F3D_ENS_TUNE_CANDIDATES; ++q) {
+    ms[q] = -1.0;
+    const int* c = kTuneCand[q];
+    int derr = 0;
+    float el = 0.f;
+    // warm-up step (builds the graphs), then `steps` timed steps on the
+    // ensemble's stream; a candidate that fails or whose barriers gave up
+    // is skipped
+    if (f3d_ens_set_tuning(e, c[0], c[1], c[2]) || f3d_ens_run(e, 1) ||
+        cudaEventRecord(ev[0], e->st) != cudaSuccess || f3d_ens_run(e, steps) ||
+        cudaEventRecord(ev[1], e->st) != cudaSuccess || f3d_ens_status(e, &derr) ||
+        cudaEventElapsedTime(&el, ev[0], ev[1]) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (derr) {
+      f3d_ens_clear_status(e);
+      continue;
+    }
+    ms[q] = el / steps;
+    if (best < 0 || ms[q] < ms[best]) best = q;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (cand_ms) memcpy(cand_ms, ms, sizeof ms);
+  if (best < 0) return set_error_msg("f3d_ens_autotune: no configuration ran");
+  for (int k = 0; k < 3; ++k) tuning[k] = kTuneCand[best][k];
+  *ms_per_step = ms[best];
+  if (cached) tune_cache_write(cache_file, key, tuning, ms[best], ms);
+  return f3d_ens_set_tuning(e, tuning[0], tuning[1], tuning[2]);
+}
+
 extern "C" int f3d_ens_step(f3d_ens* e, const double* dt, const double* time, int iiter,
                             double* fluxes) {
   if (!e || !dt || !time) return set_error_msg("f3d_ens_step: null argument");
@@ -1228,6 +1377,7 @@ extern "C" int f3d_ens_reset_state(f3d_ens* e) {
     const MemberDev& d = e->hm[m];
     const size_t ncell = (size_t)d.nx * d.ny * d.nz, nb = (size_t)e->nb;
     if (d.c32) ECK(cudaMemsetAsync(d.c32, 0, ncell * nb * 4, e->st));
+    if (d.c32lo) ECK(cudaMemsetAsync(d.c32lo, 0, ncell * nb * 4, e->st));
     if (d.c64) ECK(cudaMemsetAsync(d.c64, 0, ncell * nb * 8, e->st));
     ECK(cudaMemsetAsync(d.acum, 0, (size_t)d.nx * d.ny * nb * 8, e->st));
   }
@@ -1380,6 +1530,7 @@ extern "C" int f3d_ens_output_member_species(f3d_ens* e, int mi, const int* bin_
   a.col_du = col_du;
   a.c64 = d.c64;
   a.c32 = d.c32;
+  a.c32lo = d.c32lo;
   a.acum = d.acum;
   a.awet = e->awet.empty() ? nullptr : e->awet[mi];
   a.hm1 = d.hm1;
@@ -1452,6 +1603,43 @@ extern "C" int f3d_ens_launch_count(f3d_ens* e, long long* count) {
 extern "C" int f3d_ens_status(f3d_ens* e, int* device_error) {
   if (!e || !device_error) return set_error_msg("f3d_ens_status: null argument");
   ECK(cudaSetDevice(e->device));
+  ECK(cudaStreamSynchronize(e->st));
   ECK(cudaMemcpy(device_error, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+extern "C" int f3d_ens_clear_status(f3d_ens* e) {
+  if (!e) return set_error_msg("f3d_ens_clear_status: null ensemble");
+  ECK(cudaSetDevice(e->device));
+  ECK(cudaMemsetAsync(e->d_err, 0, sizeof(int), e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  return 0;
+}
+
+// Finite scan of one member's state and its class's device inputs (bits as
+// in f3d_ads_check_finite).
+extern "C" int f3d_ens_check_finite(f3d_ens* e, int mi, int* mask) {
+  if (!e || !mask || mi < 0 || mi >= e->nm) return set_error_msg("f3d_ens_check_finite: bad arguments");
+  ECK(cudaSetDevice(e->device));
+  const MemberDev& m = e->hm[mi];
+  const long long nx = m.nx, ny = m.ny, nz = m.nz, nb = e->nb, ncell = nx * ny * nz;
+  unsigned int* dmask = reinterpret_cast<unsigned int*>(e->d_nfail) + 2;
+  ECK(cudaMemsetAsync(dmask, 0, sizeof(unsigned int), e->st));
+  launch_nonfinite(m.c64, ncell * nb, 0, dmask, e->st);
+  launch_nonfinite(m.c32, ncell * nb, 0, dmask, e->st);
+  launch_nonfinite(m.c32lo, ncell * nb, 0, dmask, e->st);
+  launch_nonfinite(m.acum, nx * ny * nb, 1, dmask, e->st);
+  launch_nonfinite(m.ux[0], 2 * (nx + 1) * ny * nz, 2, dmask, e->st);
+  launch_nonfinite(m.vy[0], 2 * (ny + 1) * nx * nz, 3, dmask, e->st);
+  launch_nonfinite(m.wz[0], 2 * (nz + 1) * nx * ny, 4, dmask, e->st);
+  launch_nonfinite(m.k1x, (nx + 2) * ny * nz, 5, dmask, e->st);
+  launch_nonfinite(m.k2y, (ny + 2) * nx * nz, 6, dmask, e->st);
+  launch_nonfinite(m.k3z, (nz + 2) * nx * ny, 7, dmask, e->st);
+  launch_nonfinite(m.vs, nb * (nz + 1) * nx * ny, 8, dmask, e->st);
+  ECKL();
+  unsigned int h = 0;
+  ECK(cudaMemcpyAsync(&h, dmask, sizeof(h), cudaMemcpyDeviceToHost, e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  *mask = (int)h;
   return 0;
 }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -65,9 +66,14 @@ void launch_vset_field(MemberDev* members, int mi, int model, const double* rhoc
                        const double* tc, const double* bin_par, const int* bin_flags,
                        double vset_fac, int* nfail, cudaStream_t st);
 void launch_face_kk(MemberDev* members, int mi, cudaStream_t st);
+void launch_nonfinite(const double* p, long long n, int bit, unsigned int* mask, cudaStream_t st);
+void launch_nonfinite(const float* p, long long n, int bit, unsigned int* mask, cudaStream_t st);
+void launch_ads_solve_1d(int n, int lim, double* c, const double* dxp, const double* dxb,
+                         const double* u, const double* k, double dt, const double bvalue[2],
+                         const int bcode[2], double* flux, double* work, cudaStream_t st);
 // ads_fp32.cu
-void launch_sweep32(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
-                    int nblocks, int bpb, cudaStream_t st);
+void launch_sweep32(int dir, int lim, int tm, int cmp, const MemberDev* members,
+                    const WorkItem* work, int nblocks, int bpb, cudaStream_t st);
 void launch_prep32(const MemberDev* members, const int* blk_member, const int* blk_first,
                    int nblocks, int mask, cudaStream_t st);
 void launch_source32(const MemberDev* members, int nmembers, cudaStream_t st);
@@ -123,6 +129,7 @@ static const int kPrepBlock = 256;
 
 struct f3d_ctx {
   int nx = 0, ny = 0, nz = 0, nb = 0, lim = 2, tm = 2, prec = 0, device = 0;
+  int cmp = 0;  // precision form with the compensated (hi + lo) state
   cudaStream_t st = nullptr;
   MemberDev hm;            // host mirror of the member descriptor
   MemberDev* dm = nullptr; // device copy
@@ -232,6 +239,26 @@ static int build_work(f3d_ctx* c) {
   return 0;
 }
 
+// ---- bounded waits and the settling-velocity iteration limit -----------------
+namespace f3d {
+constexpr long long kDefaultWaitLimit = 1LL << 25;  // = kSpinLimit (step_dev.cuh)
+static std::atomic<long long> g_wait_limit{kDefaultWaitLimit};
+static std::atomic<int> g_vset_maxit{1000};
+long long wait_limit() { return g_wait_limit.load(); }
+int vset_maxit() { return g_vset_maxit.load(); }
+}  // namespace f3d
+
+extern "C" int f3d_set_wait_limit(long long polls) {
+  g_wait_limit.store(polls < 0 ? kDefaultWaitLimit : polls);
+  return 0;
+}
+
+extern "C" int f3d_set_vset_maxit(int maxit) {
+  if (maxit == 0 || maxit < -1) return set_err("f3d_set_vset_maxit: maxit %d (use >= 1, or -1 for 1000)", maxit);
+  g_vset_maxit.store(maxit < 0 ? 1000 : maxit);
+  return 0;
+}
+
 extern "C" int f3d_last_error(char* buf, int len) {
   if (!buf || len <= 0) return 1;
   snprintf(buf, (size_t)len, "%s", g_err.c_str());
@@ -247,13 +274,16 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
   if (limiter < 1 || limiter > 3) return set_err("f3d_ads_create: limiter %d not in 1..3", limiter);
   if (time_marching < 1 || time_marching > 2)
     return set_err("f3d_ads_create: time_marching %d not in 1..2", time_marching);
-  if (precision != F3D_PREC_FP64 && precision != F3D_PREC_FP32)
+  if (precision != F3D_PREC_FP64 && precision != F3D_PREC_FP32 && precision != F3D_PREC_FP32C)
     return set_err("f3d_ads_create: precision %d unknown", precision);
+  const int cmp = precision == F3D_PREC_FP32C;
+  if (cmp) precision = F3D_PREC_FP32;
   *out = nullptr;
   CK(cudaSetDevice(device));
   f3d_ctx* c = new f3d_ctx();
   c->nx = dims->nx; c->ny = dims->ny; c->nz = dims->nz; c->nb = dims->nbins;
   c->lim = limiter; c->tm = time_marching; c->prec = precision; c->device = device;
+  c->cmp = cmp;
   if (const char* e = getenv("F3D_BINS_PER_BLOCK")) {
     int v = atoi(e);
     if (v == 1 || v == 2 || v == 4) c->bpb = v;
@@ -302,6 +332,16 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
     rc |= dalloc(c, &f, nx); m.rdx1b32 = f;
     rc |= dalloc(c, &f, ny); m.rdx2b32 = f;
     rc |= dalloc(c, &f, nz); m.rdx3b32 = f;
+    if (cmp) {
+      rc |= dalloc(c, &m.c32lo, ncell * nb);
+      rc |= dalloc(c, &tmp, nx); m.rdxb64[0] = tmp;
+      rc |= dalloc(c, &tmp, ny); m.rdxb64[1] = tmp;
+      rc |= dalloc(c, &tmp, nz); m.rdxb64[2] = tmp;
+      float2* f2;
+      rc |= dalloc(c, &f2, nx); m.rdxb2[0] = f2;
+      rc |= dalloc(c, &f2, ny); m.rdxb2[1] = f2;
+      rc |= dalloc(c, &f2, nz); m.rdxb2[2] = f2;
+    }
   }
   rc |= dalloc(c, &tmp, nx + 4); m.dx1p = tmp;
   rc |= dalloc(c, &tmp, nx + 3); m.dx1b = tmp;
@@ -332,6 +372,7 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
   }
   CK(cudaMemsetAsync(m.c64 ? (void*)m.c64 : (void*)m.c32, 0,
                      ncell * nb * (m.c64 ? sizeof(double) : sizeof(float)), c->st));
+  if (m.c32lo) CK(cudaMemsetAsync(m.c32lo, 0, ncell * nb * sizeof(float), c->st));
   CK(cudaMemsetAsync(m.acum, 0, nx * ny * nb * sizeof(double), c->st));
   CK(cudaMemsetAsync(m.flux_tot, 0, 12 * sizeof(double), c->st));
   CK(cudaMemsetAsync(m.flux_step, 0, 6 * sizeof(double), c->st));
@@ -407,6 +448,24 @@ extern "C" int f3d_ads_set_grid(f3d_ctx* c, const double* dX1_p, const double* d
     CK(cudaMemcpy((void*)m.rdx1b32, r1.data(), nx * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy((void*)m.rdx2b32, r2.data(), ny * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy((void*)m.rdx3b32, r3.data(), nz * 4, cudaMemcpyHostToDevice));
+    if (m.c32lo) {
+      std::vector<double> q1(nx), q2(ny), q3(nz);
+      for (size_t i = 0; i < nx; ++i) q1[i] = 1.0 / dX1_b[i + 1];
+      for (size_t j = 0; j < ny; ++j) q2[j] = 1.0 / dX2_b[j + 1];
+      for (size_t k = 0; k < nz; ++k) q3[k] = 1.0 / dX3_b[k + 1];
+      CK(cudaMemcpy((void*)m.rdxb64[0], q1.data(), nx * 8, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy((void*)m.rdxb64[1], q2.data(), ny * 8, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy((void*)m.rdxb64[2], q3.data(), nz * 8, cudaMemcpyHostToDevice));
+      const std::vector<double>* qs[3] = {&q1, &q2, &q3};
+      for (int d = 0; d < 3; ++d) {
+        std::vector<float2> p2(qs[d]->size());
+        for (size_t q = 0; q < p2.size(); ++q) {
+          const float h = (float)(*qs[d])[q];
+          p2[q] = make_float2(h, (float)((*qs[d])[q] - (double)h));
+        }
+        CK(cudaMemcpy((void*)m.rdxb2[d], p2.data(), p2.size() * sizeof(float2), cudaMemcpyHostToDevice));
+      }
+    }
   }
   CK(cudaStreamSynchronize(c->st));
   c->grid_set = true;
@@ -980,6 +1039,7 @@ extern "C" int f3d_ads_output_species(f3d_ctx* c, const int* bin_in, int col_du,
   a.col_du = col_du;
   a.c64 = m.c64;
   a.c32 = m.c32;
+  a.c32lo = m.c32lo;
   a.acum = m.acum;
   a.awet = c->d_awet;
   a.hm1 = m.hm1;
@@ -1084,15 +1144,21 @@ extern "C" int f3d_ads_upload_state(f3d_ctx* c, const double* my_c, const double
     if (c->prec == F3D_PREC_FP64) {
       if (upload_conv(c, 7, my_c, (nx + 4) * (ny + 4) * (nz + 4) * nb, m.c64)) return 1;
     } else {
-      // convert on the host, rounding to nearest FP32
-      std::vector<float> tmp(nx * ny * nz * nb);
+      // convert on the host, rounding to nearest FP32 (compensated form: the
+      // pair hi = RN(c), lo = RN(c - hi))
+      std::vector<float> tmp(nx * ny * nz * nb), tlo(m.c32lo ? tmp.size() : 0);
       for (size_t b = 0; b < nb; ++b)
         for (size_t k = 0; k < nz; ++k)
           for (size_t j = 0; j < ny; ++j)
-            for (size_t i = 0; i < nx; ++i)
-              tmp[((b * nz + k) * ny + j) * nx + i] =
-                  (float)my_c[(i + 2) + (nx + 4) * ((j + 2) + (ny + 4) * ((k + 2) + (nz + 4) * b))];
+            for (size_t i = 0; i < nx; ++i) {
+              const size_t q = ((b * nz + k) * ny + j) * nx + i;
+              const double v =
+                  my_c[(i + 2) + (nx + 4) * ((j + 2) + (ny + 4) * ((k + 2) + (nz + 4) * b))];
+              tmp[q] = (float)v;
+              if (m.c32lo) tlo[q] = (float)(v - (double)tmp[q]);
+            }
       CK(cudaMemcpy(m.c32, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice));
+      if (m.c32lo) CK(cudaMemcpy(m.c32lo, tlo.data(), tlo.size() * 4, cudaMemcpyHostToDevice));
     }
   }
   if (my_acum && upload_conv(c, 8, my_acum, (nx + 4) * (ny + 4) * nb, m.acum)) return 1;
@@ -1118,6 +1184,10 @@ extern "C" int f3d_ads_download_state(f3d_ctx* c, double* my_c, double* my_acum)
       std::vector<float> t32(tmp.size());
       CK(cudaMemcpy(t32.data(), m.c32, t32.size() * 4, cudaMemcpyDeviceToHost));
       for (size_t q = 0; q < t32.size(); ++q) tmp[q] = t32[q];
+      if (m.c32lo) {
+        CK(cudaMemcpy(t32.data(), m.c32lo, t32.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < t32.size(); ++q) tmp[q] = tmp[q] + (double)t32[q];
+      }
     }
     const size_t X = nx + 4, Y = ny + 4, Z = nz + 4;
     for (size_t b = 0; b < nb; ++b)
@@ -1178,7 +1248,7 @@ static int enqueue_sweep(f3d_ctx* c, int dir) {
   if (c->prec == F3D_PREC_FP64)
     launch_sweep64(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
   else
-    launch_sweep32(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
+    launch_sweep32(dir, c->lim, c->tm, c->cmp, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
   CKL();
   return 0;
 }
@@ -1226,6 +1296,7 @@ static int enqueue_wet_radio(f3d_ctx* c, double dt) {
     a.awet = c->d_awet;
     a.c64 = m.c64;
     a.c32 = m.c32;
+    a.c32lo = m.c32lo;
     a.mask = c->wet_mask;
     launch_wet(a, c->st);
     c->launches += 1;
@@ -1246,6 +1317,7 @@ static int enqueue_wet_radio(f3d_ctx* c, double dt) {
     }
     r.c64 = m.c64;
     r.c32 = m.c32;
+    r.c32lo = m.c32lo;
     r.acum = m.acum;
     r.awet = c->wet_on ? c->d_awet : nullptr;
     r.gh64 = m.gh64;
@@ -1453,6 +1525,71 @@ extern "C" int f3d_ads_get_time_step(f3d_ctx* c, double stime, int criterion, do
   m = cfl * m;
   *my_dt = std::min(m, run_end);
   *gl_dt = std::min(m, run_end);
+  return 0;
+}
+
+// ADS_solve_1D (mod_ADS.F90:820-1053) of one pencil on the device; host
+// arrays in the reference layouts (see include/fall3d_ads.h).
+extern "C" int f3d_ads_solve_1d(int n, int limiter, double* c, const double* dxp,
+                                const double* dxb, const double* u, const double* k, double dt,
+                                const double bvalue[2], double flux[2], const int bcode[2],
+                                int device) {
+  if (n < 2 || !c || !dxp || !dxb || !u || !k || !bvalue || !flux || !bcode)
+    return set_err("f3d_ads_solve_1d: bad arguments (n >= 2, no null arrays)");
+  if (limiter < 1 || limiter > 3) return set_err("f3d_ads_solve_1d: limiter %d not in 1..3", limiter);
+  for (int s = 0; s < 2; ++s)
+    if (bcode[s] < -1 || bcode[s] > 2) return set_err("f3d_ads_solve_1d: bcode %d not in -1..2", bcode[s]);
+  CK(cudaSetDevice(device));
+  const size_t N = (size_t)n;
+  const size_t tot = (N + 4) * 3 + (N + 3) * 2 + 2 + (6 * N + 14);
+  double* d = nullptr;
+  CK(cudaMalloc(&d, tot * sizeof(double)));
+  double *dc = d, *dp = dc + N + 4, *dk = dp + N + 4, *db = dk + N + 4, *du = db + N + 3,
+         *df = du + N + 3, *dw = df + 2;
+  int rc = 0;
+  const struct { double* dst; const double* src; size_t n; } up[6] = {
+      {dc, c, N + 4}, {dp, dxp, N + 4}, {dk, k, N + 4}, {db, dxb, N + 3}, {du, u, N + 3}, {df, flux, 2}};
+  for (int q = 0; q < 6 && !rc; ++q)
+    if (cudaMemcpy(up[q].dst, up[q].src, up[q].n * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = set_err("f3d_ads_solve_1d: upload failed");
+  if (!rc) {
+    launch_ads_solve_1d(n, limiter, dc, dp, db, du, dk, dt, bvalue, bcode, df, dw, 0);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) rc = set_err("f3d_ads_solve_1d: %s", cudaGetErrorString(e));
+  }
+  if (!rc && (cudaMemcpy(c, dc, (N + 4) * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+              cudaMemcpy(flux, df, 2 * 8, cudaMemcpyDeviceToHost) != cudaSuccess))
+    rc = set_err("f3d_ads_solve_1d: download failed");
+  cudaFree(d);
+  return rc;
+}
+
+// Finite scan of the device-resident inputs and state.  Bits of *mask:
+// 1 state, 2 ground deposit, 4 u, 8 v, 16 w (both meteo snapshots),
+// 32 k1, 64 k2, 128 k3, 256 settling velocity.
+extern "C" int f3d_ads_check_finite(f3d_ctx* c, int* mask) {
+  if (!c || !mask) return set_err("f3d_ads_check_finite: null argument");
+  CK(cudaSetDevice(c->device));
+  const MemberDev& m = c->hm;
+  const long long nx = c->nx, ny = c->ny, nz = c->nz, nb = c->nb, ncell = nx * ny * nz;
+  unsigned int* dmask = reinterpret_cast<unsigned int*>(c->d_nfail) + 2;
+  CK(cudaMemsetAsync(dmask, 0, sizeof(unsigned int), c->st));
+  launch_nonfinite(m.c64, ncell * nb, 0, dmask, c->st);
+  launch_nonfinite(m.c32, ncell * nb, 0, dmask, c->st);
+  launch_nonfinite(m.c32lo, ncell * nb, 0, dmask, c->st);
+  launch_nonfinite(m.acum, nx * ny * nb, 1, dmask, c->st);
+  launch_nonfinite(m.ux[0], 2 * (nx + 1) * ny * nz, 2, dmask, c->st);
+  launch_nonfinite(m.vy[0], 2 * (ny + 1) * nx * nz, 3, dmask, c->st);
+  launch_nonfinite(m.wz[0], 2 * (nz + 1) * nx * ny, 4, dmask, c->st);
+  launch_nonfinite(m.k1x, (nx + 2) * ny * nz, 5, dmask, c->st);
+  launch_nonfinite(m.k2y, (ny + 2) * nx * nz, 6, dmask, c->st);
+  launch_nonfinite(m.k3z, (nz + 2) * nx * ny, 7, dmask, c->st);
+  launch_nonfinite(m.vs, nb * (nz + 1) * nx * ny, 8, dmask, c->st);
+  CKL();
+  unsigned int h = 0;
+  CK(cudaMemcpyAsync(&h, dmask, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *mask = (int)h;
   return 0;
 }
 

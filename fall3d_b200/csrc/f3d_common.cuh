@@ -100,7 +100,30 @@ struct MemberDev {
   // per bin as gh_offset() gives (exact form gh64, precision form gh32)
   double* gh64;
   float* gh32;
+  // compensated precision form (null otherwise): the low part of the state,
+  // laid out like c32, so that the concentration is c32 + c32lo (about 48
+  // bits), and 1/dxb per axis in FP64 ([cell], n entries) for the
+  // conservative final update of the sweeps
+  float* c32lo;
+  const double* rdxb64[3];
+  const float2* rdxb2[3];  // the same 1/dxb as an FP32 pair {hi, lo} (~48 bits)
 };
+
+// Precision-form state value of element at (c32, plus c32lo when kept).
+__host__ __device__ __forceinline__ double state32(const MemberDev& m, long long at) {
+  return m.c32lo ? (double)m.c32[at] + (double)m.c32lo[at] : (double)m.c32[at];
+}
+// Store v into the precision-form state: rounded to FP32, or split into the
+// FP32 pair c32 + c32lo when the compensated state is kept.
+__device__ __forceinline__ void set_state32(const MemberDev& m, long long at, double v) {
+  const float hi = __double2float_rn(v);
+  m.c32[at] = hi;
+  if (m.c32lo) m.c32lo[at] = __double2float_rn(v - (double)hi);
+}
+// Add inc to the precision-form state element at (FP64 add, one rounding).
+__device__ __forceinline__ void add_to_state32(const MemberDev& m, long long at, double inc) {
+  set_state32(m, at, state32(m, at) + inc);
+}
 
 // Boundary halo layers of one bin: x sweep W, E [k][j]; y sweep S, N [k][i];
 // z sweep D, U [j][i].  Element of pencil pen (the sweep's spatial pencil
@@ -131,10 +154,13 @@ struct WorkItem {
 // Correctly rounded a/b for a divisor with precomputed y = RN(1/b)
 // (Markstein's correction, applied twice so that the second correction
 // starts from a faithful quotient; P. Markstein, IBM J. Res. Dev. 34(1),
-// 1990).  Branch-free: numerators below 2^-800 are first scaled by 2^400
-// (exact) so no intermediate is subnormal, and zero numerators return the
-// correctly signed zero a*y.  Exact IEEE round-to-nearest whenever the
-// quotient is a normal number and |b| is in [2^-100, 2^100].
+// 1990).  Numerators below 2^-800 are first scaled by 2^400 (exact) so no
+// intermediate is subnormal, and zero numerators return the correctly
+// signed zero a*y.  For |b| in [2^-100, 2^100] this is IEEE round-to-nearest
+// a/b whenever the quotient is a normal number; a quotient in the subnormal
+// range (|q| < 2^-1022, only from numerators below 2^-900) would be rounded a
+// second time by the scaling back, so there the IEEE division a/b itself is
+// taken (a branch that only the far fringe of a plume ever reaches).
 __device__ __forceinline__ double div_rn_recip(double a, double b, double y) {
   const bool tiny = fabs(a) < 0x1p-800;
   const double sa = tiny ? a * 0x1p400 : a;
@@ -143,7 +169,10 @@ __device__ __forceinline__ double div_rn_recip(double a, double b, double y) {
   q = fma(r, y, q);
   r = fma(-q, b, sa);
   q = fma(r, y, q);
-  q = tiny ? q * 0x1p-400 : q;
+  if (tiny) {
+    if (fabs(q) < 0x1p-622) q = a / b;
+    else q = q * 0x1p-400;
+  }
   return (a == 0.0) ? a * y : q;
 }
 

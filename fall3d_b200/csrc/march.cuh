@@ -181,12 +181,22 @@ struct StageS {
 // by select.  The march starts at t = 0 (see run_v).  This body costs about
 // 1.4 steady steps per step against 2.1 for the guarded one, and the edge
 // blocks are a third to half of the march on short (z) pencils.
-template <class T, class Ops, int TM, bool V = false>
+//
+// CMP (precision form with a compensated state): instead of accumulating
+// new_c per cell, the march accumulates per FACE the RK-weighted sum of the
+// stage fluxes, H(f) = G1 + 2 G2 + 2 G3 + G4 (Euler: G1), in hf[f & 7], and
+// the final update of cell p is Ops::final_cmp(c(p), H(p), H(p+1), p).  A face
+// sum is shared by the two cells it separates, so the mass one cell loses is
+// exactly the mass its neighbour gains.  c(p) for that update is taken from
+// the input ring at the start of step t = p + 8, before stage 1 overwrites
+// its slot; nh is not used.
+template <class T, class Ops, int TM, bool V = false, bool CMP = false>
 struct March {
   Ops& o;
   const int n;
   T ch[8];           // c(p) at ch[p & 7]
-  T nh[8];           // new_c(p) at nh[p & 7]
+  T nh[8];           // new_c(p) at nh[p & 7] (not used by CMP)
+  T hf[8];           // CMP: H(f) at hf[f & 7]
   FaceV<T> fw[8];    // face(f) at fw[f & 7]
   StageS<T> S1, S2, S3, S4;
   T gL, gR, uR, cn1, cn2, cn3, cn4;
@@ -200,6 +210,7 @@ struct March {
     constexpr int m1 = (U + 7) & 7, m2 = (U + 6) & 7, m3 = (U + 5) & 7, m4 = (U + 4) & 7,
                   m5 = (U + 3) & 7, m6 = (U + 2) & 7, m7 = (U + 1) & 7;
     T k1 = T(0), k2 = T(0), k3 = T(0), k4 = T(0), ff = T(0);
+    const T c_fin = ch[U];  // CMP: c(t-8), finalised at the end of this step
     // ---- stage 1: arrival at q = t
     // c(p) is loaded at t = p - 4 and face(f) at t = f - 1 (a four-slot and
     // a one-slot queue in front of the rings), so their latency is hidden
@@ -226,9 +237,13 @@ struct March {
       }
       ch[U] = a;
       o.template arrive<G>(S1, t, a, fw[m1], t - 2, k1, ff);
+      if constexpr (CMP) hf[m1] = S1.F1;
     }
     if constexpr (TM == 1) {
-      if (!G || (t >= 2 && t <= n + 1)) o.store_c(t - 2, o.euler(ch[m2], k1));
+      if (!G || (t >= 2 && t <= n + 1)) {
+        if constexpr (CMP) o.store_c(t - 2, o.final_cmp(ch[m2], hf[m2], hf[m1], t - 2));
+        else o.store_c(t - 2, o.euler(ch[m2], k1));
+      }
       if (G && t == 1) flux_lo = ff;
       if (G && t == n + 1) flux_hi = ff;
       return;
@@ -242,9 +257,10 @@ struct March {
         else if (G && q >= n) a = gR;
         else {
           a = o.rk_half(ch[m2], k1);
-          nh[m2] = o.rk_new1(ch[m2], k1);
+          if constexpr (!CMP) nh[m2] = o.rk_new1(ch[m2], k1);
         }
         o.template arrive<G>(S2, q, a, fw[m3], q - 2, k2, ff);
+        if constexpr (CMP) hf[m3] = fmaf(T(2), S2.F1, hf[m3]);
       }
     }
     // ---- stage 3: q = t-4
@@ -256,9 +272,10 @@ struct March {
         else if (G && q >= n) a = gR;
         else {
           a = o.rk_half(ch[m4], k2);
-          nh[m4] = o.rk_add3(nh[m4], k2);
+          if constexpr (!CMP) nh[m4] = o.rk_add3(nh[m4], k2);
         }
         o.template arrive<G>(S3, q, a, fw[m5], q - 2, k3, ff);
+        if constexpr (CMP) hf[m5] = fmaf(T(2), S3.F1, hf[m5]);
       }
     }
     // ---- stage 4: q = t-6, output at t-8
@@ -270,10 +287,15 @@ struct March {
         else if (G && q >= n) a = gR;
         else {
           a = o.rk_full(ch[m6], k3);
-          nh[m6] = o.rk_add3(nh[m6], k3);
+          if constexpr (!CMP) nh[m6] = o.rk_add3(nh[m6], k3);
         }
         o.template arrive<G>(S4, q, a, fw[m7], q - 2, k4, ff);
-        if (!G || (q >= 2)) o.store_c(q - 2, o.rk_final(nh[U], k4));
+        if constexpr (CMP) {
+          hf[m7] = hf[m7] + S4.F1;
+          if (!G || (q >= 2)) o.store_c(q - 2, o.final_cmp(c_fin, hf[U], hf[m7], q - 2));
+        } else {
+          if (!G || (q >= 2)) o.store_c(q - 2, o.rk_final(nh[U], k4));
+        }
         if (G && q == 1) flux_lo = ff;
         if (G && q == n + 1) flux_hi = ff;
       }
@@ -288,6 +310,7 @@ struct March {
     constexpr int m1 = (U + 7) & 7, m2 = (U + 6) & 7, m3 = (U + 5) & 7, m4 = (U + 4) & 7,
                   m5 = (U + 3) & 7, m6 = (U + 2) & 7, m7 = (U + 1) & 7;
     T k1, k2, k3, k4, ff;
+    const T c_fin = ch[U];  // CMP: c(t-8), finalised at the end of this step
     {  // stage 1: q = t; c(p) enters the queue at t = p - 4 (positions past
        // the end loaded by a steady block hold c(n-1): arrive as gR)
       const T a = (t < n) ? cn1 : gR;
@@ -301,23 +324,31 @@ struct March {
       fq = o.face_v(t + 1);
       ch[U] = a;
       o.template arrive<false>(S1, t, a, fw[m1], t - 2, k1, ff);
+      if constexpr (CMP) hf[m1] = S1.F1;
     }
     {  // stage 2: q = t-2
       const T a = o.rk_half(ch[m2], k1);
-      nh[m2] = o.rk_new1(ch[m2], k1);
+      if constexpr (!CMP) nh[m2] = o.rk_new1(ch[m2], k1);
       o.template arrive<false>(S2, t - 2, a, fw[m3], t - 4, k2, ff);
+      if constexpr (CMP) hf[m3] = fmaf(T(2), S2.F1, hf[m3]);
     }
     {  // stage 3: q = t-4
       const T a = o.rk_half(ch[m4], k2);
-      nh[m4] = o.rk_add3(nh[m4], k2);
+      if constexpr (!CMP) nh[m4] = o.rk_add3(nh[m4], k2);
       o.template arrive<false>(S3, t - 4, a, fw[m5], t - 6, k3, ff);
+      if constexpr (CMP) hf[m5] = fmaf(T(2), S3.F1, hf[m5]);
     }
     {  // stage 4: q = t-6, output at t-8; ff is the flux at face q-1
       const int q = t - 6;
       const T a = o.rk_full(ch[m6], k3);
-      nh[m6] = o.rk_add3(nh[m6], k3);
+      if constexpr (!CMP) nh[m6] = o.rk_add3(nh[m6], k3);
       o.template arrive<false>(S4, q, a, fw[m7], q - 2, k4, ff);
-      if (q - 2 >= 0 && q - 2 < n) o.store_c(q - 2, o.rk_final(nh[U], k4));
+      if constexpr (CMP) {
+        hf[m7] = hf[m7] + S4.F1;
+        if (q - 2 >= 0 && q - 2 < n) o.store_c(q - 2, o.final_cmp(c_fin, hf[U], hf[m7], q - 2));
+      } else {
+        if (q - 2 >= 0 && q - 2 < n) o.store_c(q - 2, o.rk_final(nh[U], k4));
+      }
       flux_lo = (q == 1) ? ff : flux_lo;
       flux_hi = (q == n + 1) ? ff : flux_hi;
     }
@@ -345,21 +376,25 @@ struct March {
       fq = o.face_v(t + 1);
       ch[U] = (t < n) ? a : gR;
       o.template arrive<false>(S1, t, ch[U], fw[m1], t - 2, k1, ff);
+      if constexpr (CMP) hf[m1] = S1.F1;
     }
     if constexpr (t >= 2) {
       const T a = o.rk_half(ch[m2], k1);
-      nh[m2] = o.rk_new1(ch[m2], k1);
+      if constexpr (!CMP) nh[m2] = o.rk_new1(ch[m2], k1);
       o.template arrive<false>(S2, t - 2, a, fw[m3], t - 4, k2, ff);
+      if constexpr (CMP) hf[m3] = fmaf(T(2), S2.F1, hf[m3]);
     }
     if constexpr (t >= 4) {
       const T a = o.rk_half(ch[m4], k2);
-      nh[m4] = o.rk_add3(nh[m4], k2);
+      if constexpr (!CMP) nh[m4] = o.rk_add3(nh[m4], k2);
       o.template arrive<false>(S3, t - 4, a, fw[m5], t - 6, k3, ff);
+      if constexpr (CMP) hf[m5] = fmaf(T(2), S3.F1, hf[m5]);
     }
     if constexpr (t >= 6) {
       const T a = o.rk_full(ch[m6], k3);
-      nh[m6] = o.rk_add3(nh[m6], k3);
+      if constexpr (!CMP) nh[m6] = o.rk_add3(nh[m6], k3);
       o.template arrive<false>(S4, t - 6, a, fw[m7], t - 8, k4, ff);
+      if constexpr (CMP) hf[m7] = hf[m7] + S4.F1;
       if constexpr (t == 7) flux_lo = ff;  // face 0 of the last stage
     }
   }
@@ -391,6 +426,7 @@ struct March {
       ch[u] = gL;
       nh[u] = gL;
       fw[u] = fm;
+      if constexpr (CMP) hf[u] = T(0);
     }
     const int t_last = n + 7;
     o.stage_begin(0);

@@ -491,8 +491,9 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
 }
 // Bounded wait on an mbarrier phase; false after the limit (error recorded by
 // the caller, the kernel then winds down instead of spinning).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long long s = 0; s < kSpinLimit; ++s) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          long long limit = kSpinLimit) {
+  for (long long s = 0; s < limit; ++s) {
     if (mbar_test(bar, parity)) return true;
     if (s > 64) __nanosleep(32);
   }
@@ -583,6 +584,7 @@ struct InferArgs {
   unsigned long long* nfallback;
   int* nfail;
   int* err;
+  long long wait_limit;  // polls before a completion wait gives up (kSpinLimit by default)
 };
 
 // Settling velocity of arbitrary points (arrays of d, rhop, psi, rhoa, mu):
@@ -684,7 +686,7 @@ __global__ void __launch_bounds__(kTile) k_mlp_vset_points(InferArgs a) {
       }
       umma_commit(&S.mbar);
     }
-    const bool landed = mbar_wait(&S.mbar, phase);
+    const bool landed = mbar_wait(&S.mbar, phase, a.wait_limit);
     if (!__syncthreads_and(landed)) {  // block-uniform decision
       if (t == 0) atomicExch(a.err, 1);
       ok = false;
@@ -720,7 +722,9 @@ __global__ void __launch_bounds__(kTile) k_mlp_vset_points(InferArgs a) {
     __syncthreads();
     tc_fence_after();
   }
-  if (!ok) mbar_wait(&S.mbar, phase);  // a bounded chance for an MMA in flight to land
+  // an MMA in flight lands before its tensor memory is freed (the full limit,
+  // whatever the first wait's limit was)
+  if (!ok) mbar_wait(&S.mbar, phase, kSpinLimit);
   if (nfb) atomicAdd(a.nfallback, nfb);
   tc_fence_before();
   __syncthreads();
@@ -860,7 +864,7 @@ __global__ void __launch_bounds__(kTile) k_mlp_vset_field(InferArgs a) {
           }
           umma_commit(&S.mbar);
         }
-        const bool landed = mbar_wait(&S.mbar, phase);
+        const bool landed = mbar_wait(&S.mbar, phase, a.wait_limit);
         if (!__syncthreads_and(landed)) {
           if (t == 0) atomicExch(a.err, 1);
           ok = false;
@@ -902,7 +906,9 @@ __global__ void __launch_bounds__(kTile) k_mlp_vset_field(InferArgs a) {
       }
     }
   }
-  if (!ok) mbar_wait(&S.mbar, phase);  // a bounded chance for an MMA in flight to land
+  // an MMA in flight lands before its tensor memory is freed (the full limit,
+  // whatever the first wait's limit was)
+  if (!ok) mbar_wait(&S.mbar, phase, kSpinLimit);
   if (nfb) atomicAdd(a.nfallback, nfb);
   tc_fence_before();
   __syncthreads();
@@ -1285,6 +1291,7 @@ static int infer_launch(f3d_mlp* h, bool field, InferArgs& a, long long tot, cud
   a.nfallback = h->d_u64;
   a.nfail = h->d_int;
   a.err = h->d_int + 1;
+  a.wait_limit = wait_limit();
   const long long ntiles = (tot + kTile - 1) / kTile;
   long long grid = (long long)h->sms * h->infer_occ;
   if (grid > ntiles) grid = ntiles;

@@ -35,7 +35,8 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 // cs = max(0, 1e3 c / (Hm1 Hm2 Hm3)) at an interior mass point
 __device__ __forceinline__ double cs_interior(const OutArgs& a, int b, int i, int j, int k) {
   const long long q = (((long long)b * a.nz + k) * a.ny + j) * a.nx + i;
-  const double c = a.c64 ? a.c64[q] : (double)a.c32[q];
+  const double c = a.c64 ? a.c64[q]
+                         : (a.c32lo ? (double)a.c32[q] + (double)a.c32lo[q] : (double)a.c32[q]);
   const double v = 1e3 * c / (a.hm1[j] * a.hm2[j + 2] * a.hm3[i + (long long)a.nx * j]);
   return v > 0.0 ? v : 0.0;
 }

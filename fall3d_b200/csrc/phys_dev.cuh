@@ -18,6 +18,7 @@ struct WetArgs {
   double* awet;            // [bin][j][i]
   double* c64;             // exact form state (or null)
   float* c32;              // precision form state (or null)
+  float* c32lo;            // its low part (compensated precision form), or null
   unsigned long long mask; // bins that take wet deposition
   const double* dt_dev;    // ensemble: the member's device time step (dta = dt * a), or null
   double a;
@@ -32,6 +33,7 @@ struct RadioArgs {
   double pfact[64];         // exp(-kn dt) of the parent
   double* c64;
   float* c32;
+  float* c32lo;             // low part of c32 (compensated precision form), or null
   double* acum;             // [bin][j][i]
   double* awet;             // [bin][j][i] or null
   double* gh64;             // boundary halo layers (or null): the reference
@@ -47,6 +49,7 @@ struct OutArgs {
   int col_du;               // column load in Dobson units (SO2)
   const double* c64;        // state [bin][k][j][i] (one of c64, c32)
   const float* c32;
+  const float* c32lo;       // low part of c32 (compensated precision form), or null
   const double* acum;       // [bin][j][i]
   const double* awet;       // [bin][j][i] or null
   const double* hm1;        // ny

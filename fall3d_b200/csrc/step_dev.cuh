@@ -60,12 +60,16 @@ __device__ __forceinline__ void member_advance(MemberDev& m) {
 }
 
 // Grid-wide barrier for a co-resident (cooperative) launch.  bar[0] counts
-// arrivals, bar[1] is the generation.  Every wait is bounded: after
-// kSpinLimit polls the block records an error in *err and continues, so a
-// barrier can never hang the GPU.
+// arrivals, bar[1] is the generation.  Every wait is bounded: after `limit`
+// polls (kSpinLimit unless f3d_set_wait_limit lowered it) the block records
+// an error in *err and continues, so a barrier can never hang the GPU.
 constexpr long long kSpinLimit = 1LL << 25;
 
-__device__ __forceinline__ void grid_barrier(unsigned int* bar, int* err) {
+// Poll limit of the bounded device waits for the next launches (host side;
+// f3d_set_wait_limit, f3d_capi.cu).
+long long wait_limit();
+
+__device__ __forceinline__ void grid_barrier(unsigned int* bar, int* err, long long limit) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned int* gen = bar + 1;
@@ -79,7 +83,7 @@ __device__ __forceinline__ void grid_barrier(unsigned int* bar, int* err) {
     } else {
       long long spins = 0;
       while (*gen == g0) {
-        if (++spins > kSpinLimit) {
+        if (++spins > limit) {
           atomicExch(err, 1);
           break;
         }
@@ -111,6 +115,7 @@ struct FusedArgs {
   unsigned int* counters;  // [0..5] phase work counters, [6..7] barrier
   int* err;
   int bpb;
+  long long wait_limit;    // polls before a grid barrier gives up (kSpinLimit by default)
 };
 
 }  // namespace f3d

@@ -7,6 +7,12 @@
 
 namespace f3d {
 
+// Iteration limit of phys_get_vset_point (mod_Phys.F90:794: maxit = 1000) for
+// the next settling-velocity launches; f3d_set_vset_maxit (f3d_capi.cu)
+// lowers it to force the non-convergence path (flag 2) in tests.
+constexpr int kVsetMaxit = 1000;
+int vset_maxit();
+
 // Bin constants of the drag laws (mod_Phys.F90:817-819, 868-870).
 struct VsetConst {
   double rk1, rk2, a, b;
@@ -61,9 +67,8 @@ __device__ __forceinline__ double vset_cd(int model, double rey, double psi, con
 }
 
 __device__ __forceinline__ int vset_point_dev(double diam, double rhop, double psi, double rhoa, double visc,
-                              int model, double* vset_out, int* iters) {
+                              int model, double* vset_out, int* iters, int maxit = kVsetMaxit) {
   const double GI = 9.81, atol = 1e-12, rtol = 1e-6;
-  const int maxit = 1000;
   double cd = 1.0, vset = 0.0, vold, rey;
   *iters = 0;
   if (model == 4) {  // Dellino: closed form

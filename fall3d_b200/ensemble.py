@@ -15,9 +15,7 @@ member has its own wind factor, source, concentration, time step and clock.
 from __future__ import annotations
 
 import ctypes as C
-import json
 import os
-import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -28,6 +26,10 @@ from .source import (ID_COLUMN_HEIGHT, ID_U_WIND, PERTURBATION_TYPE_ABSOLUTE,
                      PERTURBATION_TYPE_RELATIVE, perturbate, place_source, suzuki)
 
 MODE_KERNELS, MODE_PERSISTENT = 0, 1
+# the autotuner's candidates, in the order f3d_ens_autotune reports them
+TUNE_CANDIDATES = [(MODE_KERNELS, 4, 0), (MODE_KERNELS, 2, 0), (MODE_KERNELS, 1, 0),
+                   (MODE_PERSISTENT, 4, 0), (MODE_PERSISTENT, 2, 0)]
+CANDIDATES = len(TUNE_CANDIDATES)
 _dp = C.POINTER(C.c_double)
 
 
@@ -277,6 +279,16 @@ class Ensemble:
         check(lib().f3d_ens_status(self._h, C.byref(e)), "f3d_ens_status")
         return e.value
 
+    def clear_status(self):
+        check(lib().f3d_ens_clear_status(self._h), "f3d_ens_clear_status")
+
+    def check_finite(self, m) -> int:
+        """Finite scan of member m's state and its class's inputs (bit mask
+        as Domain.check_finite)."""
+        k = C.c_int()
+        check(lib().f3d_ens_check_finite(self._h, int(m), C.byref(k)), "f3d_ens_check_finite")
+        return k.value
+
 
 # ---------------------------------------------------------------------------
 @dataclass
@@ -364,60 +376,27 @@ def build_ensemble(ew: EnsembleWorkload, precision=1, device=0, vset="iterative"
 def _cache_path():
     d = os.environ.get("F3D_AUTOTUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache",
                                                               "fall3d_b200")
-    return os.path.join(d, "autotune.json")
+    return os.path.join(d, "autotune.txt")
 
 
-def autotune(ens: Ensemble, key: str, steps=2, candidates=None, use_cache=True):
-    """Time each (mode, bins per block, blocks per SM) for a few steps on the
-    device clock and keep the fastest; the result is cached under `key`
-    (class shapes, bins, precision).  Member state advances during tuning,
-    so callers reset the clock/state afterwards if they need to."""
+def autotune(ens: Ensemble, key: str, steps=2, use_cache=True):
+    """f3d_ens_autotune: time each execution shape (mode, bins per block,
+    blocks per SM) for a few steps on the device and keep the fastest; the
+    result is cached under `key` (class shapes, bins, precision, GPU) in the
+    autotune cache file.  Member state advances during tuning, so callers
+    reset the clock/state afterwards if they need to."""
     path = _cache_path()
-    cache = {}
-    if use_cache and os.path.exists(path):
-        try:
-            with open(path) as f:
-                cache = json.load(f)
-        except (OSError, ValueError):
-            cache = {}
-    if use_cache and key in cache:
-        best = cache[key]
-        ens.set_tuning(*best["tuning"])
-        return best
-    import torch
-    if candidates is None:
-        candidates = [(MODE_KERNELS, b, 0) for b in (4, 2, 1)] + \
-                     [(MODE_PERSISTENT, b, 0) for b in (4, 2)]
-    s = torch.cuda.ExternalStream(ens.stream_ptr)
-    results = []
-    for cand in candidates:
-        try:
-            ens.set_tuning(*cand)
-            ens.run(1)  # warm-up (graph build)
-            ens.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(s)
-            ens.run(steps)
-            e1.record(s)
-            ens.synchronize()
-            if ens.status() != 0:
-                raise F3DError("device barrier timeout")
-            results.append({"tuning": list(cand), "ms_per_step": e0.elapsed_time(e1) / steps})
-        except F3DError as exc:
-            results.append({"tuning": list(cand), "error": str(exc)[:200]})
-    ok = [r for r in results if "ms_per_step" in r]
-    if not ok:
-        raise F3DError(f"autotune: no configuration ran: {results}")
-    best = min(ok, key=lambda r: r["ms_per_step"])
-    best = {"tuning": best["tuning"], "ms_per_step": best["ms_per_step"], "all": results,
-            "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
-    ens.set_tuning(*best["tuning"])
     if use_cache:
-        try:
-            os.makedirs(os.path.dirname(path), exist_ok=True)
-            cache[key] = best
-            with open(path, "w") as f:
-                json.dump(cache, f, indent=1)
-        except OSError:
-            pass
-    return best
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+    tok = "".join(ch if not ch.isspace() else "_" for ch in key)
+    tun = (C.c_int * 3)()
+    ms = C.c_double()
+    cand = (C.c_double * CANDIDATES)()
+    check(lib().f3d_ens_autotune(ens._h, int(steps), path.encode() if use_cache else None,
+                                 tok.encode() if use_cache else None, tun, C.byref(ms), cand),
+          "f3d_ens_autotune")
+    ens.tuning = tuple(tun)
+    return {"tuning": list(tun), "ms_per_step": ms.value,
+            "all": [{"tuning": list(TUNE_CANDIDATES[q]), "ms_per_step": cand[q]} if cand[q] >= 0 else
+                    {"tuning": list(TUNE_CANDIDATES[q]), "error": "did not run"}
+                    for q in range(CANDIDATES)]}

@@ -35,6 +35,8 @@ typedef struct {
 /* Arithmetic forms. */
 #define F3D_PREC_FP64 0 /* FP64 state and stencil, reference operation order  */
 #define F3D_PREC_FP32 1 /* FP32 state and stencil; FP64 deposit, budget, CFL */
+#define F3D_PREC_FP32C 2 /* FP32 stencil on a compensated state: FP32 pair hi + lo
+                            (~48 bits), conservative FP64 final update per cell */
 
 /* Limiters (mod_Phys.F90:58-61) and time marching (mod_Phys.F90:64-65). */
 #define F3D_LIMITER_MINMOD 1
@@ -292,6 +294,42 @@ int f3d_ads_get_time_step(f3d_ctx *ctx, double stime, int criterion,
  * interior.  per_bin (nbins, may be NULL) receives the per-bin masses. */
 int f3d_ads_mass_volume(f3d_ctx *ctx, double *mass, double *per_bin);
 
+/* ADS_solve_1D (mod_ADS.F90:820-1053): RK4 on one pencil of n >= 2 cells
+ * with boundary codes bcode[2] (-1 periodic when the face velocity enters,
+ * 0 ghosts as given, 1 Dirichlet bvalue, 2 free flow: Dirichlet bvalue on
+ * inflow, zero gradient on outflow).  Host arrays, reference layouts:
+ * c(ips-2:ipe+2) INOUT (n+4), dxp and k (n+4), dxb and u (ibs-1:ibe+1,
+ * n+3); flux[2] receives the 4th-stage boundary fluxes (F + P).  Off the
+ * reference's time loop; it is the 1-D entry of the known-answer tests. */
+int f3d_ads_solve_1d(int n, int limiter, double *c, const double *dxp,
+                     const double *dxb, const double *u, const double *k,
+                     double dt, const double bvalue[2], double flux[2],
+                     const int bcode[2], int device);
+
+/* Failure detection (mod_KindType.F90:85-95, MY_ERR; the reference checks
+ * no values, so these have no direct counterpart).
+ * f3d_ads_check_finite: an on-device scan of the resident inputs and state
+ * for NaN or infinite values; *mask (0 = all finite) has bit 1 state,
+ * 2 ground deposit, 4 u, 8 v, 16 w (both meteo snapshots), 32 k1, 64 k2,
+ * 128 k3, 256 settling velocity. */
+int f3d_ads_check_finite(f3d_ctx *ctx, int *mask);
+/* Process-wide poll limit of every bounded device wait in the kernels
+ * launched from now on (the persistent step kernel's grid barriers and the
+ * surrogate's tensor-core completion waits), for tests of the failure path:
+ * a wait that runs out records an error status (f3d_ens_status, or an
+ * error return) instead of waiting on.  polls < 0 restores the default
+ * (2^25 polls, about a second).  A kernel whose first wait gave up still
+ * waits, with the default limit, for its own tensor-core work in flight
+ * before it frees its tensor memory.  CUDA graphs keep the limit of the
+ * launches they captured. */
+int f3d_set_wait_limit(long long polls);
+/* Process-wide iteration limit of the settling-velocity fixed point
+ * (phys_get_vset_point's maxit = 1000, mod_Phys.F90:794) for the next
+ * f3d_vset_points / f3d_ads_compute_vset / f3d_ens_compute_class_vset
+ * calls; a point that has not converged within it returns flag 2
+ * (mod_Phys.F90:944-948).  maxit = -1 restores 1000. */
+int f3d_set_vset_maxit(int maxit);
+
 /* Mass in the volume for callers that cannot allocate device memory.  No
  * counterpart in the reference: a variant of f3d_ads_mass_volume for code
  * whose device memory is owned by its own runtime (an OpenACC or CUDA
@@ -487,8 +525,33 @@ int f3d_ens_get_profile(f3d_ens *ens, double *ms, int *nsteps);
 int f3d_ens_synchronize(f3d_ens *ens);
 int f3d_ens_get_stream(f3d_ens *ens, void **stream);
 int f3d_ens_launch_count(f3d_ens *ens, long long *count);
-/* Device error status: 1 after a bounded grid-barrier wait gave up. */
+/* Device error status: 1 after a bounded grid-barrier wait gave up (the
+ * persistent step kernel then winds down instead of waiting; the state of
+ * that step is not valid).  Waits for the ensemble's stream first.  No
+ * counterpart in the reference, which has no device waits; it stands for
+ * MY_ERR%flag = 1 (mod_KindType.F90:85-95). */
 int f3d_ens_status(f3d_ens *ens, int *device_error);
+/* Autotuner of the batched step (no counterpart in the reference, whose
+ * members run as separate jobs).  Times each candidate execution shape on
+ * the device -- per-phase kernels replayed from CUDA graphs with 4, 2 or 1
+ * bins per block, the persistent step kernel with 4 or 2 -- for one warm-up
+ * and `steps` timed steps (CUDA events on the ensemble's stream), keeps the
+ * fastest and sets it.  Member state and clocks advance while tuning: reset
+ * them afterwards if needed.  With cache_file and key (a single token, e.g.
+ * class shapes, bins, precision and GPU name) the result is read from and
+ * written to that text file, so a later run with the same key sets the
+ * cached shape without timing.  tuning[3] = {mode, bins per block, blocks
+ * per SM (0 = as many as fit)}; cand_ms (may be NULL) receives the
+ * F3D_ENS_TUNE_CANDIDATES candidates' ms per step (-1 where one failed). */
+#define F3D_ENS_TUNE_CANDIDATES 5
+int f3d_ens_autotune(f3d_ens *ens, int steps, const char *cache_file, const char *key,
+                     int tuning[3], double *ms_per_step, double *cand_ms);
+/* Clears the device error status, so that the host may continue after it
+ * has handled the failure (for example, restored the state). */
+int f3d_ens_clear_status(f3d_ens *ens);
+/* Finite scan of member mi's state and its class's device inputs; bits of
+ * *mask as in f3d_ads_check_finite. */
+int f3d_ens_check_finite(f3d_ens *ens, int mi, int *mask);
 
 /* ---- learned settling velocity ----------------------------------------------
  * A 5 -> 64 -> 64 -> 1 tanh network standing in for the fixed-point drag-law

@@ -697,11 +697,15 @@ void or_mass_boundaries(const double fluxes[6], double *ground,
              fabs(fluxes[3]) + fabs(fluxes[4]);
 }
 
-/* ---- phys_get_vset_point: mod_Phys.F90:757-954 */
+/* ---- phys_get_vset_point: mod_Phys.F90:757-954 (maxit = 1000 at :794) */
 int or_vset_point(double diam, double rhop, double psi, double rhoa,
                   double visc, int model, double *vset_out, int *iters) {
+  return or_vset_point_n(diam, rhop, psi, rhoa, visc, model, vset_out, iters, 1000);
+}
+
+int or_vset_point_n(double diam, double rhop, double psi, double rhoa,
+                    double visc, int model, double *vset_out, int *iters, int maxit) {
   const double atol = 1e-12, rtol = 1e-6;
-  const int maxit = 1000;
   double cd = 1.0, vset, vold, rey;
   *iters = 0;
   switch (model) {
@@ -1054,3 +1058,107 @@ int or_radionuclides(const or_dims *d, double dt, const int *bin_cat,
   }
   return 0;
 }
+
+/* ---- grid_build_arakawa_c, tasks 0 and 1: mod_Grid.F90:286-676 (serial
+ * domain: my_ibs = 1, my_ibe = gl_nbx, ...).  Fortran indices are kept in the
+ * loops; F1(a, lo, idx) addresses element idx of an array whose first
+ * element has Fortran index lo. */
+#define F1(a, lo, idx) (a)[(idx) - (lo)]
+int or_build_grid(int nx, int ny, int nz, int map_h, int map_v, double lonmin,
+                  double lonmax, double latmin, double latmax, double X3max,
+                  const double *gl_sigma, const double *hc, or_grid_full *g) {
+  const int gl_nbx = nx + 1, gl_nby = ny + 1, gl_nbz = nz + 1;
+  const double PI_ = 4.0 * atan(1.0), REARTH_ = 6356000.0;
+  double dlon, dlat;
+  /* task 0 (:326-567) */
+  if (map_h == 1 && !(lonmax > lonmin))
+    dlon = (360.0 + lonmax - lonmin) / (gl_nbx - 1);
+  else
+    dlon = (lonmax - lonmin) / (gl_nbx - 1);
+  dlat = (latmax - latmin) / (gl_nby - 1);
+  g->dlon = dlon;
+  g->dlat = dlat;
+  for (int i = 1; i <= gl_nbx; ++i) F1(g->lon_c, 1, i) = lonmin + (i - 1) * dlon;
+  for (int j = 1; j <= gl_nby; ++j) F1(g->lat_c, 1, j) = latmin + (j - 1) * dlat;
+  for (int k = 1; k <= gl_nbz; ++k) F1(g->X3_c, 1, k) = F1(gl_sigma, 1, k) * X3max;
+  for (int i = 1; i <= nx; ++i)
+    F1(g->lon_p, 1, i) = 0.5 * (F1(g->lon_c, 1, i) + F1(g->lon_c, 1, i + 1));
+  for (int j = 1; j <= ny; ++j)
+    F1(g->lat_p, 1, j) = 0.5 * (F1(g->lat_c, 1, j) + F1(g->lat_c, 1, j + 1));
+  for (int k = 1; k <= nz; ++k)
+    F1(g->X3_p, 1, k) = 0.5 * (F1(g->X3_c, 1, k) + F1(g->X3_c, 1, k + 1));
+  if (map_h == 0) {
+    for (int j = 1; j <= ny; ++j) F1(g->Hm1_p, 1, j) = 1.0;
+    for (int j = 1; j <= gl_nby; ++j) F1(g->Hm1_c, 1, j) = 1.0;
+  } else if (map_h == 1) {
+    for (int j = 1; j <= ny; ++j)
+      F1(g->Hm1_p, 1, j) = sin((90.0 - F1(g->lat_p, 1, j)) * PI_ / 180.0);
+    for (int j = 1; j <= gl_nby; ++j)
+      F1(g->Hm1_c, 1, j) = sin((90.0 - F1(g->lat_c, 1, j)) * PI_ / 180.0);
+  } else {
+    return 1; /* POLAR, MERCATOR: 'Mapping not implemented yet' */
+  }
+  for (int j = -1; j <= ny + 2; ++j) F1(g->Hm2_p, -1, j) = 1.0;
+  {
+    const double d1 = (map_h == 1) ? REARTH_ * dlon * PI_ / 180.0 : dlon;
+    const double d2 = (map_h == 1) ? REARTH_ * dlat * PI_ / 180.0 : dlat;
+    for (int i = -1; i <= nx + 2; ++i) F1(g->dX1_p, -1, i) = d1;
+    for (int i = 0; i <= nx + 2; ++i) F1(g->dX1_b, 0, i) = d1;
+    for (int j = -1; j <= ny + 2; ++j) F1(g->dX2_p, -1, j) = d2;
+    for (int j = 0; j <= ny + 2; ++j) F1(g->dX2_b, 0, j) = d2;
+  }
+  /* dX3_b(kbs_1h:kbe_1h) = (0:nz+2), dX3_p(kps_2h:kpe_2h) = (-1:nz+2) */
+  for (int k = 1; k <= gl_nbz - 1; ++k)
+    F1(g->dX3_b, 0, k) = (F1(gl_sigma, 1, k + 1) - F1(gl_sigma, 1, k)) * X3max;
+  F1(g->dX3_b, 0, 0) = F1(g->dX3_b, 0, 1);
+  for (int k = gl_nbz; k <= nz + 2; ++k) F1(g->dX3_b, 0, k) = F1(g->dX3_b, 0, gl_nbz - 1);
+  for (int k = 1; k <= gl_nbz - 2; ++k) {
+    const double X3_p = 0.5 * (F1(gl_sigma, 1, k + 1) + F1(gl_sigma, 1, k)) * X3max;
+    const double X3_p1 = 0.5 * (F1(gl_sigma, 1, k + 2) + F1(gl_sigma, 1, k + 1)) * X3max;
+    F1(g->dX3_p, -1, k) = X3_p1 - X3_p;
+  }
+  for (int k = -1; k <= 0; ++k) F1(g->dX3_p, -1, k) = F1(g->dX3_p, -1, 1);
+  for (int k = nz; k <= nz + 2; ++k) F1(g->dX3_p, -1, k) = F1(g->dX3_p, -1, nz - 1);
+  if (map_h == 1) {
+    for (int i = 1; i <= gl_nbx; ++i)
+      if (F1(g->lon_c, 1, i) > 180.0) F1(g->lon_c, 1, i) = F1(g->lon_c, 1, i) - 360.0;
+    for (int i = 1; i <= nx; ++i)
+      if (F1(g->lon_p, 1, i) > 180.0) F1(g->lon_p, 1, i) = F1(g->lon_p, 1, i) - 360.0;
+  }
+  /* task 1 (:568-670): hc(ibs:ibe, jbs:jbe), column-major */
+#define HC(i, j) hc[(size_t)((i) - 1) + (size_t)gl_nbx * (size_t)((j) - 1)]
+#define P2(a, i, j) (a)[(size_t)((i) - 1) + (size_t)nx * (size_t)((j) - 1)]
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i) {
+      P2(g->dhdx_p, i, j) = 0.5 * (HC(i + 1, j) + HC(i + 1, j + 1) - HC(i, j) - HC(i, j + 1)) /
+                            F1(g->dX1_b, 0, i);
+      P2(g->dhdy_p, i, j) = 0.5 * (-HC(i + 1, j) + HC(i + 1, j + 1) - HC(i, j) + HC(i, j + 1)) /
+                            F1(g->dX2_b, 0, j);
+    }
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i) {
+      if (map_v == 0 || map_v == 1) {
+        P2(g->Hm3_p, i, j) = 1.0;
+      } else if (map_v == 2) {
+        const double h_p = 0.25 * (HC(i, j) + HC(i + 1, j) + HC(i + 1, j + 1) + HC(i, j + 1));
+        P2(g->Hm3_p, i, j) = (X3max - h_p) / X3max;
+      } else {
+        return 1; /* SIGMA_EXPONENTIAL_DECAY: 'Mapping not implemented yet' */
+      }
+    }
+  for (int j = 1; j <= gl_nby; ++j)
+    for (int i = 1; i <= gl_nbx; ++i) {
+      const double h = HC(i, j);
+      for (int k = 1; k <= gl_nbz; ++k) {
+        double z;
+        if (map_v == 0) z = F1(g->X3_c, 1, k);
+        else if (map_v == 1) z = F1(g->X3_c, 1, k) + h;
+        else z = F1(g->X3_c, 1, k) * (X3max - h) / X3max + h;
+        g->z_c[(size_t)(i - 1) + (size_t)gl_nbx * ((size_t)(j - 1) + (size_t)gl_nby * (size_t)(k - 1))] = z;
+      }
+    }
+#undef HC
+#undef P2
+  return 0;
+}
+#undef F1

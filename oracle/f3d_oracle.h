@@ -154,6 +154,10 @@ void or_mass_boundaries(const double fluxes[6], double *ground,
  * (0 ok, 1 bad model, 2 no convergence); *iters gets the iteration count. */
 int or_vset_point(double diam, double rhop, double psi, double rhoa,
                   double visc, int model, double *vset, int *iters);
+/* The same with the iteration limit maxit in place of the reference's 1000
+ * (the non-convergence path, flag 2, for tests). */
+int or_vset_point_n(double diam, double rhop, double psi, double rhoa,
+                    double visc, int model, double *vset, int *iters, int maxit);
 
 /* phys_get_vset (mod_Phys.F90:673-740): corner air density/temperature
  * rhoc,tc (ibs:ibe, jbs:jbe, kbs:kbe) -> my_vs (i,j,kb1h,bin), unscaled.
@@ -200,6 +204,24 @@ int or_radionuclides(const or_dims *d, double dt, const int *bin_cat,
 /* ensemble_perturbate_variable (mod_Ensemble.F90:888-935). */
 double or_perturb(int var_id, int ptype, double var, double random,
                   double range);
+
+/* grid_build_arakawa_c, tasks 0 and 1 (mod_Grid.F90:286-676), serial
+ * domain.  Arrays (caller-allocated) with their reference bounds:
+ * dX1_p(-1:nx+2), dX1_b(0:nx+2), dX2_p(-1:ny+2), dX2_b(0:ny+2),
+ * dX3_p(-1:nz+2), dX3_b(0:nz+2), Hm2_p(-1:ny+2); lon_c(nx+1), lat_c(ny+1),
+ * X3_c(nz+1), lon_p(nx), lat_p(ny), X3_p(nz), Hm1_p(ny), Hm1_c(ny+1);
+ * dhdx_p, dhdy_p, Hm3_p (nx, ny); z_c (nx+1, ny+1, nz+1) column-major; the
+ * input topography hc (nx+1, ny+1).  Returns 1 for the mappings the
+ * reference leaves unimplemented. */
+typedef struct {
+  double dlon, dlat;
+  double *lon_c, *lat_c, *X3_c, *lon_p, *lat_p, *X3_p, *Hm1_p, *Hm1_c, *Hm2_p;
+  double *dX1_p, *dX1_b, *dX2_p, *dX2_b, *dX3_p, *dX3_b;
+  double *dhdx_p, *dhdy_p, *Hm3_p, *z_c;
+} or_grid_full;
+int or_build_grid(int nx, int ny, int nz, int map_h, int map_v, double lonmin,
+                  double lonmax, double latmin, double latmax, double X3max,
+                  const double *gl_sigma, const double *hc, or_grid_full *g);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,8 @@ def lib():
         L.or_mass_boundaries.argtypes = [dp, dp, dp]
         L.or_vset_point.argtypes = [C.c_double] * 5 + [C.c_int, dp, C.POINTER(C.c_int)]
         L.or_vset_point.restype = C.c_int
+        L.or_vset_point_n.argtypes = [C.c_double] * 5 + [C.c_int, dp, C.POINTER(C.c_int), C.c_int]
+        L.or_vset_point_n.restype = C.c_int
         L.or_get_vset.argtypes = [D, C.c_int, dp, dp, dp, dp, dp, C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), C.c_double, dp]
         L.or_get_vset.restype = C.c_int
@@ -85,6 +87,8 @@ def lib():
         L.or_gc_state.argtypes = [D, dp, C.c_double, dp, dp, dp, dp]
         L.or_gc_state.restype = C.c_int
         L.or_add_radial_wind.argtypes = [D, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp]
+        L.or_build_grid.argtypes = [C.c_int] * 5 + [C.c_double] * 5 + [dp, dp, C.POINTER(GridFull)]
+        L.or_build_grid.restype = C.c_int
         _lib = L
     return _lib
 
@@ -261,10 +265,14 @@ def ads_solve_1d(c, dxp, dxb, u, k, dt, bvalue=(0.0, 0.0), bcode=(2, 2), limiter
     return c, flux
 
 
-def vset_point(diam, rhop, psi, rhoa, visc, model=2):
+def vset_point(diam, rhop, psi, rhoa, visc, model=2, maxit=None):
     v = C.c_double()
     it = C.c_int()
-    flag = lib().or_vset_point(diam, rhop, psi, rhoa, visc, model, C.byref(v), C.byref(it))
+    if maxit is None:
+        flag = lib().or_vset_point(diam, rhop, psi, rhoa, visc, model, C.byref(v), C.byref(it))
+    else:
+        flag = lib().or_vset_point_n(diam, rhop, psi, rhoa, visc, model, C.byref(v), C.byref(it),
+                                     int(maxit))
     return v.value, flag, it.value
 
 
@@ -279,6 +287,32 @@ def mass_boundaries(fluxes):
     g, l = C.c_double(), C.c_double()
     lib().or_mass_boundaries(_p(np.asarray(fluxes, np.float64)), C.byref(g), C.byref(l))
     return g.value, l.value
+
+
+class GridFull(C.Structure):
+    _fields_ = [("dlon", C.c_double), ("dlat", C.c_double)] + [
+        (n, C.POINTER(C.c_double)) for n in (
+            "lon_c", "lat_c", "X3_c", "lon_p", "lat_p", "X3_p", "Hm1_p", "Hm1_c", "Hm2_p",
+            "dX1_p", "dX1_b", "dX2_p", "dX2_b", "dX3_p", "dX3_b", "dhdx_p", "dhdy_p", "Hm3_p",
+            "z_c")]
+
+
+def build_grid(nx, ny, nz, map_h, map_v, lonmin, lonmax, latmin, latmax, X3max, gl_sigma, h_c):
+    """grid_build_arakawa_c (mod_Grid.F90:286-676), tasks 0 and 1, in the C
+    restatement.  Returns a dict of the arrays (0-based storage of the
+    reference bounds, as fall3d_b200.grid keeps them) and the flag."""
+    shapes = {"lon_c": nx + 1, "lat_c": ny + 1, "X3_c": nz + 1, "lon_p": nx, "lat_p": ny, "X3_p": nz,
+              "Hm1_p": ny, "Hm1_c": ny + 1, "Hm2_p": ny + 4, "dX1_p": nx + 4, "dX1_b": nx + 3,
+              "dX2_p": ny + 4, "dX2_b": ny + 3, "dX3_p": nz + 4, "dX3_b": nz + 3,
+              "dhdx_p": (nx, ny), "dhdy_p": (nx, ny), "Hm3_p": (nx, ny), "z_c": (nx + 1, ny + 1, nz + 1)}
+    arr = {k: np.zeros(v, order="F") for k, v in shapes.items()}
+    gf = GridFull(0.0, 0.0, *[_p(arr[n]) for n, _ in GridFull._fields_[2:]])
+    sig = np.ascontiguousarray(gl_sigma, dtype=np.float64)
+    hc = np.asfortranarray(h_c, dtype=np.float64)
+    flag = lib().or_build_grid(nx, ny, nz, map_h, map_v, lonmin, lonmax, latmin, latmax, X3max,
+                               _p(sig), _p(hc), C.byref(gf))
+    arr["dlon"], arr["dlat"] = gf.dlon, gf.dlat
+    return arr, flag
 
 
 def perturb(var_id, ptype, var, random, range_):

@@ -82,7 +82,7 @@ def test_fp64_members_bitexact_to_oracle(oracle_mod, built_lib, mode):
     ens.close()
 
 
-@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_persistent_equals_kernels_and_device_clock(oracle_mod, built_lib, precision):
     cls = _classes(oracle_mod)
     outs = []
@@ -137,18 +137,25 @@ def test_member_cfl_matches_single_domain(oracle_mod, built_lib):
 
 
 def test_fp32_ensemble_error_vs_fp64(oracle_mod, built_lib):
+    """Both precision forms of every member within 1e-5 relative L2 of the
+    FP64 member; the compensated form also keeps each member's mass in the
+    volume within 1e-9 of the FP64 member's."""
     cls = _classes(oracle_mod)
-    res = []
-    for prec in (0, 1):
+    res, mass = [], []
+    for prec in (0, 1, 2):
         ens = _build(cls, prec)
         ens.compute_time_steps(0.5, 2, 0.9, 1e30)
         ens.set_clock(np.zeros(len(CLASSES)), 0)
         ens.run(5)
         res.append([interior(ens.download_member_state(m)[0]) for m in range(len(CLASSES))])
+        mass.append([ens.mass_volume(m) for m in range(len(CLASSES))])
         ens.close()
     for m in range(len(CLASSES)):
-        a, b = res[0][m], res[1][m]
-        assert np.linalg.norm(b - a) <= 1e-5 * np.linalg.norm(a), m
+        a = res[0][m]
+        for q in (1, 2):
+            assert np.linalg.norm(res[q][m] - a) <= 1e-5 * np.linalg.norm(a), (m, q)
+        assert np.linalg.norm(res[2][m] - a) <= 1e-6 * np.linalg.norm(a), m
+        assert abs(mass[2][m] / mass[0][m] - 1.0) <= 1e-9, (m, mass[2][m], mass[0][m])
 
 
 def test_autotune_picks_a_working_shape(oracle_mod, built_lib, tmp_path, monkeypatch):
@@ -157,11 +164,14 @@ def test_autotune_picks_a_working_shape(oracle_mod, built_lib, tmp_path, monkeyp
     ens = _build(cls, 1)
     ens.compute_time_steps(0.5, 2, 0.9, 1e30)
     ens.set_clock(np.zeros(len(CLASSES)), 0)
-    best = autotune(ens, "test-key", steps=2)
-    assert best["ms_per_step"] > 0 and len(best["all"]) >= 3
-    assert (tmp_path / "autotune.json").exists()
-    again = autotune(ens, "test-key")
-    assert again["tuning"] == best["tuning"]
+    best = autotune(ens, "test-key", steps=2)  # f3d_ens_autotune through the C ABI
+    assert best["ms_per_step"] > 0 and len(best["all"]) == 5
+    assert sum("ms_per_step" in r for r in best["all"]) >= 3
+    assert (tmp_path / "autotune.txt").exists()
+    again = autotune(ens, "test-key")  # read from the cache file, not re-timed
+    assert again["tuning"] == best["tuning"] and again["ms_per_step"] == best["ms_per_step"]
+    ens.run(1)
+    assert ens.status() == 0
     ens.close()
 
 

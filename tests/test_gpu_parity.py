@@ -49,6 +49,21 @@ def test_step_bitexact_ragged_shapes(oracle_mod, built_lib, shape):
     _assert_fluxes(f_o, f_g)
 
 
+def test_step_bitexact_subnormal_values(oracle_mod, built_lib):
+    """A state whose values reach the subnormal range (the far fringe of a
+    plume after many steps): the device's divisions by the grid spacings
+    must round those quotients as IEEE division does."""
+    wl = W.small_case(seed=21)
+    wl.src_vals = 0.0 * wl.src_vals  # nothing of normal size enters
+    c0, a0 = W.random_state(wl, seed=5)
+    c0 *= 1e-303  # values from ~1e-306 down into the subnormal range
+    (c_o, a_o, f_o), (c_g, a_g, f_g), _ = run_pair(oracle_mod, wl, nsteps=4, dt=7.5, c0=c0, acum0=a0)
+    nz = interior(c_o)[interior(c_o) != 0]
+    assert (np.abs(nz) < 2.2250738585072014e-308).mean() > 0.05
+    _assert_bitwise(interior(c_o), interior(c_g), "c")
+    _assert_bitwise(acum_interior(a_o), acum_interior(a_g), "acum")
+
+
 def test_tephra_c1_steps_bitexact(oracle_mod, built_lib):
     """The 100x80x40 6-bin tephra case, 6 steps from rest with the source on."""
     wl = W.tephra_c1()
