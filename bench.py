@@ -615,7 +615,9 @@ def run_ensemble(args, ws, rank, local, pg):
                      "deposit_rel": abs(d32 / d64 - 1.0) if d64 else 0.0,
                      # mass budget: in the volume + ground deposit + out through
                      # the lateral and top boundaries (mod_Grid.F90:1340-1511)
-                     "mass_rel": abs((mv32 + d32 + out32) / (mv64 + d64 + out64) - 1.0)})
+                     "mass_rel": abs((mv32 + d32 + out32) / (mv64 + d64 + out64) - 1.0),
+                     # grid_get_mass_volume alone (mod_Grid.F90:1340-1389)
+                     "mass_volume_rel": abs(mv32 / mv64 - 1.0)})
         del c64, a64, c32, a32, i64, i32
         n_c = ew.member_class.count(ci)
         # every plain member job recomputes its own settling velocity by the iteration
@@ -624,10 +626,60 @@ def run_ensemble(args, ws, rank, local, pg):
     fp64_step_ms = sum(ew.member_class.count(ci) * fp64_ms[ci] / K for ci in range(len(reps)))
     fp64_tot = fp64_step_ms + iter_amort
     out.update(fp64_value=ws * cbs / (fp64_tot / 1e3), fp64_ms_per_step=fp64_tot,
+               fp64_steps_value=ws * cbs / (fp64_step_ms / 1e3),
                fp64_class_ms_per_step=[round(x / K, 3) for x in fp64_ms], errors=errs)
     out["ens"], out["sur"], out["dts"], out["reps"] = ens, sur, dts, reps
     out["steps_per_meteo"] = steps_per_meteo
     return out
+
+
+# FP64 operations (DFMA + DADD + DMUL, thread level) per cell*bin*step of the
+# plain FP64 sweeps, from ncu on the 400x300x60x20 case
+# (profiles/k_sweep64_c2.md); FP64 pipe of the B200: 64 operations per clock
+# per SM on 148 SMs.
+FP64_OPS_PER_CELLBIN_STEP = 1015
+
+
+def fp64_roofline(steps_value, sm_mhz):
+    if not FP64_OPS_PER_CELLBIN_STEP or not sm_mhz:
+        return None
+    peak = 148 * 64 * sm_mhz * 1e6
+    achieved = FP64_OPS_PER_CELLBIN_STEP * steps_value
+    return {"bound": "fp64 pipe", "ops_per_cellbin_step": FP64_OPS_PER_CELLBIN_STEP,
+            "achieved_tops": round(achieved / 1e12, 3), "peak_tops": round(peak / 1e12, 3),
+            "frac": round(achieved / peak, 4),
+            "note": "step kernels of the plain FP64 form (settling velocity excluded); "
+                    "peak = 148 SMs x 64 FP64 ops/clock at the sampled SM clock"}
+
+
+def time_plain_fp32(args, ew, ws, local, pg, tuning):
+    """The plain FP32 form (no compensated state) on the same ensemble, for
+    reference: W + K steps from rest, device time of the K."""
+    import torch
+    from fall3d_b200.ensemble import Ensemble
+    nb = ew.nbins
+    ens = Ensemble([c.grid for c in ew.classes], nb, ew.member_class, ew.wind_factor, 2, 2, 1, local)
+    for ci, wl in enumerate(ew.classes):
+        ens.set_class_meteo(ci, wl.u12, wl.v12, wl.w12, wl.k1, wl.k2, wl.k3, None, wl.t_its, wl.t_ite)
+        ens.compute_class_vset(ci, wl.vset_model, wl.rhoc, wl.tc, wl.diam, wl.rhop, wl.psi, wl.bin_cat)
+    for m, (ijk, vals) in enumerate(ew.src):
+        ens.set_member_source(m, ijk, vals)
+    ens.compute_time_steps(0.5, 2, 0.9, ew.classes[0].run_end)
+    ens.set_tuning(*tuning)
+    ens.set_clock(np.zeros(len(ew.member_class)), 0)
+    ens.run(args.warmup)
+    ens.synchronize()
+    s = torch.cuda.ExternalStream(ens.stream_ptr, device=torch.device("cuda", local))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(pg)
+    e0.record(s)
+    ens.run(args.steps)
+    e1.record(s)
+    ens.synchronize()
+    ms = max_over_ranks(pg, e0.elapsed_time(e1)) / args.steps
+    ens.close()
+    return {"value": ws * float(ew.cell_bins()) / (ms / 1e3), "ms_per_step": round(ms, 3),
+            "note": "plain FP32 state, same workload and tuning, step kernels only"}
 
 
 def ens_roofline(r, K):
@@ -824,6 +876,7 @@ def line_ensemble(args, ws, res):
         "fp64_plain_value": res["fp64_value"],
         "fp64_ms_per_step": res["fp64_ms_per_step"],
         "speedup_vs_fp64_plain": res["value"] / res["fp64_value"],
+        "fp64_roofline": fp64_roofline(res["fp64_steps_value"], res["clocks"].get("sm_mhz")),
         "steps_only_value": res["steps_only_value"],
         "gpu_launches": res["launches"],
         "clocks": res["clocks"],
@@ -833,6 +886,7 @@ def line_ensemble(args, ws, res):
             "conc_rel_l2_max": max(x["conc_rel_l2"] for x in e),
             "deposit_rel_max": max(x["deposit_rel"] for x in e),
             "mass_rel_max": max(x["mass_rel"] for x in e),
+            "mass_volume_rel_max": max(x["mass_volume_rel"] for x in e),
             "members": e},
         "tuning": res["tuning"],
         "vset": dict(res["vset"], amortised_ms_per_step=res["vset_amortised_ms_per_step"],
@@ -852,6 +906,8 @@ def main():
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "c2", "aux"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp32c", choices=sorted(PRECISIONS))
+    ap.add_argument("--no-plain-fp32", action="store_true",
+                    help="skip timing the plain FP32 form beside the compensated headline")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -877,9 +933,15 @@ def main():
                 # the reference arm's sample, with up to 10 of its steps (about 45 s)
                 line["cpu_baseline"] = cpu_baseline_ensemble(res["workload"], res["dts"],
                                                              steps=min(args.steps, 10), warm=1)
-            print(json.dumps(line), flush=True)
+        tuning = res["ens"].tuning
         res["ens"].close()
         res["sur"].close()
+        if args.precision == "fp32c" and not args.no_plain_fp32:
+            plain = time_plain_fp32(args, res["workload"], ws, local, pg, tuning)
+            if rank == 0:
+                line["fp32_plain"] = plain
+        if rank == 0:
+            print(json.dumps(line), flush=True)
         if pg is not None:
             pg.destroy_process_group()
         return

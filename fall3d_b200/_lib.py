@@ -116,6 +116,9 @@ SIGNATURES = {
     "f3d_ens_launch_count": [_vp, C.POINTER(C.c_longlong)],
     "f3d_ens_status": [_vp, _ip],
     "f3d_ens_clear_status": [_vp],
+    "f3d_ens_keep_boundary_halo": [_vp, C.c_int],
+    "f3d_ens_set_member_gravity_current": [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp],
+    "f3d_ens_gravity_current_time_steps": [_vp, _dp, _dp, C.c_int, C.c_double, C.c_double, _ip, _dp],
     "f3d_ens_autotune": [_vp, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(C.c_int), _dp, _dp],
     "f3d_ens_check_finite": [_vp, C.c_int, _ip],
     "f3d_ads_check_finite": [_vp, _ip],

@@ -13,6 +13,8 @@
 //  * stage updates use FMA.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "f3d_common.cuh"
 #include "march.cuh"
 #include "step_dev.cuh"
@@ -37,6 +39,9 @@ __device__ __forceinline__ float xor_sign(float x, unsigned int s) {
 #endif
 #ifndef F3D_CMP_EFT
 #define F3D_CMP_EFT 1
+#endif
+#ifndef F3D_CMP_XW
+#define F3D_CMP_XW 16
 #endif
 #ifndef F3D_FFORM
 #define F3D_FFORM 0
@@ -108,15 +113,20 @@ struct Ops32 {
   float* lop;          // CMP: low part of the state, same layout and stride as cp
   const double* r64;   // CMP: 1/dxb of the pencil's cells, FP64
   const float2* r2;    // CMP: the same as FP32 pairs {hi, lo}
-  double dtf;          // CMP: weight of the face sums (dt/6 for RK4, dt for Euler), FP64
-  float dtf_hi, dtf_lo;  // CMP: dtf as an FP32 pair
+  float dtf_hi, dtf_lo;  // CMP: weight of the face sums, dt/6 (RK4) or dt (Euler),
+                         // as an FP32 pair: folded into the FP32 sums it would scale
+                         // the interior transport against the FP64 boundary terms
   const float4* fd;   // face data {u(its), u(ite), kf, 1/dxb(f-1)} (MemberDev::f4)
   const float* vsub;  // z: settling velocity of the bin
   long long vs;
   int nf;  // cells of the pencil (faces 0..nf)
   float s0, s1, wfac;
   float dt, hdt, dt3, dt6;
-  XTile<float, (TM == 2) ? 1 : 2> xt;  // x pencils: shared-memory staging of the rows
+  // x pencils: shared-memory staging of the rows (the compensated form also
+  // stages the low part, in narrower chunks so that both tiles fit)
+  static constexpr int XW = CMP ? F3D_CMP_XW : 32;
+  XTile<float, (TM == 2) ? 1 : 2, XW> xt;
+  XLoTile<XW> lt;
 
   __device__ __forceinline__ float load_c(int p) const {
     if constexpr (DIR == DIR_X) {
@@ -131,10 +141,22 @@ struct Ops32 {
     if constexpr (DIR == DIR_X) xt.store(p, v);
     else cp[p * cs] = v;
   }
-  __device__ __forceinline__ void stage_init() { if constexpr (DIR == DIR_X) xt.init(); }
-  __device__ __forceinline__ void stage_begin(int T0) { if constexpr (DIR == DIR_X) xt.block_begin(T0); }
-  __device__ __forceinline__ void stage_end(int T0) { if constexpr (DIR == DIR_X) xt.block_end(T0); }
-  __device__ __forceinline__ void stage_finish() { if constexpr (DIR == DIR_X) xt.finish(); }
+  __device__ __forceinline__ void stage_init() {
+    if constexpr (DIR == DIR_X) xt.init();
+    if constexpr (DIR == DIR_X && CMP) lt.init();
+  }
+  __device__ __forceinline__ void stage_begin(int T0) {
+    if constexpr (DIR == DIR_X) xt.block_begin(T0);
+    if constexpr (DIR == DIR_X && CMP) lt.block_begin(T0);
+  }
+  __device__ __forceinline__ void stage_end(int T0) {
+    if constexpr (DIR == DIR_X) xt.block_end(T0);
+    if constexpr (DIR == DIR_X && CMP) lt.block_end(T0);
+  }
+  __device__ __forceinline__ void stage_finish() {
+    if constexpr (DIR == DIR_X) xt.finish();
+    if constexpr (DIR == DIR_X && CMP) lt.finish();
+  }
   __device__ __forceinline__ FaceV<float> face(int f) const {
     if constexpr (F3D_FACE_PF > 0) {
       const long long fp = (long long)min(f + F3D_FACE_PF, nf) * vs;
@@ -173,20 +195,32 @@ struct Ops32 {
   __device__ __forceinline__ float rk_final(float nw, float k) const { return fmaf(dt6, k, nw); }
 
   // Compensated final update of cell p (CMP): c(p) = hi + lo advanced by
-  // dtf (H(p+1) - H(p)) / dxb(p) in FP64 and split back into hi + lo.  The
-  // difference of two FP32 face sums is exact in FP64 and 1/dxb is FP64, so
-  // the cell's change times its volume is the two shared face sums to FP64
-  // rounding: the sweep conserves mass to ~1e-16 of the transported mass,
-  // and the state carries ~48 bits.
-  __device__ __forceinline__ float final_cmp(float chi, float hl, float hr, int p) {
-    float* lp = lop + (long long)p * cs;
-    prefetch_line(lop + (long long)min(p + 16, nf - 1) * cs);  // a later cell's low part
-    const float clo = *lp;
+  // dtf (H(p+1) - H(p)) / dxb(p) and split back into hi + lo.  The difference of
+  // the two FP32 face sums is formed exactly and 1/dxb carries ~48 bits, so
+  // the cell's change times its volume is the two face sums it shares with
+  // its neighbours to ~2^-47: the sweep conserves mass to ~1e-14 of the
+  // transported mass, and the state carries ~48 bits.
+  // low part of cell p (y, z: global, with an L1 prefetch of a later cell's
+  // line; x: the staged tile)
+  __device__ __forceinline__ float lo_fetch(int p) {
+    if constexpr (DIR == DIR_X) {
+      return lt.at(p);
+    } else {
+      prefetch_line(lop + (long long)min(p + 16, nf - 1) * cs);
+      return lop[(long long)p * cs];
+    }
+  }
+  __device__ __forceinline__ void lo_store(int p, float v) {
+    if constexpr (DIR == DIR_X) lt.at(p) = v;
+    else lop[(long long)p * cs] = v;
+  }
+  __device__ __forceinline__ float final_cmp(float chi, float clo, float hl, float hr, int p) {
 #if F3D_CMP_EFT
-    // The same in FP32 pair arithmetic (error-free transformations; every
-    // operation explicitly rounded, none contracted):
+    // In FP32 pair arithmetic (error-free transformations; every operation
+    // explicitly rounded, none contracted):
     //   hr - hl = s + e exactly (Knuth's TwoSum),
-    //   X = (s + e) (1/dxb as hi + lo), D = X (dtf as hi + lo), each to ~2^-48,
+    //   X = (s + e) (1/dxb as hi + lo), D = X (dtf as hi + lo), each to ~2^-47
+    //   (Dekker's products by FMA),
     //   (chi + clo) + D summed with TwoSum and renormalised to hi + lo.
     const float s = __fsub_rn(hr, hl);
     const float sb = __fsub_rn(s, hr);
@@ -205,13 +239,13 @@ struct Ops32 {
     float te = __fadd_rn(__fsub_rn(chi, __fsub_rn(t, tb)), __fsub_rn(d, tb));
     te = __fadd_rn(te, __fadd_rn(clo, de));
     const float nhi = __fadd_rn(t, te);
-    *lp = __fsub_rn(te, __fsub_rn(nhi, t));
+    lo_store(p, __fsub_rn(te, __fsub_rn(nhi, t)));
     return nhi;
 #else
-    const double dlt = ((double)hr - (double)hl) * (dtf * __ldg(r64 + p));
+    const double dlt = ((double)hr - (double)hl) * ((double)dtf_hi + (double)dtf_lo) * __ldg(r64 + p);
     const double c64 = ((double)chi + (double)clo) + dlt;
     const float nhi = __double2float_rn(c64);
-    *lp = __double2float_rn(c64 - (double)nhi);
+    lo_store(p, __double2float_rn(c64 - (double)nhi));
     return nhi;
 #endif
   }
@@ -290,13 +324,15 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       int k = (int)(pen / ny);
       n = nx;
       o.cp = m.c32 + (((long long)b * nz + k) * ny + j) * nx;
+      constexpr int xbytes = decltype(o.xt)::BYTES + (CMP ? decltype(o.lt)::BYTES : 0);
+      o.xt.setup(f3d_smem + warp * xbytes, lane_ok ? o.cp : nullptr, threadIdx.x & 31, nx);
       if constexpr (CMP) {
         o.lop = m.c32lo + (((long long)b * nz + k) * ny + j) * nx;
         o.r64 = m.rdxb64[0];
         o.r2 = m.rdxb2[0];
+        o.lt.setup(f3d_smem + warp * xbytes + decltype(o.xt)::BYTES, o.xt.rows,
+                   (long long)(m.c32lo - m.c32), threadIdx.x & 31, nx);
       }
-      o.xt.setup(f3d_smem + warp * decltype(o.xt)::BYTES, lane_ok ? o.cp : nullptr,
-                 threadIdx.x & 31, nx);
       o.cs = 1;
       long long fo = (long long)k * (nx + 1) * ny + j;
       o.fd = (m.gc_cur ? m.gc4[0] : m.f4[0]) + fo;
@@ -359,9 +395,9 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
     o.dt3 = o.dt * (1.f / 3.f);
     o.dt6 = o.dt * (1.f / 6.f);
     if constexpr (CMP) {
-      o.dtf = (TM == 2) ? dt / 6.0 : dt;
-      o.dtf_hi = __double2float_rn(o.dtf);
-      o.dtf_lo = __double2float_rn(o.dtf - (double)o.dtf_hi);
+      const double dtf = (TM == 2) ? dt / 6.0 : dt;
+      o.dtf_hi = __double2float_rn(dtf);
+      o.dtf_lo = __double2float_rn(dtf - (double)o.dtf_hi);
     }
     // the edge blocks run the unguarded body (cheaper than the guarded one)
     March<float, Ops32<LIM, DIR, TM, CMP>, TM, true, CMP> M(o, n);
@@ -403,9 +439,14 @@ template <int DIR, bool CMP>
 static void launch_dir32(int lim, int tm, const MemberDev* members, const WorkItem* work,
                          int nblocks, int bpb, cudaStream_t st) {
   dim3 g(nblocks), b(128);
-  // RK4 x tiles keep one output buffer (XTile<float, 1>), Euler two
-  const int smem_max = (DIR == DIR_X) ? 4 * XTile<float, 2>::BYTES : 0;
-  const int smem = (DIR == DIR_X) ? 4 * ((tm == 2) ? XTile<float, 1>::BYTES : XTile<float, 2>::BYTES) : 0;
+  // RK4 x tiles keep one output buffer (XTile<float, 1>), Euler two; the
+  // compensated form stages the low part as well, in chunks of F3D_CMP_XW
+  constexpr int cw = CMP ? F3D_CMP_XW : 32;
+  constexpr int lob = CMP ? XLoTile<cw>::BYTES : 0;
+  const int smem_max = (DIR == DIR_X) ? 4 * (XTile<float, 2, cw>::BYTES + lob) : 0;
+  const int smem = (DIR == DIR_X)
+                       ? 4 * (((tm == 2) ? XTile<float, 1, cw>::BYTES : XTile<float, 2, cw>::BYTES) + lob)
+                       : 0;
   static bool attr_set = false;
   if (!attr_set && smem_max > 0) {
     cudaFuncSetAttribute(k_sweep32<DIR, 1, 1, CMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
@@ -585,7 +626,10 @@ __global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
   }
 }
 
-int fused32_smem() { return 4 * XTile<float, 2>::BYTES; }
+int fused32_smem() {
+  return 4 * std::max(XTile<float, 2>::BYTES,
+                      XTile<float, 2, F3D_CMP_XW>::BYTES + XLoTile<F3D_CMP_XW>::BYTES);
+}
 
 template <bool CMP>
 static const void* fused32_func_t(int lim, int tm) {

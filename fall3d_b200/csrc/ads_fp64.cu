@@ -16,6 +16,13 @@
 #include "march.cuh"
 #include "step_dev.cuh"
 
+#ifndef F3D_PF64
+#define F3D_PF64 1
+#endif
+#ifndef F3D_V64
+#define F3D_V64 1
+#endif
+
 namespace f3d {
 
 // Limiter r(i) from d1 = c(i)-c(i-1), d0 = c(i+1)-c(i)  (mod_ADS.F90:1124-1223).
@@ -56,7 +63,7 @@ struct Ops64 {
       return xt.load(p);
     } else {
       // the line of a later position into L1 ahead of its load
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(cp + (long long)min(p + 8, nf - 1) * cs));
+      if (F3D_PF64) asm volatile("prefetch.global.L1 [%0];" ::"l"(cp + (long long)min(p + 8, nf - 1) * cs));
       return cp[p * cs];
     }
   }
@@ -70,7 +77,7 @@ struct Ops64 {
   __device__ __forceinline__ void stage_end(int T0) { if constexpr (DIR == DIR_X) xt.block_end(T0); }
   __device__ __forceinline__ void stage_finish() { if constexpr (DIR == DIR_X) xt.finish(); }
   __device__ __forceinline__ FaceV<double> face(int f) const {
-    {
+    if (F3D_PF64) {
       const long long fp = (long long)min(f + 8, nf) * vs;
       asm volatile("prefetch.global.L1 [%0];" ::"l"(vel + fp));
       asm volatile("prefetch.global.L1 [%0];" ::"l"(kk + fp));
@@ -222,7 +229,7 @@ __device__ __forceinline__ void sweep64_item(const MemberDev* __restrict__ membe
     o.dt = m.dt;
     o.hdt = 0.5 * m.dt;
     // RK4: the edge blocks run the unguarded body (cheaper than the guarded one)
-    March<double, Ops64<LIM, DIR>, TM, true> M(o, n);
+    March<double, Ops64<LIM, DIR>, TM, (F3D_V64 != 0)> M(o, n);
     M.run();
     const double dt = m.dt;
     if (lane_ok) {

@@ -64,6 +64,8 @@ void launch_meteo_corners(const MetGeo& g, const double* uc, const double* vc, c
 void launch_meteo_kconst(int nx, int ny, int nz, double kh, double kv, double* k1, double* k2,
                          double* k3, cudaStream_t st);
 void launch_face_kk(MemberDev* members, int mi, cudaStream_t st);
+void launch_gc_winds(MemberDev* members, int mi, int nx, int ny, int nz, int fp32, const GcArgs& g,
+                     cudaStream_t st);
 void launch_nonfinite(const double* p, long long n, int bit, unsigned int* mask, cudaStream_t st);
 void launch_nonfinite(const float* p, long long n, int bit, unsigned int* mask, cudaStream_t st);
 void launch_fp32_fields(MemberDev* members, int mi, cudaStream_t st);
@@ -125,7 +127,9 @@ struct EnsClass {
   double* powpb = nullptr;       // wet deposition: P^b per column
   int* ktop = nullptr;           // and the cells below the boundary-layer top
   bool wet_set = false;
-  double* zc = nullptr;          // corner heights (output reductions)
+  double* zc = nullptr;          // corner heights (output reductions, gravity current)
+  std::vector<double> gc_host;   // lon_c, lat_c, lon_p, lat_p, Hm1_c of the class grid
+  double* gc_xy = nullptr;       // the same on the device
 };
 
 }  // namespace
@@ -134,6 +138,9 @@ struct f3d_ens {
   int ncls = 0, nm = 0, nb = 0, lim = 2, tm = 2, prec = 0, device = 0;
   int cmp = 0;  // precision form with the compensated (hi + lo) state
   int mode = F3D_ENS_MODE_KERNELS, bpb = 4, ctas_per_sm = 0;
+  // gravity current per member (F3D_add_radial_wind): parameters and whether set
+  std::vector<std::vector<double>> gc_p;
+  bool gc_any = false;
   cudaStream_t st = nullptr;
   std::vector<EnsClass> cls;
   std::vector<int> member_class;
@@ -863,6 +870,17 @@ extern "C" int f3d_ens_upload_member_state(f3d_ens* e, int mi, const double* my_
     }
   }
   if (my_acum && ens_upload_conv(e, k, 8, my_acum, (nx + 4) * (ny + 4) * nb, m.acum)) return 1;
+  if (my_c && (m.gh64 || m.gh32)) {  // the halo cells of the given state
+    std::vector<double> g;
+    gh_gather_ref(m.nx, m.ny, m.nz, (int)nb, my_c, g);
+    if (m.gh64) {
+      ECK(cudaMemcpy(m.gh64, g.data(), g.size() * 8, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> t(g.size());
+      for (size_t q = 0; q < g.size(); ++q) t[q] = (float)g[q];
+      ECK(cudaMemcpy(m.gh32, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+    }
+  }
   return 0;
 }
 
@@ -891,6 +909,17 @@ extern "C" int f3d_ens_download_member_state(f3d_ens* e, int mi, double* my_c, d
         for (size_t j = 0; j < ny; ++j)
           memcpy(&my_c[2 + (nx + 4) * ((j + 2) + (ny + 4) * ((kk + 2) + (nz + 4) * b))],
                  &tmp[((b * nz + kk) * ny + j) * nx], nx * 8);
+    if (m.gh64 || m.gh32) {  // the kept boundary halo layers
+      std::vector<double> g((size_t)gh_per_bin(m.nx, m.ny, m.nz) * nb);
+      if (m.gh64) {
+        ECK(cudaMemcpy(g.data(), m.gh64, g.size() * 8, cudaMemcpyDeviceToHost));
+      } else {
+        std::vector<float> t(g.size());
+        ECK(cudaMemcpy(t.data(), m.gh32, t.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < t.size(); ++q) g[q] = t[q];
+      }
+      gh_scatter_ref(m.nx, m.ny, m.nz, (int)nb, g, my_c);
+    }
   }
   if (my_acum) {
     std::vector<double> tmp(nx * ny * nb);
@@ -1064,6 +1093,9 @@ int enqueue_wet_radio(f3d_ens* e) {
       r.c32 = d.c32;
       r.c32lo = d.c32lo;
       r.acum = d.acum;
+      r.gh64 = d.gh64;
+      r.gh32 = d.gh32;
+      r.ngh = gh_per_bin(d.nx, d.ny, d.nz);
       r.awet = e->awet.empty() ? nullptr : e->awet[m];
       launch_radio(r, e->st);
       e->launches += 1;
@@ -1080,9 +1112,12 @@ int wet_radio_launches(const f3d_ens* e) {
   return n + (e->radio_on ? e->nm : 0);
 }
 
-int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullptr) {
+int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullptr,
+                 const std::vector<std::pair<int, GcArgs>>* gcl = nullptr) {
   if (ev) ECK(cudaEventRecord(ev[0], e->st));
-  if (e->mode == F3D_ENS_MODE_PERSISTENT) {
+  // a step with the gravity current runs the per-phase kernels, which take
+  // the radial wind between the wind preparation and the sweeps
+  if (e->mode == F3D_ENS_MODE_PERSISTENT && !(gcl && !gcl->empty())) {
     const void* func;
     int smem;
     if (fused_setup(e, &func, &smem)) return 1;
@@ -1108,12 +1143,16 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullpt
     if (ev) ECK(cudaEventRecord(ev[5], e->st));
     return 0;
   }
-  if (e->prec == F3D_PREC_FP64) {
-    launch_prep64(e->dm, e->dprep_member, e->dprep_first, e->nprep, 7, e->st);
-    launch_source64(e->dm, e->nm, e->st);
-  } else {
-    launch_source32(e->dm, e->nm, e->st);
+  if (e->prec == F3D_PREC_FP64) launch_prep64(e->dm, e->dprep_member, e->dprep_first, e->nprep, 7, e->st);
+  if (gcl) {  // F3D_add_radial_wind on the members' interpolated winds (mod_F3D.F90:1443-1445)
+    for (const auto& q : *gcl) {
+      const MemberDev& m = e->hm[q.first];
+      launch_gc_winds(e->dm, q.first, m.nx, m.ny, m.nz, e->prec == F3D_PREC_FP32, q.second, e->st);
+      e->launches += 1;
+    }
   }
+  if (e->prec == F3D_PREC_FP64) launch_source64(e->dm, e->nm, e->st);
+  else launch_source32(e->dm, e->nm, e->st);
   e->launches += (e->prec == F3D_PREC_FP64) ? 2 : 1;
   if (ev) ECK(cudaEventRecord(ev[1], e->st));
   const int order[3] = {xfirst ? DIR_X : DIR_Y, xfirst ? DIR_Y : DIR_X, DIR_Z};
@@ -1193,6 +1232,9 @@ int kernels_per_step(const f3d_ens* e) {
 
 extern "C" int f3d_ens_run(f3d_ens* e, int nsteps) {
   if (!e || nsteps < 0) return set_error_msg("f3d_ens_run: bad arguments");
+  if (e->gc_any)
+    return set_error_msg("f3d_ens_run: a member has a gravity current, whose radial wind and time "
+                         "step change every step; advance with f3d_ens_step");
   for (const EnsClass& k : e->cls)
     if (k.rep >= 0 && (!k.meteo_set || !k.grid_set)) return set_error_msg("f3d_ens_run: class not ready");
   ECK(cudaSetDevice(e->device));
@@ -1211,6 +1253,145 @@ extern "C" int f3d_ens_run(f3d_ens* e, int nsteps) {
     ECK(cudaGraphLaunch(g, e->st));
     e->launches += kernels_per_step(e);
     e->iiter += 1;
+  }
+  return 0;
+}
+
+// Boundary halo layers of every member (as f3d_ads_keep_boundary_halo): the
+// sweeps keep the free-flow ghost values they compute, the decay decays them,
+// and the output reductions and downloads use them instead of zero.
+extern "C" int f3d_ens_keep_boundary_halo(f3d_ens* e, int on) {
+  if (!e) return set_error_msg("f3d_ens_keep_boundary_halo: null ensemble");
+  ECK(cudaSetDevice(e->device));
+  for (int mi = 0; mi < e->nm; ++mi) {
+    MemberDev& d = e->hm[mi];
+    if (!on) {  // the buffers stay with the ensemble until it is destroyed
+      d.gh64 = nullptr;
+      d.gh32 = nullptr;
+      continue;
+    }
+    const size_t n = (size_t)gh_per_bin(d.nx, d.ny, d.nz) * e->nb;
+    if (e->prec == F3D_PREC_FP64) {
+      if (!d.gh64 && ealloc(e, &d.gh64, n)) return 1;
+      ECK(cudaMemset(d.gh64, 0, n * 8));
+    } else {
+      if (!d.gh32 && ealloc(e, &d.gh32, n)) return 1;
+      ECK(cudaMemset(d.gh32, 0, n * 4));
+    }
+  }
+  drop_graphs(e);
+  return upload_members(e);
+}
+
+// ---- gravity current per member: F3D_add_radial_wind (mod_F3D.F90:978-1226) --
+namespace {
+bool ens_gc_args(const f3d_ens* e, int mi, double time, GcArgs* g, double st[7]) {
+  const std::vector<double>& p = e->gc_p[mi];
+  if (p.empty()) {
+    memset(g, 0, sizeof(*g));
+    for (int q = 0; q < 7; ++q) st[q] = 0.0;
+    return false;
+  }
+  const EnsClass& k = e->cls[e->member_class[mi]];
+  const double* lon_c = k.gc_host.data();
+  const double* lat_c = lon_c + (k.nx + 1);
+  const double* hm1_c = lat_c + (k.ny + 1) + k.nx + k.ny;
+  if (!gc_scalars(p.data(), lon_c, lat_c, hm1_c, time, g, st)) return false;
+  g->lon_c = k.gc_xy;
+  g->lat_c = g->lon_c + (k.nx + 1);
+  g->lon_p = g->lat_c + (k.ny + 1);
+  g->lat_p = g->lon_p + k.nx;
+  g->hm1_c = g->lat_p + k.ny;
+  g->hm1_p = e->hm[mi].hm1;
+  g->zc = k.zc;
+  return true;
+}
+}  // namespace
+
+extern "C" int f3d_ens_set_member_gravity_current(f3d_ens* e, int mi, const double params[11],
+                                                  const double* lon_c, const double* lat_c,
+                                                  const double* lon_p, const double* lat_p,
+                                                  const double* Hm1_c) {
+  if (!e || mi < 0 || mi >= e->nm) return set_error_msg("f3d_ens_set_member_gravity_current: bad member");
+  ECK(cudaSetDevice(e->device));
+  if (e->gc_p.empty()) e->gc_p.resize(e->nm);
+  if (!params) {  // switch the member's current off
+    e->gc_p[mi].clear();
+    e->gc_any = false;
+    for (const auto& p : e->gc_p) e->gc_any = e->gc_any || !p.empty();
+    if (e->hm[mi].gc_cur) {
+      e->hm[mi].gc_cur = 0;
+      if (upload_members(e)) return 1;
+    }
+    return 0;
+  }
+  EnsClass& k = e->cls[e->member_class[mi]];
+  if (!k.grid_set) return set_error_msg("f3d_ens_set_member_gravity_current: class grid not set");
+  if (!k.zc)
+    return set_error_msg("f3d_ens_set_member_gravity_current: corner heights not set "
+                         "(f3d_ens_set_class_corner_heights)");
+  const size_t n = (size_t)(k.nx + 1) + (k.ny + 1) + k.nx + k.ny + (k.ny + 1);
+  if (lon_c || lat_c || lon_p || lat_p || Hm1_c) {
+    if (!lon_c || !lat_c || !lon_p || !lat_p || !Hm1_c)
+      return set_error_msg("f3d_ens_set_member_gravity_current: give all five coordinate arrays");
+    k.gc_host.resize(n);
+    double* h = k.gc_host.data();
+    const size_t o_lat_c = k.nx + 1, o_lon_p = o_lat_c + k.ny + 1, o_lat_p = o_lon_p + k.nx,
+                 o_hm1_c = o_lat_p + k.ny;
+    memcpy(h, lon_c, (k.nx + 1) * 8);
+    memcpy(h + o_lat_c, lat_c, (k.ny + 1) * 8);
+    memcpy(h + o_lon_p, lon_p, k.nx * 8);
+    memcpy(h + o_lat_p, lat_p, k.ny * 8);
+    memcpy(h + o_hm1_c, Hm1_c, (k.ny + 1) * 8);
+    if (!k.gc_xy && ealloc(e, &k.gc_xy, n)) return 1;
+    ECK(cudaMemcpy(k.gc_xy, h, n * 8, cudaMemcpyHostToDevice));
+  } else if (k.gc_host.size() != n) {
+    return set_error_msg("f3d_ens_set_member_gravity_current: the class's coordinates not given");
+  }
+  MemberDev& m = e->hm[mi];
+  if (e->prec == F3D_PREC_FP32 && !m.gc4[0]) {  // this step's x and y face records
+    if (ealloc(e, &m.gc4[0], (size_t)(k.nx + 1) * k.ny * k.nz) ||
+        ealloc(e, &m.gc4[1], (size_t)(k.ny + 1) * k.nx * k.nz))
+      return 1;
+    if (upload_members(e)) return 1;
+  }
+  e->gc_p[mi].assign(params, params + 11);
+  e->gc_any = true;
+  return 0;
+}
+
+extern "C" int f3d_ens_gravity_current_time_steps(f3d_ens* e, const double* times,
+                                                  const double* stimes, int criterion, double cfl,
+                                                  double run_end, int* active, double* dts) {
+  if (!e || !times || !stimes || !active || !dts)
+    return set_error_msg("f3d_ens_gravity_current_time_steps: null argument");
+  if (criterion != 1 && criterion != 2)
+    return set_error_msg("f3d_ens_gravity_current_time_steps: criterion %d not in 1..2", criterion);
+  ECK(cudaSetDevice(e->device));
+  std::vector<GcArgs> gs(e->nm);
+  for (int m = 0; m < e->nm; ++m) {
+    double st[7];
+    active[m] = ens_gc_args(e, m, times[m], &gs[m], st) ? 1 : 0;
+  }
+  bool any = false;
+  for (int m = 0; m < e->nm; ++m) {
+    if (!active[m]) continue;
+    any = true;
+    ECK(cudaMemsetAsync(e->d_red + 3 * (size_t)m, 0, 3 * sizeof(double), e->st));
+    launch_cfl(e->dm, m, stimes[m], criterion, e->d_red + 3 * (size_t)m, e->st, &gs[m]);
+  }
+  if (!any) return 0;
+  ECKL();
+  ECK(cudaMemcpyAsync(e->h_pin, e->d_red, 3 * (size_t)e->nm * sizeof(double), cudaMemcpyDeviceToHost,
+                      e->st));
+  ECK(cudaStreamSynchronize(e->st));
+  for (int m = 0; m < e->nm; ++m) {
+    if (!active[m]) continue;
+    const double* r = e->h_pin + 3 * (size_t)m;
+    double x = std::max(std::max(r[0], r[1]), r[2]);  // mod_Grid.F90:1125-1127
+    if (x > 0.0) x = 1.0 / x;
+    x = cfl * x;
+    dts[m] = std::min(x, run_end);
   }
   return 0;
 }
@@ -1325,10 +1506,25 @@ extern "C" int f3d_ens_step(f3d_ens* e, const double* dt, const double* time, in
     if (k.rep >= 0 && (!k.meteo_set || !k.grid_set)) return set_error_msg("f3d_ens_step: class not ready");
   ECK(cudaSetDevice(e->device));
   if (update_radio_factors(e, dt)) return 1;
+  std::vector<std::pair<int, GcArgs>> gcl;
+  if (e->gc_any) {  // the members whose current acts at their time
+    bool changed = false;
+    for (int m = 0; m < e->nm; ++m) {
+      GcArgs g;
+      double st[7];
+      const bool on = ens_gc_args(e, m, time[m], &g, st);
+      if (on) gcl.emplace_back(m, g);
+      if (e->prec == F3D_PREC_FP32 && e->hm[m].gc_cur != (on ? 1 : 0)) {
+        e->hm[m].gc_cur = on ? 1 : 0;  // the precision form's x/y sweeps read gc4
+        changed = true;
+      }
+    }
+    if (changed && upload_members(e)) return 1;
+  }
   launch_set_steps(e->dm, e->nm, dt, time, iiter, e->st);
   e->launches += (e->nm + 63) / 64;
   ECKL();
-  if (enqueue_step(e, iiter % 2 == 0, false)) return 1;
+  if (enqueue_step(e, iiter % 2 == 0, false, nullptr, &gcl)) return 1;
   e->iiter = iiter + 1;
   if (fluxes) {
     ECK(cudaMemcpyAsync(e->h_pin, e->flux_step, 6 * (size_t)e->nm * 8, cudaMemcpyDeviceToHost, e->st));
@@ -1378,6 +1574,9 @@ extern "C" int f3d_ens_reset_state(f3d_ens* e) {
     const size_t ncell = (size_t)d.nx * d.ny * d.nz, nb = (size_t)e->nb;
     if (d.c32) ECK(cudaMemsetAsync(d.c32, 0, ncell * nb * 4, e->st));
     if (d.c32lo) ECK(cudaMemsetAsync(d.c32lo, 0, ncell * nb * 4, e->st));
+    const size_t ngh = (size_t)gh_per_bin(d.nx, d.ny, d.nz) * nb;
+    if (d.gh64) ECK(cudaMemsetAsync(d.gh64, 0, ngh * 8, e->st));
+    if (d.gh32) ECK(cudaMemsetAsync(d.gh32, 0, ngh * 4, e->st));
     if (d.c64) ECK(cudaMemsetAsync(d.c64, 0, ncell * nb * 8, e->st));
     ECK(cudaMemsetAsync(d.acum, 0, (size_t)d.nx * d.ny * nb * 8, e->st));
   }
@@ -1537,6 +1736,8 @@ extern "C" int f3d_ens_output_member_species(f3d_ens* e, int mi, const int* bin_
   a.hm2 = d.hm2;
   a.hm3 = d.hm3;
   a.zc = k.zc;
+  a.gh64 = d.gh64;
+  a.gh32 = d.gh32;
   if (con_sur || col_mass || cloud_top) {
     const size_t ncs = (size_t)__builtin_popcountll(a.mask) * k.nx * k.ny * k.nz;
     const size_t need = ncs + (size_t)(k.nz + 1) * ncol;

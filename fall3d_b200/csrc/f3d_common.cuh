@@ -157,10 +157,12 @@ struct WorkItem {
 // 1990).  Numerators below 2^-800 are first scaled by 2^400 (exact) so no
 // intermediate is subnormal, and zero numerators return the correctly
 // signed zero a*y.  For |b| in [2^-100, 2^100] this is IEEE round-to-nearest
-// a/b whenever the quotient is a normal number; a quotient in the subnormal
-// range (|q| < 2^-1022, only from numerators below 2^-900) would be rounded a
-// second time by the scaling back, so there the IEEE division a/b itself is
-// taken (a branch that only the far fringe of a plume ever reaches).
+// a/b.  A quotient in the subnormal range (numerators below ~2^-900 only, the
+// far fringe of a plume) is rounded a second time by the scaling back; that
+// double rounding differs from a single one only when the scaled quotient q
+// lies exactly halfway between two subnormals, and then the exact remainder
+// sa - q b (one FMA) tells on which side the true quotient lies, so the tie
+// is resolved by one subnormal ulp.  No division and no call on any path.
 __device__ __forceinline__ double div_rn_recip(double a, double b, double y) {
   const bool tiny = fabs(a) < 0x1p-800;
   const double sa = tiny ? a * 0x1p400 : a;
@@ -169,11 +171,17 @@ __device__ __forceinline__ double div_rn_recip(double a, double b, double y) {
   q = fma(r, y, q);
   r = fma(-q, b, sa);
   q = fma(r, y, q);
-  if (tiny) {
-    if (fabs(q) < 0x1p-622) q = a / b;
-    else q = q * 0x1p-400;
+  double res = tiny ? q * 0x1p-400 : q;
+#ifndef F3D_DIV_TIE
+#define F3D_DIV_TIE 1
+#endif
+  if (F3D_DIV_TIE && tiny) {
+    const double rem = fma(-q, b, sa);     // exact: the true quotient is q + rem / b
+    const double d = q - res * 0x1p400;    // exact: q's distance from the rounded result
+    if (fabs(d) == 0x1p-675 && rem != 0.0 && ((d > 0.0) == ((rem > 0.0) == (b > 0.0))))
+      res = res + copysign(0x1p-1074, d);  // a tie the true quotient lies beyond
   }
-  return (a == 0.0) ? a * y : q;
+  return (a == 0.0) ? a * y : res;
 }
 
 }  // namespace f3d

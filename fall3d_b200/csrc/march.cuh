@@ -52,9 +52,9 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // is complete at t = (m+1)W + 7 and chunk m+1's first write comes at
 // t = (m+1)W + 8, the block that flushes chunk m before writing.  The
 // smaller tile lets more blocks share an SM.
-template <class T, int NOUT = 2>
+template <class T, int NOUT = 2, int W_ = 128 / (int)sizeof(T)>
 struct XTile {
-  static constexpr int W = 128 / (int)sizeof(T);  // positions per chunk
+  static constexpr int W = W_;                    // positions per chunk (a multiple of 8)
   static constexpr int LDW = W + 1;               // padded row pitch
   static constexpr int RPI = 32 / W;              // rows per warp instruction
   static constexpr int BYTES = (2 + NOUT) * 32 * LDW * (int)sizeof(T) + 32 * 8;
@@ -149,6 +149,89 @@ struct XTile {
   }
 };
 
+// Per-warp staging of the low part of the compensated state along x pencils:
+// the cells are finalised in place in a two-buffer tile.  With the RK4 march
+// the low part of cell p is read at t = p + 7 and written at t = p + 8, so
+// chunk m (positions mW .. mW + W - 1) is complete after block T0 = (m+1)W,
+// which flushes it and issues the copy of chunk m + 2 into the same buffer;
+// that chunk is first read by block T0 = (m+2)W, which waits for it.  The
+// rows are those of the state's staging (XTile::rows) shifted by `delta`
+// elements (the low part's offset from the state).
+template <int W>
+struct XLoTile {
+  static constexpr int LDW = W + 1;
+  static constexpr int BYTES = 2 * 32 * LDW * 4;
+  float* buf;            // [2][32][LDW]
+  float* const* rows;    // the state's row base pointers
+  long long delta;
+  int lane, n, next_flush;
+
+  __device__ __forceinline__ void setup(void* base, float* const* rows_, long long delta_, int lane_,
+                                        int n_) {
+    buf = reinterpret_cast<float*>(base);
+    rows = rows_;
+    delta = delta_;
+    lane = lane_;
+    n = n_;
+    next_flush = 0;
+  }
+  __device__ __forceinline__ void load_chunk(int m) {
+    const int p0 = m * W, sub = lane / W, col = lane % W;
+    float* dst = buf + (m & 1) * 32 * LDW;
+    const float* any = nullptr;
+    for (int r = 0; r < 32 && !any; ++r)
+      if (rows[r]) any = rows[r] + delta;
+    if (!any) return;
+#pragma unroll 8
+    for (int r0 = 0; r0 < 32; r0 += 32 / W) {
+      const int r = r0 + sub, p = p0 + col;
+      const float* rp = rows[r];
+      const bool ok = rp && p < n;
+      cp_async_elem(dst + r * LDW + col, ok ? rp + delta + p : any, ok ? 4 : 0);
+    }
+    cp_async_commit();
+  }
+  __device__ __forceinline__ void flush_chunk(int m) {
+    const int p0 = m * W, sub = lane / W, col = lane % W;
+    const float* src = buf + (m & 1) * 32 * LDW;
+#pragma unroll 8
+    for (int r0 = 0; r0 < 32; r0 += 32 / W) {
+      const int r = r0 + sub, p = p0 + col;
+      float* rp = rows[r];
+      if (rp && p < n) rp[delta + p] = src[r * LDW + col];
+    }
+  }
+  __device__ __forceinline__ float& at(int p) {
+    return buf[((p / W) & 1) * 32 * LDW + lane * LDW + (p % W)];
+  }
+  __device__ __forceinline__ void init() {
+    load_chunk(0);
+    if (W < n) load_chunk(1);
+    cp_async_wait_all();
+    __syncwarp();
+  }
+  __device__ __forceinline__ void block_begin(int T0) {
+    if (T0 >= 2 * W && T0 % W == 0) {  // chunk T0/W, issued after block T0 - W
+      cp_async_wait_all();
+      __syncwarp();
+    }
+  }
+  __device__ __forceinline__ void block_end(int T0) {
+    if (T0 >= W && T0 % W == 0) {
+      __syncwarp();
+      flush_chunk(T0 / W - 1);
+      next_flush = T0 / W;
+      __syncwarp();
+      if ((T0 / W + 1) * W < n) load_chunk(T0 / W + 1);
+    }
+  }
+  __device__ __forceinline__ void finish() {
+    cp_async_wait_all();
+    __syncwarp();
+    for (int m = next_flush; m * W < n; ++m) flush_chunk(m);
+  }
+};
+
 // Default (no staging) hooks for y and z pencils.
 struct NoStage {
   __device__ __forceinline__ void init() {}
@@ -197,6 +280,8 @@ struct March {
   T ch[8];           // c(p) at ch[p & 7]
   T nh[8];           // new_c(p) at nh[p & 7] (not used by CMP)
   T hf[8];           // CMP: H(f) at hf[f & 7]
+  T lo_next;         // CMP, RK4: the low part of the next cell to finalise,
+                     // loaded one step ahead of its use
   FaceV<T> fw[8];    // face(f) at fw[f & 7]
   StageS<T> S1, S2, S3, S4;
   T gL, gR, uR, cn1, cn2, cn3, cn4;
@@ -211,6 +296,11 @@ struct March {
                   m5 = (U + 3) & 7, m6 = (U + 2) & 7, m7 = (U + 1) & 7;
     T k1 = T(0), k2 = T(0), k3 = T(0), k4 = T(0), ff = T(0);
     const T c_fin = ch[U];  // CMP: c(t-8), finalised at the end of this step
+    T lo_fin = T(0);
+    if constexpr (CMP && TM == 2) {  // its low part, and the next one's load
+      lo_fin = lo_next;
+      lo_next = o.lo_fetch(min(max(t - 7, 0), n - 1));
+    }
     // ---- stage 1: arrival at q = t
     // c(p) is loaded at t = p - 4 and face(f) at t = f - 1 (a four-slot and
     // a one-slot queue in front of the rings), so their latency is hidden
@@ -241,7 +331,8 @@ struct March {
     }
     if constexpr (TM == 1) {
       if (!G || (t >= 2 && t <= n + 1)) {
-        if constexpr (CMP) o.store_c(t - 2, o.final_cmp(ch[m2], hf[m2], hf[m1], t - 2));
+        if constexpr (CMP)
+          o.store_c(t - 2, o.final_cmp(ch[m2], o.lo_fetch(t - 2), hf[m2], hf[m1], t - 2));
         else o.store_c(t - 2, o.euler(ch[m2], k1));
       }
       if (G && t == 1) flux_lo = ff;
@@ -292,7 +383,7 @@ struct March {
         o.template arrive<G>(S4, q, a, fw[m7], q - 2, k4, ff);
         if constexpr (CMP) {
           hf[m7] = hf[m7] + S4.F1;
-          if (!G || (q >= 2)) o.store_c(q - 2, o.final_cmp(c_fin, hf[U], hf[m7], q - 2));
+          if (!G || (q >= 2)) o.store_c(q - 2, o.final_cmp(c_fin, lo_fin, hf[U], hf[m7], q - 2));
         } else {
           if (!G || (q >= 2)) o.store_c(q - 2, o.rk_final(nh[U], k4));
         }
@@ -311,6 +402,11 @@ struct March {
                   m5 = (U + 3) & 7, m6 = (U + 2) & 7, m7 = (U + 1) & 7;
     T k1, k2, k3, k4, ff;
     const T c_fin = ch[U];  // CMP: c(t-8), finalised at the end of this step
+    T lo_fin = T(0);
+    if constexpr (CMP) {  // its low part, and the next one's load
+      lo_fin = lo_next;
+      lo_next = o.lo_fetch(min(max(t - 7, 0), n - 1));
+    }
     {  // stage 1: q = t; c(p) enters the queue at t = p - 4 (positions past
        // the end loaded by a steady block hold c(n-1): arrive as gR)
       const T a = (t < n) ? cn1 : gR;
@@ -345,7 +441,7 @@ struct March {
       o.template arrive<false>(S4, q, a, fw[m7], q - 2, k4, ff);
       if constexpr (CMP) {
         hf[m7] = hf[m7] + S4.F1;
-        if (q - 2 >= 0 && q - 2 < n) o.store_c(q - 2, o.final_cmp(c_fin, hf[U], hf[m7], q - 2));
+        if (q - 2 >= 0 && q - 2 < n) o.store_c(q - 2, o.final_cmp(c_fin, lo_fin, hf[U], hf[m7], q - 2));
       } else {
         if (q - 2 >= 0 && q - 2 < n) o.store_c(q - 2, o.rk_final(nh[U], k4));
       }
@@ -438,6 +534,7 @@ struct March {
     iter_head<5>();
     iter_head<6>();
     iter_head<7>();
+    if constexpr (CMP) lo_next = o.lo_fetch(0);  // cell 0 is finalised at t = 8
     o.stage_end(0);
 #pragma unroll 1
     for (int T0 = 8; T0 <= t_last; T0 += 8) {

@@ -4,7 +4,10 @@
 // them, and handed to the kernels of deposit_dev.cu.
 #pragma once
 #include <cmath>
+#include <cstring>
 #include <vector>
+
+#include "phys_dev.cuh"
 
 namespace f3d {
 
@@ -100,6 +103,119 @@ inline double mass_sink_sum(int nx, int ny, const double* col) {
   for (int j = 0; j < ny; ++j)
     for (int i = 0; i < nx; ++i) my_mass = my_mass + col[i + (size_t)nx * j];
   return 0.0 + my_mass;
+}
+
+// Scalars of the gravity current, F3D_add_radial_wind (mod_F3D.F90:978-1226),
+// at `time`, with the host C library's sqrt and pow (:1026-1070).  p holds
+// {lon, lat, start_time, end_time, c_flow_rate, k_entrain, brunt_vaisala,
+// lambda_grav, mass_flow_rate, h_tot, input_min_radius}; lon_c, lat_c and
+// hm1_c are the first two corner coordinates and scale factor of the grid.
+// Returns false where the routine returns early (outside [start_time,
+// end_time] or no mass flow).  st = {vol_flow_rate, min_radius,
+// radius_grav, c_grav_factor, th_grav, hmin, hmax}; g receives the scalars
+// (the caller sets its device pointers).
+inline bool gc_scalars(const double p[11], const double* lon_c, const double* lat_c,
+                       const double* hm1_c, double time, GcArgs* g, double st[7]) {
+  const double PI = 4.0 * std::atan(1.0), REARTH = 6356000.0;  // mod_KindType.F90:43-44
+  std::memset(g, 0, sizeof(*g));
+  for (int q = 0; q < 7; ++q) st[q] = 0.0;
+  if (time < p[2] || time > p[3] || p[8] <= 0.0) return false;
+  double deltax = REARTH * hm1_c[0] * (lon_c[0] - lon_c[1]) * PI / 180.0;
+  double deltay = REARTH * (lat_c[0] - lat_c[1]) * PI / 180.0;
+  double radius = 1.5 * std::sqrt(deltax * deltax + deltay * deltay);
+  double min_radius = radius;  // parallel_max over one rank
+  if (p[10] > 0.0) min_radius = p[10];
+  const double c_flow_rate = p[4], k_entrain = p[5], brunt_vaisala = p[6], lambda_grav = p[7],
+               mass_flow_rate = p[8], h_tot = p[9];
+  const double tse = time - p[2];
+  const double vol_flow_rate = c_flow_rate * std::sqrt(k_entrain) * std::pow(mass_flow_rate, 0.75) /
+                               std::pow(brunt_vaisala, 1.25);
+  const double c_gravr = 3.0 * lambda_grav * brunt_vaisala * vol_flow_rate / (2.0 * PI);
+  double radius_grav = std::pow(c_gravr * (tse * tse), 0.33333);
+  radius_grav = std::fmax(radius_grav, min_radius);
+  const double c_gravu = std::sqrt(2.0 * lambda_grav * brunt_vaisala * vol_flow_rate / (3.0 * PI));
+  const double c_grav_factor = 0.75 * c_gravu * std::sqrt(radius_grav);
+  const double th_grav = c_gravu / (std::sqrt(radius_grav) * lambda_grav * brunt_vaisala);
+  const double h_umbr = h_tot / 1.2;
+  const double hmin = std::fmax(h_umbr - 0.5 * th_grav, 0.5 * h_tot);
+  const double hmax = std::fmin(h_umbr + 0.5 * th_grav, h_tot);
+  g->on = 1;
+  g->xc = p[0];
+  g->yc = p[1];
+  g->rearth = REARTH;
+  g->pi = PI;
+  g->min_radius = min_radius;
+  g->radius_grav = radius_grav;
+  g->c_grav_factor = c_grav_factor;
+  g->hmin = hmin;
+  g->hmax = hmax;
+  st[0] = vol_flow_rate;
+  st[1] = min_radius;
+  st[2] = radius_grav;
+  st[3] = c_grav_factor;
+  st[4] = th_grav;
+  st[5] = hmin;
+  st[6] = hmax;
+  return true;
+}
+
+// Boundary halo layers <-> the reference's halo-inclusive state arrays
+// my_c(ips-2:ipe+2, jps-2:jpe+2, kps-2:kpe+2, nbins): the first halo cell at
+// both ends of every pencil (both halo layers hold it after a sweep,
+// mod_ADS.F90:1246,1258,...), in the gh_offset layout (f3d_common.cuh).
+inline void gh_gather_ref(int nx_, int ny_, int nz_, int nb_, const double* my_c,
+                          std::vector<double>& g) {
+  const long long nx = nx_, ny = ny_, nz = nz_, nb = nb_;
+  const long long X = nx + 4, Y = ny + 4, Z = nz + 4, per = gh_per_bin(nx_, ny_, nz_);
+  g.assign((size_t)(per * nb), 0.0);
+  auto at = [&](long long i, long long j, long long k, long long b) {
+    return my_c[(i + 2) + X * ((j + 2) + Y * ((k + 2) + Z * b))];
+  };
+  for (long long b = 0; b < nb; ++b) {
+    double* gb = g.data() + b * per;
+    for (long long k = 0; k < nz; ++k)
+      for (long long j = 0; j < ny; ++j) {
+        gb[gh_offset(0, 0, k * ny + j, nx_, ny_, nz_)] = at(-1, j, k, b);
+        gb[gh_offset(0, 1, k * ny + j, nx_, ny_, nz_)] = at(nx, j, k, b);
+      }
+    for (long long k = 0; k < nz; ++k)
+      for (long long i = 0; i < nx; ++i) {
+        gb[gh_offset(1, 0, k * nx + i, nx_, ny_, nz_)] = at(i, -1, k, b);
+        gb[gh_offset(1, 1, k * nx + i, nx_, ny_, nz_)] = at(i, ny, k, b);
+      }
+    for (long long j = 0; j < ny; ++j)
+      for (long long i = 0; i < nx; ++i) {
+        gb[gh_offset(2, 0, j * nx + i, nx_, ny_, nz_)] = at(i, j, -1, b);
+        gb[gh_offset(2, 1, j * nx + i, nx_, ny_, nz_)] = at(i, j, nz, b);
+      }
+  }
+}
+
+inline void gh_scatter_ref(int nx_, int ny_, int nz_, int nb_, const std::vector<double>& g,
+                           double* my_c) {
+  const long long nx = nx_, ny = ny_, nz = nz_, nb = nb_;
+  const long long X = nx + 4, Y = ny + 4, Z = nz + 4, per = gh_per_bin(nx_, ny_, nz_);
+  auto at = [&](long long i, long long j, long long k, long long b) -> double& {
+    return my_c[(i + 2) + X * ((j + 2) + Y * ((k + 2) + Z * b))];
+  };
+  for (long long b = 0; b < nb; ++b) {
+    const double* gb = g.data() + b * per;
+    for (long long k = 0; k < nz; ++k)
+      for (long long j = 0; j < ny; ++j) {
+        at(-1, j, k, b) = at(-2, j, k, b) = gb[gh_offset(0, 0, k * ny + j, nx_, ny_, nz_)];
+        at(nx, j, k, b) = at(nx + 1, j, k, b) = gb[gh_offset(0, 1, k * ny + j, nx_, ny_, nz_)];
+      }
+    for (long long k = 0; k < nz; ++k)
+      for (long long i = 0; i < nx; ++i) {
+        at(i, -1, k, b) = at(i, -2, k, b) = gb[gh_offset(1, 0, k * nx + i, nx_, ny_, nz_)];
+        at(i, ny, k, b) = at(i, ny + 1, k, b) = gb[gh_offset(1, 1, k * nx + i, nx_, ny_, nz_)];
+      }
+    for (long long j = 0; j < ny; ++j)
+      for (long long i = 0; i < nx; ++i) {
+        at(i, j, -1, b) = at(i, j, -2, b) = gb[gh_offset(2, 0, j * nx + i, nx_, ny_, nz_)];
+        at(i, j, nz, b) = at(i, j, nz + 1, b) = gb[gh_offset(2, 1, j * nx + i, nx_, ny_, nz_)];
+      }
+  }
 }
 
 }  // namespace f3d

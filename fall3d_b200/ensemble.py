@@ -63,6 +63,7 @@ class Ensemble:
               "f3d_ens_create")
         self._h = h
         self.precision = precision
+        self.tuning = (MODE_KERNELS, 4, 0)  # the library's initial execution shape
         self._keep = []
         for ci, g in enumerate(self.grids):
             arrs = [np.ascontiguousarray(getattr(g, n), dtype=np.float64) for n in
@@ -233,14 +234,48 @@ class Ensemble:
         check(lib().f3d_ens_get_member_awet(self._h, int(m), _p(out)), "f3d_ens_get_member_awet")
         return out
 
+    def keep_boundary_halo(self, on=True):
+        """Keep every member's boundary halo layers (f3d_ens_keep_boundary_halo)."""
+        check(lib().f3d_ens_keep_boundary_halo(self._h, int(bool(on))), "f3d_ens_keep_boundary_halo")
+
+    def _ensure_corner_heights(self, ci):
+        if ci not in getattr(self, "_zc_set", set()):
+            g = self.grids[ci]
+            check(lib().f3d_ens_set_class_corner_heights(self._h, ci, _p(np.asfortranarray(g.z_c, np.float64))),
+                  "f3d_ens_set_class_corner_heights")
+            self._zc_set = getattr(self, "_zc_set", set()) | {ci}
+
+    def set_member_gravity_current(self, m, lon, lat, start_time, end_time, c_flow_rate, k_entrain,
+                                   brunt_vaisala, lambda_grav, mass_flow_rate, h_tot, input_min_radius=0.0):
+        """F3D_add_radial_wind (mod_F3D.F90:978-1226) for member m; the
+        ensemble then advances with step() (host-driven) only."""
+        ci = self.member_classes[m]
+        g = self.grids[ci]
+        self._ensure_corner_heights(ci)
+        p = np.array([lon, lat, start_time, end_time, c_flow_rate, k_entrain, brunt_vaisala, lambda_grav,
+                      mass_flow_rate, h_tot, input_min_radius], dtype=np.float64)
+        xy = [np.ascontiguousarray(getattr(g, n), dtype=np.float64) for n in
+              ("lon_c", "lat_c", "lon_p", "lat_p", "Hm1_c")]
+        check(lib().f3d_ens_set_member_gravity_current(self._h, int(m), _p(p), *[_p(a) for a in xy]),
+              "f3d_ens_set_member_gravity_current")
+
+    def gravity_current_time_steps(self, times, stimes, dts, criterion=2, cfl=0.9, run_end=1e30):
+        """update_step time steps (mod_F3D.F90:1446-1452) of the members whose
+        current acts at times[m]; returns (active mask, dts with those set)."""
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        s = np.ascontiguousarray(stimes, dtype=np.float64)
+        d = np.array(dts, dtype=np.float64)
+        act = np.zeros(self.nm, np.int32)
+        check(lib().f3d_ens_gravity_current_time_steps(self._h, _p(t), _p(s), int(criterion), float(cfl),
+                                                       float(run_end), _ip(act), _p(d)),
+              "f3d_ens_gravity_current_time_steps")
+        return act.astype(bool), d
+
     def output_member_species(self, m, bins, col_du=False):
         """nc_IO_out_res's per-species fields of member m at the corners."""
         ci = self.member_classes[m]
         g = self.grids[ci]
-        if ci not in getattr(self, "_zc_set", set()):
-            check(lib().f3d_ens_set_class_corner_heights(self._h, ci, _p(np.asfortranarray(g.z_c, np.float64))),
-                  "f3d_ens_set_class_corner_heights")
-            self._zc_set = getattr(self, "_zc_set", set()) | {ci}
+        self._ensure_corner_heights(ci)
         sel = np.zeros(self.nbins, np.int32)
         sel[list(bins)] = 1
         keys = ("con_sur", "col_mass", "cloud_top", "grn_load")

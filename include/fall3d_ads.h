@@ -531,6 +531,33 @@ int f3d_ens_launch_count(f3d_ens *ens, long long *count);
  * counterpart in the reference, which has no device waits; it stands for
  * MY_ERR%flag = 1 (mod_KindType.F90:85-95). */
 int f3d_ens_status(f3d_ens *ens, int *device_error);
+/* Boundary halo layers of every member, as f3d_ads_keep_boundary_halo: the
+ * free-flow ghost values of the sweeps are kept (and decayed), the output
+ * reductions read them at the edge corners, and member up/downloads carry
+ * them in the halo cells of my_c.  on = 0 stops keeping them. */
+int f3d_ens_keep_boundary_halo(f3d_ens *ens, int on);
+/* Gravity current of member mi (F3D_add_radial_wind, mod_F3D.F90:978-1226),
+ * as f3d_ads_set_gravity_current for a single domain: params[11] = {lon,
+ * lat, start_time, end_time, c_flow_rate, k_entrain, brunt_vaisala,
+ * lambda_grav, mass_flow_rate, h_tot, input_min_radius}; the five
+ * coordinate arrays of the member's class grid are needed on the first call
+ * of a class (may be NULL afterwards); the class's corner heights must be set
+ * (f3d_ens_set_class_corner_heights).  params NULL switches the member's
+ * current off.  While any member has a current the ensemble advances with
+ * host-driven steps only (f3d_ens_step; f3d_ens_run refuses): every step
+ * inside the member's window adds the radial wind to its interpolated winds
+ * (mod_F3D.F90:1443-1445). */
+int f3d_ens_set_member_gravity_current(f3d_ens *ens, int mi, const double params[11],
+                                       const double *lon_c, const double *lat_c,
+                                       const double *lon_p, const double *lat_p,
+                                       const double *Hm1_c);
+/* The update_step time step of every member whose current acts at times[m]
+ * (mod_F3D.F90:1446-1452): grid_get_time_step on its winds with the radial
+ * wind at interpolation factor stimes[m]; active[m] = 1 and dts[m] set for
+ * those members, active[m] = 0 and dts[m] untouched for the others. */
+int f3d_ens_gravity_current_time_steps(f3d_ens *ens, const double *times, const double *stimes,
+                                       int criterion, double cfl, double run_end, int *active,
+                                       double *dts);
 /* Autotuner of the batched step (no counterpart in the reference, whose
  * members run as separate jobs).  Times each candidate execution shape on
  * the device -- per-phase kernels replayed from CUDA graphs with 4, 2 or 1

@@ -26,7 +26,7 @@ def _case(n, seed, stretched):
 @pytest.mark.parametrize("limiter", [1, 2, 3])
 def test_solve_1d_bitexact(oracle_mod, built_lib, bc, signs, limiter):
     n = 97
-    seed = 7 + 100 * limiter + 10 * (bc[0] + 2) + (bc[1] + 2) + 1000 * (signs[0] + signs[1])
+    seed = 7 + 100 * limiter + 10 * (bc[0] + 2) + (bc[1] + 2) + 1000 * (signs[0] + 2) + 3000 * (signs[1] + 2)
     c, dxp, dxb, u, k = _case(n, seed, stretched=limiter != 2)
     u[1] = signs[0] * abs(u[1])
     u[n + 1] = signs[1] * abs(u[n + 1])
