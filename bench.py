@@ -313,7 +313,7 @@ def time_steps(dom, dt, K, W, device, pg, t0=0.0):
 def run_c2(args, ws, rank, local, pg):
     import torch
     from fall3d_b200 import workloads as W
-    from fall3d_b200.ads import PREC_FP32, PREC_FP64
+    from fall3d_b200.ads import PREC_FP64
     torch.cuda.set_device(local)
     wl = W.random_c2(seed=rank)
     g = wl.grid
@@ -327,14 +327,16 @@ def run_c2(args, ws, rank, local, pg):
     fp64_value = ws * cbs * K / (ms64 / 1e3)
     c64 = dom64.download_state()[0] if rank == 0 else None
     dom64.close()
-    # ---- FP32 precision form (headline on this workload)
-    dom, dt32 = setup_domain(wl, PREC_FP32, local)
+    # ---- the precision form (headline on this workload)
+    prec = PRECISIONS[args.precision]
+    dom, dt32 = setup_domain(wl, prec, local)
     with ClockSampler(local) as clk:
         ms, launches, t_end = time_steps(dom, dt32, K, Wu, local, pg)
     ms = max_over_ranks(pg, ms)
     value = ws * cbs * K / (ms / 1e3)
     out.update(value=value, ms_per_step=ms / K, fp64_value=fp64_value, launches=launches,
                clocks=clk.summary(), fp64_ms_per_step=ms64 / K)
+    out["fp64_roofline"] = fp64_roofline(fp64_value / ws, out["clocks"].get("sm_mhz"))
     if c64 is not None:
         # FP32 form against the FP64 form after the same W+K steps (dt of the
         # FP64 CFL reduction in both)
@@ -355,13 +357,15 @@ def run_c2(args, ws, rank, local, pg):
     dom.set_profiling(False)
     per = {"x": prof[1] / n, "y": prof[2] / n, "z": prof[3] / n}
     dom_k = max(per, key=per.get)
-    byts = sweep_bytes(wl, 4, dom_k)
+    # the compensated form also reads and writes the low part (4 B each)
+    byts = sweep_bytes(wl, 4, dom_k) + (2.0 * 4 * cbs if prec == 2 else 0.0)
     peak, kind = hbm_peak()
     achieved = byts / (per[dom_k] / 1e3) / 1e9
-    out["roofline"] = {"bound": "hbm", "kernel": f"k_sweep32<{ 'xyz'.index(dom_k)},2,2> ({dom_k} sweep)",
+    out["roofline"] = {"bound": "hbm",
+                       "kernel": f"k_sweep32<{'xyz'.index(dom_k)},2,2,{int(prec == 2)}> ({dom_k} sweep)",
                        "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                        "frac": round(achieved / peak, 4), "peak_kind": kind,
-                       "traffic": load_traffic(f"sweep32_{dom_k}", "c2"),
+                       "traffic": load_traffic(f"sweep32{'c' if prec == 2 else ''}_{dom_k}", "c2"),
                        "algorithmic_bytes": byts, "launch_ms": round(per[dom_k], 4),
                        "sweep_ms": {k: round(v, 4) for k, v in per.items()}}
     # ---- e2e through the C ABI with host buffers
@@ -637,7 +641,7 @@ def run_ensemble(args, ws, rank, local, pg):
 # plain FP64 sweeps, from ncu on the 400x300x60x20 case
 # (profiles/k_sweep64_c2.md); FP64 pipe of the B200: 64 operations per clock
 # per SM on 148 SMs.
-FP64_OPS_PER_CELLBIN_STEP = 1015
+FP64_OPS_PER_CELLBIN_STEP = 1066
 
 
 def fp64_roofline(steps_value, sm_mhz):
@@ -718,8 +722,9 @@ def ens_roofline(r, K):
         dk = max(sw, key=sw.get)
         byts = bytes_dir(dk)
         t = sw[dk]
-        name = f"k_sweep32<{'xyz'.index(dk)},2,2> ({dk} sweep of all 64 members)"
-        tkey = f"sweep32_{dk}"
+        cmp = int(r["state_bytes"] == 8)
+        name = f"k_sweep32<{'xyz'.index(dk)},2,2,{cmp}> ({dk} sweep of all 64 members)"
+        tkey = f"sweep32{'c' if cmp else ''}_{dk}"
     achieved = byts / (t / 1e3) / 1e9
     return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": kind,
@@ -954,13 +959,14 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"c2: {g.nx}x{g.ny}x{g.nz} grid, {wl.nbins} bins, FP32 precision "
-                                   "form (FP64 deposit/flux sums), one domain per GPU",
+            "config": {"workload": f"c2: {g.nx}x{g.ny}x{g.nz} grid, {wl.nbins} bins, one domain per GPU",
+                       "form": FORMS[args.precision],
                        "parallelism": f"replicas x{ws}",
                        "l2": f"inputs larger than L2: c is {g.nx*g.ny*g.nz*wl.nbins*4/2**20:.0f} MiB "
                              f"vs {L2_BYTES/2**20:.0f} MiB L2"},
             "fp64_plain_value": res["fp64_value"],
             "fp64_ms_per_step": res["fp64_ms_per_step"],
+            "fp64_roofline": res["fp64_roofline"],
             "speedup_vs_fp64": res["value"] / res["fp64_value"],
             "gpu_launches": res["launches"],
             "clocks": res["clocks"],
