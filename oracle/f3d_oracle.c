@@ -1162,3 +1162,150 @@ int or_build_grid(int nx, int ny, int nz, int map_h, int map_v, double lonmin,
   return 0;
 }
 #undef F1
+
+/* ---- the meteo term of the step (serial domain: my_ibs = 1, my_ibe = nx+1,
+ * my_ips = 1, my_ipe = nx, likewise j and k).  Loops keep the reference's
+ * Fortran indices; each array is addressed by its own lower bound.
+ *
+ *   grid_get_stagered_velocity   mod_Grid.F90:685-752
+ *   grid_get_scaled_velocity     mod_Grid.F90:761-870
+ *   grid_get_scaled_variables    mod_Grid.F90:879-1017, the k1/k2/k3 part
+ *
+ * uc, vc, wc: corner winds (ibs:ibe, jbs:jbe, kbs:kbe), ground level already
+ * zeroed by the caller (mod_F3D.F90:676-683).  Outputs u (ibs-1:ibe+1,
+ * jps:jpe, kps:kpe), v (ips:ipe, jbs-1:jbe+1, kps:kpe), w (ips:ipe, jps:jpe,
+ * kbs-1:kbe+1).  k1 (ips-2:ipe+2, jps:jpe, kps:kpe), k2 (ips:ipe,
+ * jps-2:jpe+2, kps:kpe), k3 (ips:ipe, jps:jpe, kps-2:kpe+2) are scaled in
+ * place.  Grid arrays: Hm1_p (jps:jpe), Hm2_p (jps-2:jpe+2), Hm3_p, dhdx_p,
+ * dhdy_p (ips:ipe, jps:jpe), X3_c (kbs:kbe), X3_p (kps:kpe).  map_v: 0
+ * Cartesian, 1 sigma without decay, 2 sigma with linear decay.  Returns 1
+ * for any other mapping (the reference's 'Mapping not implemented yet' /
+ * 'Incorrect vertical mapping'), 0 otherwise.  The serial domain has no
+ * neighbours, so the domain_swap_* halo exchanges do nothing. */
+int or_meteo_term(int nx, int ny, int nz, int map_v, double X3max, const double *X3_c,
+                  const double *X3_p, const double *Hm1_p, const double *Hm2_p,
+                  const double *Hm3_p, const double *dhdx_p, const double *dhdy_p,
+                  const double *uc, const double *vc, const double *wc, double *u, double *v,
+                  double *w, double *k1, double *k2, double *k3) {
+  const long NBX = nx + 1, NBY = ny + 1;
+#define CRN(a, i, j, k) (a)[((i) - 1) + NBX * (((j) - 1) + NBY * (long)((k) - 1))]
+#define UF(i, j, k) u[(i) + (long)(nx + 3) * (((j) - 1) + (long)ny * ((k) - 1))]
+#define VF(i, j, k) v[((i) - 1) + (long)nx * ((j) + (long)(ny + 3) * ((k) - 1))]
+#define WF(i, j, k) w[((i) - 1) + (long)nx * (((j) - 1) + (long)ny * (k))]
+#define K1(i, j, k) k1[((i) + 1) + (long)(nx + 4) * (((j) - 1) + (long)ny * ((k) - 1))]
+#define K2(i, j, k) k2[((i) - 1) + (long)nx * (((j) + 1) + (long)(ny + 4) * ((k) - 1))]
+#define K3(i, j, k) k3[((i) - 1) + (long)nx * (((j) - 1) + (long)ny * ((k) + 1))]
+#define P2(a, i, j) (a)[((i) - 1) + (long)nx * ((j) - 1)]
+  if (map_v < 0 || map_v > 2) return 1;
+  /* staggered u: faces i = 1..nx+1, one halo each side */
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx + 1; ++i)
+        UF(i, j, k) = 0.25 * (CRN(uc, i, j, k) + CRN(uc, i, j + 1, k) + CRN(uc, i, j, k + 1) +
+                              CRN(uc, i, j + 1, k + 1));
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      UF(0, j, k) = UF(1, j, k);
+      UF(nx + 2, j, k) = UF(nx + 1, j, k);
+    }
+  /* staggered v */
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i)
+      for (int j = 1; j <= ny + 1; ++j)
+        VF(i, j, k) = 0.25 * (CRN(vc, i, j, k) + CRN(vc, i + 1, j, k) + CRN(vc, i, j, k + 1) +
+                              CRN(vc, i + 1, j, k + 1));
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) {
+      VF(i, 0, k) = VF(i, 1, k);
+      VF(i, ny + 2, k) = VF(i, ny + 1, k);
+    }
+  /* staggered w */
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i)
+      for (int k = 1; k <= nz + 1; ++k)
+        WF(i, j, k) = 0.25 * (CRN(wc, i, j, k) + CRN(wc, i + 1, j, k) + CRN(wc, i, j + 1, k) +
+                              CRN(wc, i + 1, j + 1, k));
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i) {
+      WF(i, j, 0) = WF(i, j, 1);
+      WF(i, j, nz + 2) = WF(i, j, nz + 1);
+    }
+  /* scaled u and v */
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const double Hm1 = Hm1_p[j - 1];
+      for (int i = 0; i <= nx + 2; ++i) UF(i, j, k) = UF(i, j, k) / Hm1;
+    }
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 0; j <= ny + 2; ++j) {
+      const double Hm2 = 0.5 * (Hm2_p[j + 1] + Hm2_p[j]); /* Hm2_p(j) + Hm2_p(j-1) */
+      for (int i = 1; i <= nx; ++i) VF(i, j, k) = VF(i, j, k) / Hm2;
+    }
+  /* scaled w: the terrain correction */
+  if (map_v != 0) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double Hm3 = P2(Hm3_p, i, j);
+        for (int k = 1; k <= nz + 1; ++k) {
+          double hx = P2(dhdx_p, i, j), hy = P2(dhdy_p, i, j);
+          if (map_v == 2) {
+            const double hz = 1.0 - X3_c[k - 1] / X3max;
+            hx = hx * hz;
+            hy = hy * hz;
+          }
+          const double uw = 0.25 * (CRN(uc, i, j, k) + CRN(uc, i + 1, j, k) + CRN(uc, i, j + 1, k) +
+                                    CRN(uc, i + 1, j + 1, k));
+          const double vw = 0.25 * (CRN(vc, i, j, k) + CRN(vc, i + 1, j, k) + CRN(vc, i, j + 1, k) +
+                                    CRN(vc, i + 1, j + 1, k));
+          WF(i, j, k) = (WF(i, j, k) - hx * uw - hy * vw) / Hm3;
+        }
+      }
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        WF(i, j, 0) = WF(i, j, 1);
+        WF(i, j, nz + 2) = WF(i, j, nz + 1);
+      }
+  }
+  /* scaled k3 (mass points), then its two halos each side */
+  if (map_v != 0)
+    for (int k = 1; k <= nz; ++k) {
+      const double hz = (map_v == 2) ? 1.0 - X3_p[k - 1] / X3max : 1.0;
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+          const double Hm3 = P2(Hm3_p, i, j);
+          double hx = P2(dhdx_p, i, j), hy = P2(dhdy_p, i, j);
+          if (map_v == 2) {
+            hx = hx * hz;
+            hy = hy * hz;
+          }
+          K3(i, j, k) = (K3(i, j, k) + hx * hx * K1(i, j, k) + hy * hy * K2(i, j, k)) / (Hm3 * Hm3);
+        }
+    }
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i) {
+      K3(i, j, -1) = K3(i, j, 1);
+      K3(i, j, 0) = K3(i, j, 1);
+      K3(i, j, nz + 2) = K3(i, j, nz);
+      K3(i, j, nz + 1) = K3(i, j, nz);
+    }
+  /* scaled k1 and k2 */
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const double Hm1 = Hm1_p[j - 1];
+      for (int i = -1; i <= nx + 2; ++i) K1(i, j, k) = K1(i, j, k) / (Hm1 * Hm1);
+    }
+  for (int k = 1; k <= nz; ++k)
+    for (int j = -1; j <= ny + 2; ++j) {
+      const double Hm2 = Hm2_p[j + 1];
+      for (int i = 1; i <= nx; ++i) K2(i, j, k) = K2(i, j, k) / (Hm2 * Hm2);
+    }
+#undef CRN
+#undef UF
+#undef VF
+#undef WF
+#undef K1
+#undef K2
+#undef K3
+#undef P2
+  return 0;
+}

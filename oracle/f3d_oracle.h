@@ -222,6 +222,11 @@ typedef struct {
 int or_build_grid(int nx, int ny, int nz, int map_h, int map_v, double lonmin,
                   double lonmax, double latmin, double latmax, double X3max,
                   const double *gl_sigma, const double *hc, or_grid_full *g);
+int or_meteo_term(int nx, int ny, int nz, int map_v, double X3max, const double *X3_c,
+                  const double *X3_p, const double *Hm1_p, const double *Hm2_p,
+                  const double *Hm3_p, const double *dhdx_p, const double *dhdy_p,
+                  const double *uc, const double *vc, const double *wc, double *u, double *v,
+                  double *w, double *k1, double *k2, double *k3);
 
 #ifdef __cplusplus
 }

@@ -78,6 +78,8 @@ def lib():
         L.or_wet_deposition.argtypes = [D, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp, dp]
         L.or_radionuclides.argtypes = [D, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int), dp, dp, dp]
         L.or_perturb.restype = C.c_double
+        L.or_meteo_term.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double] + [dp] * 16
+        L.or_meteo_term.restype = C.c_int
         L.or_time_step_uv.argtypes = [D, G, C.c_double, C.c_double, C.c_int, dp, dp, dp, dp, dp, dp,
                                       dp, dp, dp, dp, dp, C.c_int]
         L.or_current_winds.argtypes = [D, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp]
@@ -313,6 +315,30 @@ def build_grid(nx, ny, nz, map_h, map_v, lonmin, lonmax, latmin, latmax, X3max, 
                                _p(sig), _p(hc), C.byref(gf))
     arr["dlon"], arr["dlat"] = gf.dlon, gf.dlat
     return arr, flag
+
+
+def meteo_term(g, uc, vc, wc, k1, k2, k3):
+    """The meteo term in the C restatement: grid_get_stagered_velocity
+    (mod_Grid.F90:685-752), grid_get_scaled_velocity (:761-870) and the
+    k1/k2/k3 part of grid_get_scaled_variables (:879-1017).  uc, vc, wc are
+    one time level's corner winds with the ground level zeroed; k1, k2, k3
+    the unscaled diffusion with their halos.  Returns u (nx+3, ny, nz),
+    v (nx, ny+3, nz), w (nx, ny, nz+3) and the scaled k1, k2, k3 (copies).
+    g supplies the grid metrics (a fall3d_b200.grid.ArakawaCGrid or the
+    arrays of build_grid with nx, ny, nz, map_v, X3max)."""
+    nx, ny, nz = g.nx, g.ny, g.nz
+    f = lambda a: np.asfortranarray(a, dtype=np.float64)  # noqa: E731
+    uc, vc, wc = f(uc), f(vc), f(wc)
+    k1, k2, k3 = (np.array(a, dtype=np.float64, order="F", copy=True) for a in (k1, k2, k3))
+    grid = [f(getattr(g, n)) for n in ("X3_c", "X3_p", "Hm1_p", "Hm2_p", "Hm3_p", "dhdx_p", "dhdy_p")]
+    u = np.zeros((nx + 3, ny, nz), order="F")
+    v = np.zeros((nx, ny + 3, nz), order="F")
+    w = np.zeros((nx, ny, nz + 3), order="F")
+    flag = lib().or_meteo_term(nx, ny, nz, int(g.map_v), float(g.X3max), *[_p(a) for a in grid],
+                               _p(uc), _p(vc), _p(wc), _p(u), _p(v), _p(w), _p(k1), _p(k2), _p(k3))
+    if flag:
+        raise ValueError("Mapping not implemented yet")
+    return u, v, w, k1, k2, k3
 
 
 def perturb(var_id, ptype, var, random, range_):

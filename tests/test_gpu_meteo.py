@@ -1,9 +1,11 @@
-"""On-device meteo term (f3d_ads_set_meteo_corners) against the host builders.
+"""On-device meteo term (f3d_ads_set_meteo_corners) against the oracle.
 
-The host path stages and scales the corner winds and the diffusion with the
-numpy restatement of grid_get_stagered_velocity / grid_get_scaled_velocity /
-grid_get_scaled_variables (fall3d_b200.meteo) and uploads the step-layout
-arrays with f3d_ads_set_meteo.  The device path uploads the raw corner winds
+The reference path stages and scales the corner winds and the diffusion with
+the oracle's C restatement of grid_get_stagered_velocity /
+grid_get_scaled_velocity / grid_get_scaled_variables (oracle.meteo_term; the
+product's host builders in fall3d_b200.meteo equal it bit for bit,
+tests/test_meteo_ref.py) and uploads the step-layout arrays with
+f3d_ads_set_meteo.  The device path uploads the raw corner winds
 of the two time levels (ground level not zeroed: the library does it, as
 mod_F3D.F90:676-683 does) and the unscaled diffusion.  Both must give the
 same CFL time step and the same state after several steps, bit for bit, on a
@@ -14,7 +16,6 @@ import pytest
 
 from fall3d_b200 import grid as G
 from fall3d_b200 import meteo
-from fall3d_b200 import workloads as W
 from fall3d_b200.ads import PREC_FP32, PREC_FP64, Domain
 
 pytestmark = pytest.mark.gpu
@@ -39,12 +40,20 @@ def _case(map_v, seed=3):
     return g, winds, (k1, k2, k3), c0
 
 
-def _host_arrays(g, winds, ks):
+def _host_arrays(oracle_mod, g, winds, ks):
+    """Step-layout arrays (the transposes of mod_F3D.F90:931-944) of the
+    oracle's meteo term for both time levels."""
     uc, vc, wc = ([a.copy(order="F") for a in pair] for pair in winds)
+    us, vs, ws = [], [], []
     for s in range(2):
         meteo.zero_ground(uc[s], vc[s], wc[s])
-    k1, k2, k3 = (a.copy(order="F") for a in ks)
-    return W._to_layout(g, tuple(uc), tuple(vc), tuple(wc), k1, k2, k3)
+        u, v, w, k1, k2, k3 = oracle_mod.meteo_term(g, uc[s], vc[s], wc[s], *ks)
+        us.append(u)
+        vs.append(np.transpose(v, (1, 0, 2)))
+        ws.append(np.transpose(w, (2, 0, 1)))
+    f = np.asfortranarray
+    return (f(np.stack(us, axis=3)), f(np.stack(vs, axis=3)), f(np.stack(ws, axis=3)), f(k1),
+            f(np.transpose(k2, (1, 0, 2))), f(np.transpose(k3, (2, 0, 1))))
 
 
 def _run(dom, g, c0, nsteps=3):
@@ -64,9 +73,9 @@ def _run(dom, g, c0, nsteps=3):
 
 @pytest.mark.parametrize("map_v", [G.MAP_V_CARTESIAN, G.MAP_V_SIGMA_NO_DECAY, G.MAP_V_SIGMA_LINEAR_DECAY])
 @pytest.mark.parametrize("precision", [PREC_FP64, PREC_FP32])
-def test_device_meteo_term_equals_host_builders(built_lib, map_v, precision):
+def test_device_meteo_term_equals_oracle(oracle_mod, built_lib, map_v, precision):
     g, winds, ks, c0 = _case(map_v)
-    u12, v12, w12, k1, k2, k3 = _host_arrays(g, winds, ks)
+    u12, v12, w12, k1, k2, k3 = _host_arrays(oracle_mod, g, winds, ks)
     host = Domain(g, NB, precision=precision)
     host.set_meteo(u12, v12, w12, k1, k2, k3, None, 0.0, 3600.0)
     r_host = _run(host, g, c0)
@@ -82,13 +91,13 @@ def test_device_meteo_term_equals_host_builders(built_lib, map_v, precision):
     assert np.abs(r_dev[1]).max() > 0
 
 
-def test_device_meteo_constant_diffusion(built_lib):
+def test_device_meteo_constant_diffusion(oracle_mod, built_lib):
     g, winds, _, c0 = _case(G.MAP_V_SIGMA_LINEAR_DECAY, seed=4)
     kh, kv = 1500.0, 60.0
     ks = (np.full((NX + 4, NY, NZ), kh, order="F"), np.full((NX, NY + 4, NZ), kh, order="F"),
           np.full((NX, NY, NZ + 4), kv, order="F"))
     host = Domain(g, NB)
-    host.set_meteo(*_host_arrays(g, winds, ks), None, 0.0, 3600.0)
+    host.set_meteo(*_host_arrays(oracle_mod, g, winds, ks), None, 0.0, 3600.0)
     r_host = _run(host, g, c0)
     host.close()
     dev = Domain(g, NB)
@@ -100,9 +109,9 @@ def test_device_meteo_constant_diffusion(built_lib):
     assert np.array_equal(r_host[1], r_dev[1])
 
 
-def test_ensemble_class_meteo_corners(built_lib):
+def test_ensemble_class_meteo_corners(oracle_mod, built_lib):
     """Two grid classes set from corner winds on the device give the members
-    the bits of the same classes set from host-built step-layout arrays."""
+    the bits of the same classes set from the oracle's step-layout arrays."""
     from fall3d_b200.ensemble import Ensemble
     cases = [_case(G.MAP_V_SIGMA_LINEAR_DECAY, seed=5), _case(G.MAP_V_SIGMA_NO_DECAY, seed=6)]
     grids = [c[0] for c in cases]
@@ -114,7 +123,7 @@ def test_ensemble_class_meteo_corners(built_lib):
         ens = Ensemble(grids, NB, members, factors, 2, 2, 0)
         for ci, (g, winds, ks, _) in enumerate(cases):
             if path == "host":
-                ens.set_class_meteo(ci, *_host_arrays(g, winds, ks), None, 0.0, 3600.0)
+                ens.set_class_meteo(ci, *_host_arrays(oracle_mod, g, winds, ks), None, 0.0, 3600.0)
             else:
                 ens.set_class_terrain(ci, g)
                 ens.set_class_meteo_corners(ci, winds[0], winds[1], winds[2], *ks, t_its=0.0, t_ite=3600.0)
