@@ -162,7 +162,7 @@ def run_aux(args, local):
     comes from ncu on this workload."""
     import torch
     from fall3d_b200 import workloads as W
-    from fall3d_b200.ads import PREC_FP32, Domain
+    from fall3d_b200.ads import PREC_FP32, Domain, set_zsweep_epilogue
     torch.cuda.set_device(local)
     wl = W.random_c2(seed=0)
     g = wl.grid
@@ -216,6 +216,10 @@ def run_aux(args, local):
     ms["step_plain"] = round(ms["step_plain"] / K, 4)
     dom.phys_wet_deposition(8.4e-5, 0.79, pre, pblh, cat, wl.diam)
     dom.phys_radionuclides(cat, spe)
+    set_zsweep_epilogue(False)  # separate passes after the z sweep
+    timed("step_wet_decay_separate", steps)
+    ms["step_wet_decay_separate"] = round(ms["step_wet_decay_separate"] / K, 4)
+    set_zsweep_epilogue(True)  # the default: inside the z sweep
     timed("step_wet_decay", steps)
     ms["step_wet_decay"] = round(ms["step_wet_decay"] / K, 4)
     dom.set_gravity_current(g.lon_p[g.nx // 2], g.lat_p[g.ny // 2], -3600.0, 1e9, 430.0, 0.1, 0.02, 0.2, 1e6,

@@ -125,6 +125,7 @@ SIGNATURES = {
     "f3d_ads_solve_1d": [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp, _dp, _ip, C.c_int],
     "f3d_set_wait_limit": [C.c_longlong],
     "f3d_set_vset_maxit": [C.c_int],
+    "f3d_set_zsweep_epilogue": [C.c_int],
     "f3d_mlp_create": [C.c_int, _dp, C.c_double, C.c_ulonglong, C.c_int, C.POINTER(_vp)],
     "f3d_mlp_destroy": [_vp],
     "f3d_mlp_generate": [_vp, C.c_longlong, C.c_ulonglong, C.POINTER(C.c_longlong)],

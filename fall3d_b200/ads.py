@@ -417,6 +417,12 @@ def set_vset_maxit(maxit: int):
     check(lib().f3d_set_vset_maxit(int(maxit)), "f3d_set_vset_maxit")
 
 
+def set_zsweep_epilogue(on: bool = True):
+    """Wet deposition and decay inside the z sweep (True, the default) or
+    as separate passes after it (f3d_set_zsweep_epilogue)."""
+    check(lib().f3d_set_zsweep_epilogue(int(bool(on))), "f3d_set_zsweep_epilogue")
+
+
 # ---- particle shape factor (per-bin setup, host) ----------------------------
 _PI = 4.0 * math.atan(1.0)  # mod_KindType.F90:43
 

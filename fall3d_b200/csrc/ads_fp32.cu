@@ -98,6 +98,24 @@ __device__ __forceinline__ float half_phid(float d1, float d0) {
 #ifndef F3D_PF_L2
 #define F3D_PF_L2 0
 #endif
+#ifndef F3D_Z_EDGE_CMP
+#define F3D_Z_EDGE_CMP 1
+#endif
+// Element offsets along a pencil (p * stride within one bin of one member,
+// and the face offsets likewise): 32-bit, which cuts the index arithmetic of
+// the sweeps (4-9% faster); the hosts accept precision-form grids only while
+// (nx+1)(ny+1)(nz+1) stays below 2^31 (kMaxPencilSpan).
+#ifndef F3D_STRIDE32
+#define F3D_STRIDE32 1
+#endif
+#if F3D_STRIDE32
+typedef int pstride_t;
+#else
+typedef long long pstride_t;
+#endif
+#ifndef F3D_Z_EDGE_PLAIN
+#define F3D_Z_EDGE_PLAIN 0
+#endif
 __device__ __forceinline__ void prefetch_line(const void* p) {
   if (F3D_PF_L2) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
   else asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
@@ -106,10 +124,10 @@ __device__ __forceinline__ void prefetch_line(const void* p) {
 // Per-pencil operations of the precision form.  The current wind is
 // interpolated in time on the fly from the two meteo snapshots and scaled by
 // the member's wind factor (ensemble perturbation of u, v).
-template <int LIM, int DIR, int TM, bool CMP = false>
+template <int LIM, int DIR, int TM, bool CMP = false, bool EPI = false>
 struct Ops32 {
   float* cp;
-  long long cs;
+  pstride_t cs;
   float* lop;          // CMP: low part of the state, same layout and stride as cp
   const double* r64;   // CMP: 1/dxb of the pencil's cells, FP64
   const float2* r2;    // CMP: the same as FP32 pairs {hi, lo}
@@ -118,28 +136,36 @@ struct Ops32 {
                          // the interior transport against the FP64 boundary terms
   const float4* fd;   // face data {u(its), u(ite), kf, 1/dxb(f-1)} (MemberDev::f4)
   const float* vsub;  // z: settling velocity of the bin
-  long long vs;
+  pstride_t vs;
   int nf;  // cells of the pencil (faces 0..nf)
   float s0, s1, wfac;
   float dt, hdt, dt3, dt6;
   // x pencils: shared-memory staging of the rows (the compensated form also
   // stages the low part, in narrower chunks so that both tiles fit)
   static constexpr int XW = CMP ? F3D_CMP_XW : 32;
+  // z pencils are short (tens of levels): the head, steady and edge bodies
+  // all run within a few blocks of each other; with kEdgeOnly the march
+  // runs the edge body for every block after the head, a smaller code
+  // footprint at a higher cost per step
+  static constexpr bool kEdgeOnly = (DIR == DIR_Z) && (CMP ? F3D_Z_EDGE_CMP : F3D_Z_EDGE_PLAIN);
   XTile<float, (TM == 2) ? 1 : 2, XW> xt;
   XLoTile<XW> lt;
+  // EPI (z): the column's wet deposition and decay (an empty struct otherwise)
+  std::conditional_t<EPI, ZEpi, NoEpi> epi;
 
   __device__ __forceinline__ float load_c(int p) const {
     if constexpr (DIR == DIR_X) {
       return xt.load(p);
     } else {
-      if constexpr (F3D_C_PF > 0) prefetch_line(cp + (long long)min(p + F3D_C_PF, nf - 1) * cs);
+      if constexpr (F3D_C_PF > 0) prefetch_line(cp + (pstride_t)min(p + F3D_C_PF, nf - 1) * cs);
       return cp[p * cs];
     }
   }
-  __device__ __forceinline__ float load_last() const { return cp[(long long)(nf - 1) * cs]; }
+  __device__ __forceinline__ float load_last() const { return cp[(pstride_t)(nf - 1) * cs]; }
   __device__ __forceinline__ void store_c(int p, float v) {
     if constexpr (DIR == DIR_X) xt.store(p, v);
-    else cp[p * cs] = v;
+    else if constexpr (EPI && !CMP) cp[p * cs] = epi.apply32(p, v);
+    else cp[p * cs] = v;  // the compensated pair went through the epilogue in final_cmp
   }
   __device__ __forceinline__ void stage_init() {
     if constexpr (DIR == DIR_X) xt.init();
@@ -159,7 +185,7 @@ struct Ops32 {
   }
   __device__ __forceinline__ FaceV<float> face(int f) const {
     if constexpr (F3D_FACE_PF > 0) {
-      const long long fp = (long long)min(f + F3D_FACE_PF, nf) * vs;
+      const pstride_t fp = (pstride_t)min(f + F3D_FACE_PF, nf) * vs;
       prefetch_line(fd + fp);
       if constexpr (DIR == DIR_Z) prefetch_line(vsub + fp);
     }
@@ -206,13 +232,13 @@ struct Ops32 {
     if constexpr (DIR == DIR_X) {
       return lt.at(p);
     } else {
-      prefetch_line(lop + (long long)min(p + 16, nf - 1) * cs);
-      return lop[(long long)p * cs];
+      prefetch_line(lop + (pstride_t)min(p + 16, nf - 1) * cs);
+      return lop[(pstride_t)p * cs];
     }
   }
   __device__ __forceinline__ void lo_store(int p, float v) {
     if constexpr (DIR == DIR_X) lt.at(p) = v;
-    else lop[(long long)p * cs] = v;
+    else lop[(pstride_t)p * cs] = v;
   }
   __device__ __forceinline__ float final_cmp(float chi, float clo, float hl, float hr, int p) {
 #if F3D_CMP_EFT
@@ -238,16 +264,21 @@ struct Ops32 {
     const float tb = __fsub_rn(t, chi);
     float te = __fadd_rn(__fsub_rn(chi, __fsub_rn(t, tb)), __fsub_rn(d, tb));
     te = __fadd_rn(te, __fadd_rn(clo, de));
-    const float nhi = __fadd_rn(t, te);
-    lo_store(p, __fsub_rn(te, __fsub_rn(nhi, t)));
-    return nhi;
+    float nhi = __fadd_rn(t, te);
+    float nlo = __fsub_rn(te, __fsub_rn(nhi, t));
 #else
     const double dlt = ((double)hr - (double)hl) * ((double)dtf_hi + (double)dtf_lo) * __ldg(r64 + p);
     const double c64 = ((double)chi + (double)clo) + dlt;
-    const float nhi = __double2float_rn(c64);
-    lo_store(p, __double2float_rn(c64 - (double)nhi));
-    return nhi;
+    float nhi = __double2float_rn(c64);
+    float nlo = __double2float_rn(c64 - (double)nhi);
 #endif
+    if constexpr (EPI) {  // the pair is exact in FP64; one split after both processes
+      const double v = epi.apply(p, (double)nhi + (double)nlo);
+      nhi = __double2float_rn(v);
+      nlo = __double2float_rn(__dsub_rn(v, (double)nhi));
+    }
+    lo_store(p, nlo);
+    return nhi;
   }
 
   // KT right-hand side with G = P - F per face; h = 0.5 phi(r) dc
@@ -299,8 +330,10 @@ __device__ __forceinline__ void block_reduce2_f64(double a, double b, double* ou
 }
 
 // One work item (32 pencils x bpb bins of one member) of a sweep; called by
-// the per-sweep kernels and by the persistent fused step kernel.
-template <int DIR, int LIM, int TM, bool CMP = false>
+// the per-sweep kernels and by the persistent fused step kernel.  EPI (z
+// only): the wet deposition and decay epilogue, a kernel instance of its own
+// so that the sweeps without it keep their register allocation.
+template <int DIR, int LIM, int TM, bool CMP = false, bool EPI = false>
 __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ members,
                                              const WorkItem w, int bpb, unsigned char* f3d_smem) {
   const MemberDev& m = members[w.member];
@@ -316,7 +349,7 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
   const long long pen = pen_raw < nsp ? pen_raw : nsp - 1;
   double clo = 0.0, chi = 0.0;
   if (run_it) {
-    Ops32<LIM, DIR, TM, CMP> o;
+    Ops32<LIM, DIR, TM, CMP, EPI> o;
     double area;
     int n, i = 0, j = 0;
     if (DIR == DIR_X) {
@@ -365,12 +398,13 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
         o.r64 = m.rdxb64[2];
         o.r2 = m.rdxb2[2];
       }
-      o.cs = (long long)nx * ny;
+      o.cs = (pstride_t)nx * ny;
       long long fo = (long long)j * nx + i;
       o.fd = m.f4[2] + fo;
-      o.vs = (long long)nx * ny;
+      o.vs = (pstride_t)nx * ny;
       o.vsub = m.vs32 + (long long)b * (nz + 1) * ny * nx + fo;
       area = m.dx2b[j + 1] * m.dx1b[i + 1];
+      if constexpr (EPI) o.epi = zepi_setup(m, b, fo);
     }
     const double dt = m.dt;
     o.s1 = (float)m.stime;
@@ -400,7 +434,7 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
       o.dtf_lo = __double2float_rn(dtf - (double)o.dtf_hi);
     }
     // the edge blocks run the unguarded body (cheaper than the guarded one)
-    March<float, Ops32<LIM, DIR, TM, CMP>, TM, true, CMP> M(o, n);
+    March<float, Ops32<LIM, DIR, TM, CMP, EPI>, TM, true, CMP> M(o, n);
     M.run();
     if (lane_ok) {
       clo = (double)M.flux_lo * area * dt;
@@ -414,28 +448,35 @@ __device__ __forceinline__ void sweep32_item(const MemberDev* __restrict__ membe
     if (DIR == DIR_Z) {
       double* a = m.acum + ((long long)b * ny + j) * nx + i;
       *a = *a + fabs((double)M.flux_lo) * dt;
+      if constexpr (EPI) zepi_finish(m, o.epi, b, (long long)j * nx + i);
     }
   }
   block_reduce2_f64(clo, chi, m.flux_part + 2 * (long long)w.slot);
 }
 
 #ifndef F3D_CMP_BLOCKS
-#define F3D_CMP_BLOCKS 3
+#define F3D_CMP_BLOCKS 4
+#endif
+#ifndef F3D_CMP_Y_BLOCKS
+#define F3D_CMP_Y_BLOCKS 4
 #endif
 #ifndef F3D_CMP_YZ_BLOCKS
 #define F3D_CMP_YZ_BLOCKS 4
 #endif
-template <int DIR, int LIM, int TM, bool CMP>
+template <int DIR, int LIM, int TM, bool CMP, bool EPI = false>
 // 4 blocks of 128 threads per SM (128 registers); with one output buffer the
 // RK4 x tiles (4 x 12.6 KB per block) fit 4 blocks as well.  The compensated
-// x sweep runs 3 blocks (170 registers): at 128 it spills.
-__global__ void __launch_bounds__(128, CMP ? (DIR == DIR_X ? F3D_CMP_BLOCKS : F3D_CMP_YZ_BLOCKS) : 4)
+// x sweep runs 4 blocks too: at 128 registers it spills a few bytes, and it
+// measured 13% faster than 3 blocks at 168 registers.
+__global__ void __launch_bounds__(128, CMP ? (DIR == DIR_X ? F3D_CMP_BLOCKS
+                                                          : (DIR == DIR_Y ? F3D_CMP_Y_BLOCKS : F3D_CMP_YZ_BLOCKS))
+                                              : 4)
     k_sweep32(const MemberDev* __restrict__ members, const WorkItem* __restrict__ work, int bpb) {
   extern __shared__ __align__(16) unsigned char f3d_smem[];
-  sweep32_item<DIR, LIM, TM, CMP>(members, work[blockIdx.x], bpb, f3d_smem);
+  sweep32_item<DIR, LIM, TM, CMP, EPI>(members, work[blockIdx.x], bpb, f3d_smem);
 }
 
-template <int DIR, bool CMP>
+template <int DIR, bool CMP, bool EPI = false>
 static void launch_dir32(int lim, int tm, const MemberDev* members, const WorkItem* work,
                          int nblocks, int bpb, cudaStream_t st) {
   dim3 g(nblocks), b(128);
@@ -457,7 +498,7 @@ static void launch_dir32(int lim, int tm, const MemberDev* members, const WorkIt
     cudaFuncSetAttribute(k_sweep32<DIR, 3, 2, CMP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     attr_set = true;
   }
-#define F3D_L(L, T) k_sweep32<DIR, L, T, CMP><<<g, b, smem, st>>>(members, work, bpb)
+#define F3D_L(L, T) k_sweep32<DIR, L, T, CMP, EPI><<<g, b, smem, st>>>(members, work, bpb)
   if (tm == 1) {
     if (lim == 1) F3D_L(1, 1); else if (lim == 2) F3D_L(2, 1); else F3D_L(3, 1);
   } else {
@@ -466,16 +507,20 @@ static void launch_dir32(int lim, int tm, const MemberDev* members, const WorkIt
 #undef F3D_L
 }
 
-void launch_sweep32(int dir, int lim, int tm, int cmp, const MemberDev* members,
+// epi: the z sweep runs the wet deposition and decay epilogue (the members'
+// epi_on)
+void launch_sweep32(int dir, int lim, int tm, int cmp, int epi, const MemberDev* members,
                     const WorkItem* work, int nblocks, int bpb, cudaStream_t st) {
   if (nblocks <= 0) return;
   if (cmp) {
     if (dir == DIR_X) launch_dir32<DIR_X, true>(lim, tm, members, work, nblocks, bpb, st);
     else if (dir == DIR_Y) launch_dir32<DIR_Y, true>(lim, tm, members, work, nblocks, bpb, st);
+    else if (epi) launch_dir32<DIR_Z, true, true>(lim, tm, members, work, nblocks, bpb, st);
     else launch_dir32<DIR_Z, true>(lim, tm, members, work, nblocks, bpb, st);
   } else {
     if (dir == DIR_X) launch_dir32<DIR_X, false>(lim, tm, members, work, nblocks, bpb, st);
     else if (dir == DIR_Y) launch_dir32<DIR_Y, false>(lim, tm, members, work, nblocks, bpb, st);
+    else if (epi) launch_dir32<DIR_Z, false, true>(lim, tm, members, work, nblocks, bpb, st);
     else launch_dir32<DIR_Z, false>(lim, tm, members, work, nblocks, bpb, st);
   }
 }
@@ -587,10 +632,10 @@ __device__ __forceinline__ void source32_all(MemberDev* members, int nmembers) {
 
 // Out-of-line sweep items for the persistent kernel: each direction keeps its
 // own register allocation instead of one inlined union of all three.
-template <int DIR, int LIM, int TM, bool CMP>
+template <int DIR, int LIM, int TM, bool CMP, bool EPI = false>
 __device__ __noinline__ void sweep32_item_call(MemberDev* members, WorkItem w, int bpb,
                                                unsigned char* smem) {
-  sweep32_item<DIR, LIM, TM, CMP>(members, w, bpb, smem);
+  sweep32_item<DIR, LIM, TM, CMP, EPI>(members, w, bpb, smem);
 }
 
 // One whole time step of every member in one persistent kernel: source,
@@ -615,6 +660,7 @@ __global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
       const WorkItem w = a.work[dir][it];
       if (dir == 0) sweep32_item_call<0, LIM, TM, CMP>(a.members, w, a.bpb, f3d_smem);
       else if (dir == 1) sweep32_item_call<1, LIM, TM, CMP>(a.members, w, a.bpb, f3d_smem);
+      else if (a.epi) sweep32_item_call<2, LIM, TM, CMP, true>(a.members, w, a.bpb, f3d_smem);
       else sweep32_item_call<2, LIM, TM, CMP>(a.members, w, a.bpb, f3d_smem);
     }
     grid_barrier(a.counters + 6, a.err, a.wait_limit);

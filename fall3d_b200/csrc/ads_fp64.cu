@@ -45,7 +45,9 @@ __device__ __forceinline__ double limiter64(double d1, double d0) {
 }
 
 // Per-pencil operations of the FP64 form, reference operation order.
-template <int LIM, int DIR>
+// EPI (z only): wet deposition and decay applied to each cell as it is
+// stored (ZEpi).
+template <int LIM, int DIR, bool EPI = false>
 struct Ops64 {
   double* cp;
   long long cs;
@@ -57,6 +59,8 @@ struct Ops64 {
   int nf;              // cells of the pencil (faces 0..nf)
   double dt, hdt;
   XTile<double> xt;    // x pencils: shared-memory staging of the rows
+  ZEpi epi;            // EPI: the column's wet deposition and decay
+  static constexpr bool kEdgeOnly = false;
 
   __device__ __forceinline__ double load_c(int p) const {
     if constexpr (DIR == DIR_X) {
@@ -70,6 +74,7 @@ struct Ops64 {
   __device__ __forceinline__ double load_last() const { return cp[(long long)(nf - 1) * cs]; }
   __device__ __forceinline__ void store_c(int p, double v) {
     if constexpr (DIR == DIR_X) xt.store(p, v);
+    else if constexpr (EPI) cp[p * cs] = epi.apply(p, v);
     else cp[p * cs] = v;
   }
   __device__ __forceinline__ void stage_init() { if constexpr (DIR == DIR_X) xt.init(); }
@@ -163,14 +168,88 @@ __device__ __forceinline__ void block_reduce2(double a, double b, double* out) {
   }
 }
 
+// One pencil of a sweep: march, boundary fluxes, kept ghosts and (z) the
+// deposit; EPI adds the wet deposition and decay epilogue (z only).
+template <int DIR, int LIM, int TM, bool EPI>
+__device__ __forceinline__ void sweep64_pencil(const MemberDev& m, long long pen, int b, bool lane_ok,
+                                               int warp, unsigned char* f3d_smem, double& clo,
+                                               double& chi) {
+  const int nx = m.nx, ny = m.ny, nz = m.nz;
+  Ops64<LIM, DIR, EPI> o;
+  double area;
+  int n, i = 0, j = 0;
+  if (DIR == DIR_X) {
+    j = (int)(pen % ny);
+    int k = (int)(pen / ny);
+    n = nx;
+    o.cp = m.c64 + (((long long)b * nz + k) * ny + j) * nx;
+    o.xt.setup(f3d_smem + warp * XTile<double>::BYTES, lane_ok ? o.cp : nullptr,
+               threadIdx.x & 31, nx);
+    o.cs = 1;
+    long long fo = (long long)k * (nx + 1) * ny + j;
+    o.vel = m.ucur + fo;
+    o.kk = m.kkf[0] + fo;
+    o.vs = ny;
+    o.vsub = nullptr;
+    area = m.dx3b[k + 1] * m.dx2b[j + 1];
+  } else if (DIR == DIR_Y) {
+    i = (int)(pen % nx);
+    int k = (int)(pen / nx);
+    n = ny;
+    o.cp = m.c64 + ((long long)b * nz + k) * ny * (long long)nx + i;
+    o.cs = nx;
+    long long fo = (long long)k * (ny + 1) * nx + i;
+    o.vel = m.vcur + fo;
+    o.kk = m.kkf[1] + fo;
+    o.vs = nx;
+    o.vsub = nullptr;
+    area = m.dx3b[k + 1] * m.dx1b[i + 1];
+  } else {
+    i = (int)(pen % nx);
+    j = (int)(pen / nx);
+    n = nz;
+    o.cp = m.c64 + (long long)b * nz * ny * nx + (long long)j * nx + i;
+    o.cs = (long long)nx * ny;
+    long long fo = (long long)j * nx + i;
+    o.vel = m.wcur + fo;
+    o.kk = m.kkf[2] + fo;
+    o.vs = (long long)nx * ny;
+    o.vsub = m.vs + (long long)b * (nz + 1) * ny * nx + fo;
+    area = m.dx2b[j + 1] * m.dx1b[i + 1];
+    if constexpr (EPI) o.epi = zepi_setup(m, b, fo);
+  }
+  o.geo = m.geo[DIR];
+  o.nf = n;
+  o.dt = m.dt;
+  o.hdt = 0.5 * m.dt;
+  // RK4: the edge blocks run the unguarded body (cheaper than the guarded one)
+  March<double, Ops64<LIM, DIR, EPI>, TM, (F3D_V64 != 0)> M(o, n);
+  M.run();
+  const double dt = m.dt;
+  if (lane_ok) {
+    clo = M.flux_lo * area * dt;
+    chi = M.flux_hi * area * dt;
+    if (m.gh64) {  // the free-flow ghosts of this pencil (mod_ADS.F90:1227-1326)
+      double* g = m.gh64 + (long long)b * gh_per_bin(nx, ny, nz);
+      g[gh_offset(DIR, 0, pen, nx, ny, nz)] = M.gL;
+      g[gh_offset(DIR, 1, pen, nx, ny, nz)] = M.gR;
+    }
+  }
+  if (DIR == DIR_Z && lane_ok) {
+    const long long ij = (long long)j * nx + i;
+    double* a = m.acum + (long long)b * ny * nx + ij;
+    *a = *a + fabs(M.flux_lo) * dt;  // mod_ADS.F90:791
+    if constexpr (EPI) zepi_finish(m, o.epi, b, ij);
+  }
+}
+
 // One work item of a sweep (per-sweep kernels and the persistent step kernel).
-template <int DIR, int LIM, int TM>
+template <int DIR, int LIM, int TM, bool EPI = false>
 __device__ __forceinline__ void sweep64_item(const MemberDev* __restrict__ members,
                                              const WorkItem w, int bpb, unsigned char* f3d_smem) {
   const MemberDev& m = members[w.member];
-  const int nx = m.nx, ny = m.ny, nz = m.nz;
-  const long long nsp = (DIR == DIR_X) ? (long long)ny * nz
-                        : (DIR == DIR_Y) ? (long long)nx * nz : (long long)nx * ny;
+  const long long nsp = (DIR == DIR_X) ? (long long)m.ny * m.nz
+                        : (DIR == DIR_Y) ? (long long)m.nx * m.nz : (long long)m.nx * m.ny;
   const int warp = threadIdx.x >> 5;
   const long long pen_raw = (long long)w.pen0 + 32 * (warp / bpb) + (threadIdx.x & 31);
   const long long pen0w = (long long)w.pen0 + 32 * (warp / bpb);
@@ -182,97 +261,54 @@ __device__ __forceinline__ void sweep64_item(const MemberDev* __restrict__ membe
   const long long pen = pen_raw < nsp ? pen_raw : nsp - 1;
   double clo = 0.0, chi = 0.0;  // contributions flux*area*dt
   if (run_it) {
-    Ops64<LIM, DIR> o;
-    double area;
-    int n, i = 0, j = 0;
-    if (DIR == DIR_X) {
-      j = (int)(pen % ny);
-      int k = (int)(pen / ny);
-      n = nx;
-      o.cp = m.c64 + (((long long)b * nz + k) * ny + j) * nx;
-      o.xt.setup(f3d_smem + warp * XTile<double>::BYTES, lane_ok ? o.cp : nullptr,
-                 threadIdx.x & 31, nx);
-      o.cs = 1;
-      long long fo = (long long)k * (nx + 1) * ny + j;
-      o.vel = m.ucur + fo;
-      o.kk = m.kkf[0] + fo;
-      o.vs = ny;
-      o.vsub = nullptr;
-      area = m.dx3b[k + 1] * m.dx2b[j + 1];
-    } else if (DIR == DIR_Y) {
-      i = (int)(pen % nx);
-      int k = (int)(pen / nx);
-      n = ny;
-      o.cp = m.c64 + ((long long)b * nz + k) * ny * (long long)nx + i;
-      o.cs = nx;
-      long long fo = (long long)k * (ny + 1) * nx + i;
-      o.vel = m.vcur + fo;
-      o.kk = m.kkf[1] + fo;
-      o.vs = nx;
-      o.vsub = nullptr;
-      area = m.dx3b[k + 1] * m.dx1b[i + 1];
-    } else {
-      i = (int)(pen % nx);
-      j = (int)(pen / nx);
-      n = nz;
-      o.cp = m.c64 + (long long)b * nz * ny * nx + (long long)j * nx + i;
-      o.cs = (long long)nx * ny;
-      long long fo = (long long)j * nx + i;
-      o.vel = m.wcur + fo;
-      o.kk = m.kkf[2] + fo;
-      o.vs = (long long)nx * ny;
-      o.vsub = m.vs + (long long)b * (nz + 1) * ny * nx + fo;
-      area = m.dx2b[j + 1] * m.dx1b[i + 1];
-    }
-    o.geo = m.geo[DIR];
-    o.nf = n;
-    o.dt = m.dt;
-    o.hdt = 0.5 * m.dt;
-    // RK4: the edge blocks run the unguarded body (cheaper than the guarded one)
-    March<double, Ops64<LIM, DIR>, TM, (F3D_V64 != 0)> M(o, n);
-    M.run();
-    const double dt = m.dt;
-    if (lane_ok) {
-      clo = M.flux_lo * area * dt;
-      chi = M.flux_hi * area * dt;
-      if (m.gh64) {  // the free-flow ghosts of this pencil (mod_ADS.F90:1227-1326)
-        double* g = m.gh64 + (long long)b * gh_per_bin(nx, ny, nz);
-        g[gh_offset(DIR, 0, pen, nx, ny, nz)] = M.gL;
-        g[gh_offset(DIR, 1, pen, nx, ny, nz)] = M.gR;
-      }
-    }
-    if (DIR == DIR_Z) {
-      double* a = m.acum + ((long long)b * ny + j) * nx + i;
-      *a = *a + fabs(M.flux_lo) * dt;  // mod_ADS.F90:791
-    }
+    // the epilogue is a kernel instance of its own (chosen at launch), so
+    // that the sweeps without it keep their register allocation
+    sweep64_pencil<DIR, LIM, TM, DIR == DIR_Z && EPI>(m, pen, b, lane_ok, warp, f3d_smem, clo, chi);
   }
   block_reduce2(clo, chi, m.flux_part + 2 * (long long)w.slot);
 }
 
-template <int DIR, int LIM, int TM>
-__global__ void __launch_bounds__(128) k_sweep64(const MemberDev* __restrict__ members,
-                                                 const WorkItem* __restrict__ work, int bpb) {
+// y and z: 3 blocks of 128 threads per SM (168 registers, a few hundred
+// bytes spilled), 9-10% faster than 2 blocks at 222-230 registers; x keeps
+// the compiler's own choice (2 blocks), 4% faster there than 3.
+#ifndef F3D_FP64_MINB
+#define F3D_FP64_MINB 3
+#endif
+template <int DIR, int LIM, int TM, bool EPI = false>
+__global__ void __launch_bounds__(128, F3D_FP64_MINB) k_sweep64(const MemberDev* __restrict__ members,
+                                                                 const WorkItem* __restrict__ work,
+                                                                 int bpb) {
   extern __shared__ __align__(16) unsigned char f3d_smem[];
-  sweep64_item<DIR, LIM, TM>(members, work[blockIdx.x], bpb, f3d_smem);
+  sweep64_item<DIR, LIM, TM, EPI>(members, work[blockIdx.x], bpb, f3d_smem);
+}
+template <int LIM, int TM>
+__global__ void __launch_bounds__(128) k_sweep64x(const MemberDev* __restrict__ members,
+                                                  const WorkItem* __restrict__ work, int bpb) {
+  extern __shared__ __align__(16) unsigned char f3d_smem[];
+  sweep64_item<DIR_X, LIM, TM>(members, work[blockIdx.x], bpb, f3d_smem);
 }
 
 // Host launchers -------------------------------------------------------------
-template <int DIR>
+template <int DIR, bool EPI = false>
 static void launch_dir64(int lim, int tm, const MemberDev* members,
                          const WorkItem* work, int nblocks, int bpb, cudaStream_t st) {
   dim3 g(nblocks), b(128);
   const int smem = (DIR == DIR_X) ? 4 * XTile<double>::BYTES : 0;
   static bool attr_set = false;
   if (!attr_set && smem > 0) {
-    cudaFuncSetAttribute(k_sweep64<DIR, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep64<DIR, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep64<DIR, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep64<DIR, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep64<DIR, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_sweep64<DIR, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64x<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64x<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64x<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64x<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64x<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_sweep64x<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     attr_set = true;
   }
-#define F3D_L(L, T) k_sweep64<DIR, L, T><<<g, b, smem, st>>>(members, work, bpb)
+#define F3D_L(L, T)                                                             \
+  do {                                                                          \
+    if constexpr (DIR == DIR_X) k_sweep64x<L, T><<<g, b, smem, st>>>(members, work, bpb); \
+    else k_sweep64<DIR, L, T, EPI><<<g, b, smem, st>>>(members, work, bpb);     \
+  } while (0)
   if (tm == 1) {
     if (lim == 1) F3D_L(1, 1); else if (lim == 2) F3D_L(2, 1); else F3D_L(3, 1);
   } else {
@@ -281,11 +317,14 @@ static void launch_dir64(int lim, int tm, const MemberDev* members,
 #undef F3D_L
 }
 
-void launch_sweep64(int dir, int lim, int tm, const MemberDev* members,
+// epi: the z sweep runs the wet deposition and decay epilogue (the members'
+// epi_on)
+void launch_sweep64(int dir, int lim, int tm, int epi, const MemberDev* members,
                     const WorkItem* work, int nblocks, int bpb, cudaStream_t st) {
   if (nblocks <= 0) return;
   if (dir == DIR_X) launch_dir64<DIR_X>(lim, tm, members, work, nblocks, bpb, st);
   else if (dir == DIR_Y) launch_dir64<DIR_Y>(lim, tm, members, work, nblocks, bpb, st);
+  else if (epi) launch_dir64<DIR_Z, true>(lim, tm, members, work, nblocks, bpb, st);
   else launch_dir64<DIR_Z>(lim, tm, members, work, nblocks, bpb, st);
 }
 
@@ -367,10 +406,10 @@ __device__ __forceinline__ void source64_all(MemberDev* members, int nmembers) {
   }
 }
 
-template <int DIR, int LIM, int TM>
+template <int DIR, int LIM, int TM, bool EPI = false>
 __device__ __noinline__ void sweep64_item_call(MemberDev* members, WorkItem w, int bpb,
                                                unsigned char* smem) {
-  sweep64_item<DIR, LIM, TM>(members, w, bpb, smem);
+  sweep64_item<DIR, LIM, TM, EPI>(members, w, bpb, smem);
 }
 
 // FP64 form of the persistent step kernel (see k_fused32); the first phase
@@ -397,6 +436,7 @@ __global__ void __launch_bounds__(128) k_fused64(FusedArgs a) {
       const WorkItem w = a.work[dir][it];
       if (dir == 0) sweep64_item_call<0, LIM, TM>(a.members, w, a.bpb, f3d_smem);
       else if (dir == 1) sweep64_item_call<1, LIM, TM>(a.members, w, a.bpb, f3d_smem);
+      else if (a.epi) sweep64_item_call<2, LIM, TM, true>(a.members, w, a.bpb, f3d_smem);
       else sweep64_item_call<2, LIM, TM>(a.members, w, a.bpb, f3d_smem);
     }
     grid_barrier(a.counters + 6, a.err, a.wait_limit);

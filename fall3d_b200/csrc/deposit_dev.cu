@@ -18,6 +18,10 @@
 // P^b, the boundary-layer test and the decay factors are evaluated on the
 // host, with the same C library as the CPU restatement; the kernels do the
 // per-cell arithmetic in the reference's order (compiled with --fmad=false).
+//
+// With the z sweep's epilogue (MemberDev::epi_on) both processes run inside
+// the z sweep, cell by cell; k_radio then only sets the daughter bins from
+// their parents and decays the kept halo layers (RadioArgs::tail).
 #include <cuda_runtime.h>
 
 #include "f3d_common.cuh"
@@ -62,8 +66,10 @@ __global__ void k_wet(WetArgs a) {
 }
 
 template <class T>
-__device__ __forceinline__ void decay_cell(const RadioArgs& a, T* c, long long q, long long stride) {
+__device__ __forceinline__ void decay_cell(const RadioArgs& a, T* c, long long q, long long stride,
+                                           bool daughters_only = false) {
   for (int r = 0; r < a.nr; ++r) {
+    if (daughters_only && a.parent[r] < 0) continue;  // decayed by the z sweep's epilogue
     const double f = a.fdev ? a.fdev[r] : a.fact[r];
     const double pf = a.fdev ? a.fdev[a.nr + r] : a.pfact[r];
     T* p = c + (long long)a.bin[r] * stride + q;
@@ -74,8 +80,9 @@ __device__ __forceinline__ void decay_cell(const RadioArgs& a, T* c, long long q
 
 // The same on the compensated pair hi + lo of the precision form.
 __device__ __forceinline__ void decay_cell_pair(const RadioArgs& a, float* hi, float* lo, long long q,
-                                                long long stride) {
+                                                long long stride, bool daughters_only = false) {
   for (int r = 0; r < a.nr; ++r) {
+    if (daughters_only && a.parent[r] < 0) continue;
     const double f = a.fdev ? a.fdev[r] : a.fact[r];
     const double pf = a.fdev ? a.fdev[a.nr + r] : a.pfact[r];
     const long long at = (long long)a.bin[r] * stride + q;
@@ -93,17 +100,22 @@ __device__ __forceinline__ void decay_cell_pair(const RadioArgs& a, float* hi, f
 __global__ void k_radio(RadioArgs a) {
   const long long n2 = (long long)a.nx * a.ny, n3 = n2 * a.nz;
   const long long ng = (a.gh64 || a.gh32) ? a.ngh : 0;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n3 + n2 + ng;
+  bool daughters = false;
+  for (int r = 0; r < a.nr; ++r) daughters = daughters || a.parent[r] >= 0;
+  // after the epilogue only the halo layers remain when no bin is a daughter
+  const long long e0 = (a.tail && !daughters) ? n3 + n2 : 0;
+  const bool dOnly = a.tail != 0;
+  for (long long e = e0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n3 + n2 + ng;
        e += (long long)gridDim.x * blockDim.x) {
     if (e < n3) {
-      if (a.c64) decay_cell(a, a.c64, e, n3);
-      else if (a.c32lo) decay_cell_pair(a, a.c32, a.c32lo, e, n3);
-      else decay_cell(a, a.c32, e, n3);
+      if (a.c64) decay_cell(a, a.c64, e, n3, dOnly);
+      else if (a.c32lo) decay_cell_pair(a, a.c32, a.c32lo, e, n3, dOnly);
+      else decay_cell(a, a.c32, e, n3, dOnly);
     } else if (e < n3 + n2) {
       const long long q = e - n3;
-      decay_cell(a, a.acum, q, n2);
-      if (a.awet) decay_cell(a, a.awet, q, n2);
-    } else {
+      decay_cell(a, a.acum, q, n2, dOnly);
+      if (a.awet) decay_cell(a, a.awet, q, n2, dOnly);
+    } else {  // halo layers: the sweeps' ghosts, not seen by the epilogue
       const long long q = e - n3 - n2;
       if (a.gh64) decay_cell(a, a.gh64, q, ng);
       else decay_cell(a, a.gh32, q, ng);

@@ -24,9 +24,9 @@
 
 namespace f3d {
 int set_error_msg(const char* fmt, ...);
-void launch_sweep64(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
+void launch_sweep64(int dir, int lim, int tm, int epi, const MemberDev* members, const WorkItem* work,
                     int nblocks, int bpb, cudaStream_t st);
-void launch_sweep32(int dir, int lim, int tm, int cmp, const MemberDev* members,
+void launch_sweep32(int dir, int lim, int tm, int cmp, int epi, const MemberDev* members,
                     const WorkItem* work, int nblocks, int bpb, cudaStream_t st);
 void launch_prep64(const MemberDev* members, const int* blk_member, const int* blk_first,
                    int nblocks, int mask, cudaStream_t st);
@@ -348,6 +348,10 @@ extern "C" int f3d_ens_create(int nclasses, const f3d_dims* dims, int nmembers,
   for (int c = 0; c < nclasses; ++c)
     if (dims[c].nx < 1 || dims[c].ny < 1 || dims[c].nz < 1 || dims[c].nbins != nb)
       return set_error_msg("f3d_ens_create: class %d dims invalid or bins differ", c);
+  for (int c = 0; c < nclasses; ++c)
+    if (precision != F3D_PREC_FP64 && !pencil_span_ok(dims[c].nx, dims[c].ny, dims[c].nz))
+      return set_error_msg("f3d_ens_create: class %d grid too large for the precision form "
+                           "((nx+1)(ny+1)(nz+1) must stay below 2^31)", c);
   for (int m = 0; m < nmembers; ++m)
     if (members[m].grid_class < 0 || members[m].grid_class >= nclasses)
       return set_error_msg("f3d_ens_create: member %d class %d out of range", m, members[m].grid_class);
@@ -1049,15 +1053,64 @@ int update_radio_factors(f3d_ens* e, const double* dt) {
   return 0;
 }
 
+// Configure every member's z-sweep epilogue (wet deposition and decay inside
+// the z sweep, f3d_set_zsweep_epilogue); a change re-uploads the descriptors
+// and drops the step graphs, whose launches differ.
+int sync_epilogue(f3d_ens* e) {
+  const bool on = zsweep_epilogue() && (e->wet_on || e->radio_on);
+  const size_t nr = e->radio.bin.size();
+  bool changed = false;
+  for (int m = 0; m < e->nm; ++m) {
+    MemberDev& d = e->hm[m];
+    const EnsClass& k = e->cls[e->member_class[m]];
+    MemberDev w = d;
+    const bool wet = on && e->wet_on && k.wet_set;
+    w.epi_on = on ? 1 : 0;
+    w.wet_mask = wet ? e->wet_mask : 0ull;
+    w.wet_a = e->wet_a;
+    w.powpb = wet ? k.powpb : nullptr;
+    w.ktop = wet ? k.ktop : nullptr;
+    w.awet = e->awet.empty() ? nullptr : e->awet[m];
+    const bool dec = on && e->radio_on && e->d_radfact;
+    w.radf = dec ? e->d_radfact + 2 * nr * (size_t)m : nullptr;
+    w.daughter_mask = 0ull;
+    for (int b = 0; b < 64; ++b) w.rad_r[b] = -1;
+    if (dec)
+      for (size_t q = 0; q < nr; ++q) {
+        w.rad_r[e->radio.bin[q]] = (signed char)q;
+        if (e->radio.parent[q] >= 0) w.daughter_mask |= 1ull << e->radio.bin[q];
+      }
+    if (memcmp(&w, &d, sizeof(MemberDev)) != 0) {
+      d = w;
+      changed = true;
+    }
+  }
+  if (changed) {
+    drop_graphs(e);
+    if (upload_members(e)) return 1;
+  }
+  return 0;
+}
+
+// With the epilogue on, what the z sweep leaves to k_radio: the daughter
+// bins, set from their parents, and the kept halo layers.
+bool radio_tail_needed(const f3d_ens* e, int m) {
+  if (!e->radio_on) return false;
+  const MemberDev& d = e->hm[m];
+  return d.daughter_mask != 0ull || d.gh64 || d.gh32;
+}
+
 // Wet deposition and radioactive decay of every member after its sweeps
-// (mod_F3D.F90:1493-1520), one launch each per member.
+// (mod_F3D.F90:1493-1520), one launch each per member, or (epilogue on) the
+// remainder of the decay that the z sweep leaves.
 int enqueue_wet_radio(f3d_ens* e) {
   for (int m = 0; m < e->nm; ++m) {
     const MemberDev& d = e->hm[m];
     const EnsClass& k = e->cls[e->member_class[m]];
     const double* dt_dev = reinterpret_cast<const double*>(
         reinterpret_cast<const char*>(e->dm + m) + offsetof(MemberDev, dt));
-    if (e->wet_on && k.wet_set) {
+    if (d.epi_on && !radio_tail_needed(e, m)) continue;
+    if (e->wet_on && k.wet_set && !d.epi_on) {
       WetArgs a;
       memset(&a, 0, sizeof(a));
       a.nx = d.nx;
@@ -1089,6 +1142,7 @@ int enqueue_wet_radio(f3d_ens* e) {
         r.parent[q] = e->radio.parent[q];
       }
       r.fdev = e->d_radfact + 2 * (size_t)r.nr * m;
+      r.tail = d.epi_on;
       r.c64 = d.c64;
       r.c32 = d.c32;
       r.c32lo = d.c32lo;
@@ -1107,9 +1161,15 @@ int enqueue_wet_radio(f3d_ens* e) {
 
 int wet_radio_launches(const f3d_ens* e) {
   int n = 0;
-  for (int m = 0; m < e->nm; ++m)
+  for (int m = 0; m < e->nm; ++m) {
+    if (e->hm[m].epi_on) {
+      n += radio_tail_needed(e, m) ? 1 : 0;
+      continue;
+    }
     if (e->wet_on && e->cls[e->member_class[m]].wet_set) ++n;
-  return n + (e->radio_on ? e->nm : 0);
+    if (e->radio_on) ++n;
+  }
+  return n;
 }
 
 int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullptr,
@@ -1136,6 +1196,7 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullpt
     a.err = e->d_err;
     a.bpb = e->bpb;
     a.wait_limit = wait_limit();
+    a.epi = e->hm[0].epi_on;  // the same for every member
     void* args[] = {&a};
     ECK(cudaLaunchCooperativeKernel(func, dim3(e->fused_grid), dim3(128), args, (size_t)smem, e->st));
     e->launches += 1;
@@ -1159,9 +1220,10 @@ int enqueue_step(f3d_ens* e, bool xfirst, bool advance, cudaEvent_t* ev = nullpt
   for (int q = 0; q < 3; ++q) {
     const int d = order[q];
     if (e->prec == F3D_PREC_FP64)
-      launch_sweep64(d, e->lim, e->tm, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
+      launch_sweep64(d, e->lim, e->tm, e->hm[0].epi_on, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
     else
-      launch_sweep32(d, e->lim, e->tm, e->cmp, e->dm, e->dwork[d], e->nwork[d], e->bpb, e->st);
+      launch_sweep32(d, e->lim, e->tm, e->cmp, e->hm[0].epi_on, e->dm, e->dwork[d], e->nwork[d], e->bpb,
+                     e->st);
     e->launches += 1;
     if (ev) ECK(cudaEventRecord(ev[2 + q], e->st));
   }
@@ -1238,6 +1300,7 @@ extern "C" int f3d_ens_run(f3d_ens* e, int nsteps) {
   for (const EnsClass& k : e->cls)
     if (k.rep >= 0 && (!k.meteo_set || !k.grid_set)) return set_error_msg("f3d_ens_run: class not ready");
   ECK(cudaSetDevice(e->device));
+  if (sync_epilogue(e)) return 1;
   if (e->prof) {
     for (int s = 0; s < nsteps; ++s) {
       const bool xfirst = (e->mode == F3D_ENS_MODE_PERSISTENT) || (e->iiter % 2 == 0);
@@ -1506,6 +1569,7 @@ extern "C" int f3d_ens_step(f3d_ens* e, const double* dt, const double* time, in
     if (k.rep >= 0 && (!k.meteo_set || !k.grid_set)) return set_error_msg("f3d_ens_step: class not ready");
   ECK(cudaSetDevice(e->device));
   if (update_radio_factors(e, dt)) return 1;
+  if (sync_epilogue(e)) return 1;
   std::vector<std::pair<int, GcArgs>> gcl;
   if (e->gc_any) {  // the members whose current acts at their time
     bool changed = false;

@@ -19,7 +19,7 @@
 
 namespace f3d {
 // ads_fp64.cu
-void launch_sweep64(int dir, int lim, int tm, const MemberDev* members, const WorkItem* work,
+void launch_sweep64(int dir, int lim, int tm, int epi, const MemberDev* members, const WorkItem* work,
                     int nblocks, int bpb, cudaStream_t st);
 void launch_prep64(const MemberDev* members, const int* blk_member, const int* blk_first,
                    int nblocks, int mask, cudaStream_t st);
@@ -72,7 +72,7 @@ void launch_ads_solve_1d(int n, int lim, double* c, const double* dxp, const dou
                          const double* u, const double* k, double dt, const double bvalue[2],
                          const int bcode[2], double* flux, double* work, cudaStream_t st);
 // ads_fp32.cu
-void launch_sweep32(int dir, int lim, int tm, int cmp, const MemberDev* members,
+void launch_sweep32(int dir, int lim, int tm, int cmp, int epi, const MemberDev* members,
                     const WorkItem* work, int nblocks, int bpb, cudaStream_t st);
 void launch_prep32(const MemberDev* members, const int* blk_member, const int* blk_first,
                    int nblocks, int mask, cudaStream_t st);
@@ -185,6 +185,9 @@ struct f3d_ctx {
   bool radio_on = false;
   std::vector<int> rad_bin, rad_parent;
   std::vector<double> rad_kn, rad_pkn;
+  double* d_radf = nullptr;       // z-sweep epilogue: this step's decay factors
+  std::vector<double> radf_host;  // their host copy, for the dt they were made for
+  double radf_dt = -1.0;
 };
 
 template <class T>
@@ -244,9 +247,16 @@ namespace f3d {
 constexpr long long kDefaultWaitLimit = 1LL << 25;  // = kSpinLimit (step_dev.cuh)
 static std::atomic<long long> g_wait_limit{kDefaultWaitLimit};
 static std::atomic<int> g_vset_maxit{1000};
+static std::atomic<int> g_zepi{1};
 long long wait_limit() { return g_wait_limit.load(); }
 int vset_maxit() { return g_vset_maxit.load(); }
+int zsweep_epilogue() { return g_zepi.load(); }
 }  // namespace f3d
+
+extern "C" int f3d_set_zsweep_epilogue(int on) {
+  g_zepi.store(on ? 1 : 0);
+  return 0;
+}
 
 extern "C" int f3d_set_wait_limit(long long polls) {
   g_wait_limit.store(polls < 0 ? kDefaultWaitLimit : polls);
@@ -276,6 +286,10 @@ extern "C" int f3d_ads_create(const f3d_dims* dims, int limiter, int time_marchi
     return set_err("f3d_ads_create: time_marching %d not in 1..2", time_marching);
   if (precision != F3D_PREC_FP64 && precision != F3D_PREC_FP32 && precision != F3D_PREC_FP32C)
     return set_err("f3d_ads_create: precision %d unknown", precision);
+  if (precision != F3D_PREC_FP64 && !pencil_span_ok(dims->nx, dims->ny, dims->nz))
+    return set_err("f3d_ads_create: grid %d x %d x %d too large for the precision form "
+                   "((nx+1)(ny+1)(nz+1) must stay below 2^31); use the FP64 form", dims->nx, dims->ny,
+                   dims->nz);
   const int cmp = precision == F3D_PREC_FP32C;
   if (cmp) precision = F3D_PREC_FP32;
   *out = nullptr;
@@ -1164,9 +1178,10 @@ extern "C" int f3d_ads_download_state(f3d_ctx* c, double* my_c, double* my_acum)
 static int enqueue_sweep(f3d_ctx* c, int dir) {
   c->launches += 1;
   if (c->prec == F3D_PREC_FP64)
-    launch_sweep64(dir, c->lim, c->tm, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
+    launch_sweep64(dir, c->lim, c->tm, c->hm.epi_on, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
   else
-    launch_sweep32(dir, c->lim, c->tm, c->cmp, c->dm, c->dwork[dir], c->nblk[dir], c->bpb, c->st);
+    launch_sweep32(dir, c->lim, c->tm, c->cmp, c->hm.epi_on, c->dm, c->dwork[dir], c->nblk[dir], c->bpb,
+                   c->st);
   CKL();
   return 0;
 }
@@ -1197,10 +1212,67 @@ static int check_ready(f3d_ctx* c, const char* who) {
   return 0;
 }
 
+// Decay factors exp(-kn dt) of the radionuclide bins and of their parents
+// (host libm, as the CPU restatement evaluates them).
+static void radio_factors(const std::vector<double>& kn, const std::vector<double>& pkn,
+                          const std::vector<int>& parent, double dt, double* fact, double* pfact) {
+  for (size_t q = 0; q < kn.size(); ++q) {
+    fact[q] = exp(-kn[q] * dt);
+    pfact[q] = parent[q] >= 0 ? exp(-pkn[q] * dt) : 1.0;
+  }
+}
+
+// Configure the z sweep's wet deposition and decay epilogue for a step of dt:
+// the member descriptor is uploaded when a field changes, the decay factors
+// when dt changes.
+static int sync_epilogue(f3d_ctx* c, double dt) {
+  MemberDev& m = c->hm;
+  const bool on = zsweep_epilogue() && (c->wet_on || c->radio_on);
+  MemberDev want = m;
+  want.epi_on = on ? 1 : 0;
+  want.wet_mask = (on && c->wet_on) ? c->wet_mask : 0ull;
+  want.wet_a = c->wet_a;
+  want.powpb = c->d_powpb;
+  want.ktop = c->d_ktop;
+  want.awet = c->wet_on ? c->d_awet : nullptr;
+  want.radf = nullptr;
+  want.daughter_mask = 0ull;
+  for (int b = 0; b < 64; ++b) want.rad_r[b] = -1;
+  if (on && c->radio_on) {
+    const size_t nr = c->rad_bin.size();
+    if (!c->d_radf && dalloc(c, &c->d_radf, 2 * 64)) return 1;
+    if (c->radf_dt != dt || c->radf_host.size() != 2 * nr) {
+      c->radf_host.assign(2 * nr, 1.0);
+      radio_factors(c->rad_kn, c->rad_pkn, c->rad_parent, dt, c->radf_host.data(),
+                    c->radf_host.data() + nr);
+      // from pageable memory: the call returns once the values are staged
+      CK(cudaMemcpyAsync(c->d_radf, c->radf_host.data(), 2 * nr * 8, cudaMemcpyHostToDevice, c->st));
+      c->radf_dt = dt;
+    }
+    want.radf = c->d_radf;
+    for (size_t q = 0; q < nr; ++q) {
+      want.rad_r[c->rad_bin[q]] = (signed char)q;
+      if (c->rad_parent[q] >= 0) want.daughter_mask |= 1ull << c->rad_bin[q];
+    }
+  }
+  if (memcmp(&want, &m, sizeof(MemberDev)) != 0) {
+    m = want;
+    if (upload_member(c)) return 1;
+  }
+  return 0;
+}
+
 // Wet deposition and radioactive decay after the sweeps (mod_F3D.F90:1497-1520).
+// With the z sweep's epilogue on, only the daughter bins and the kept halo
+// layers are left to k_radio.
 static int enqueue_wet_radio(f3d_ctx* c, double dt) {
   MemberDev& m = c->hm;
-  if (c->wet_on) {
+  if (m.epi_on) {
+    bool daughters = false;
+    for (int p : c->rad_parent) daughters = daughters || p >= 0;
+    if (!c->radio_on || !(daughters || m.gh64 || m.gh32)) return 0;
+  }
+  if (c->wet_on && !m.epi_on) {
     WetArgs a;
     memset(&a, 0, sizeof(a));
     a.nx = c->nx;
@@ -1230,9 +1302,9 @@ static int enqueue_wet_radio(f3d_ctx* c, double dt) {
     for (int q = 0; q < r.nr; ++q) {
       r.bin[q] = c->rad_bin[q];
       r.parent[q] = c->rad_parent[q];
-      r.fact[q] = exp(-c->rad_kn[q] * dt);
-      r.pfact[q] = c->rad_parent[q] >= 0 ? exp(-c->rad_pkn[q] * dt) : 1.0;
     }
+    radio_factors(c->rad_kn, c->rad_pkn, c->rad_parent, dt, r.fact, r.pfact);
+    r.tail = m.epi_on;
     r.c64 = m.c64;
     r.c32 = m.c32;
     r.c32lo = m.c32lo;
@@ -1263,6 +1335,7 @@ static int enqueue_step(f3d_ctx* c, double dt, double time, int iiter) {
     c->hm.gc_cur = gc_on ? 1 : 0;
     if (upload_member(c)) return 1;
   }
+  if (sync_epilogue(c, dt)) return 1;
   launch_set_step(c->dm, 0, dt, time, iiter, c->st);
   c->launches += 1;
   CKL();

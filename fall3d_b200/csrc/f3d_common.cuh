@@ -21,10 +21,18 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 namespace f3d {
 
 constexpr double kEps = 1e-12;  // EPSILON, mod_KindType.F90:42
+
+// The precision form's sweeps address a member's cells and faces within one
+// bin by 32-bit element offsets: (nx+1)(ny+1)(nz+1) must stay below this.
+constexpr long long kMaxPencilSpan = 1LL << 31;
+__host__ __device__ inline bool pencil_span_ok(long long nx, long long ny, long long nz) {
+  return (nx + 1) * (ny + 1) * (nz + 1) < kMaxPencilSpan;
+}
 
 enum Dir { DIR_X = 0, DIR_Y = 1, DIR_Z = 2 };
 
@@ -107,7 +115,97 @@ struct MemberDev {
   float* c32lo;
   const double* rdxb64[3];
   const float2* rdxb2[3];  // the same 1/dxb as an FP32 pair {hi, lo} (~48 bits)
+  // Wet deposition and radioactive decay as the z sweep's epilogue
+  // (mod_F3D.F90:1493-1520; z is the last sweep of a step): as each cell's
+  // final value leaves the march it is scavenged (bins of wet_mask, cells
+  // below the column's ktop) and decayed (radionuclide bins), and the
+  // column's wet and dry deposits are updated by the thread that owns them.
+  // epi_on = 0 leaves both processes to the separate kernels.
+  int epi_on;
+  unsigned long long wet_mask;       // bins that take wet deposition (0: none)
+  double wet_a;                      // lambda = min(1, dt wet_a P^b)
+  const double* powpb;               // P^b per column [j][i]
+  const int* ktop;                   // cells k < ktop of the column are below the PBL top
+  double* awet;                      // wet deposit [bin][j][i] (null without wet deposition)
+  const double* radf;                // this step's {exp(-kn dt)[nr], parent's [nr]}, or null
+  signed char rad_r[64];             // radionuclide index of each bin, -1 for none
+  unsigned long long daughter_mask;  // bins set from their parent after the sweep (Y90)
 };
+
+// Host: whether steps run wet deposition and decay as the z sweep's
+// epilogue (f3d_set_zsweep_epilogue; on by default).
+int zsweep_epilogue();
+
+// The epilogue's per-cell arithmetic, in the order of the separate kernels
+// (phys_wet_deposition, then phys_radionuclides): a cell below the PBL top
+// adds (dX3_p lambda) c to the column's wet deposit and keeps (1 - lambda) c;
+// a radionuclide bin then takes c f.  Every operation is explicitly rounded
+// (no contraction), so the fused and the separate paths agree bit for bit.
+struct ZEpi {
+  double lam;          // wet: min(1, dt a P^b) of the column
+  int kt;              // wet: cells below the PBL top (0: no wet deposition)
+  const double* dx3p;  // dX3_p with the reference offset (kps-2)
+  double aw;           // wet deposit of the column, accumulated in k order
+  double f;            // decay factor of the bin
+  bool dec;            // the bin decays in the epilogue
+  __device__ __forceinline__ double apply(int k, double c) {
+    if (k < kt) {
+      aw = __dadd_rn(aw, __dmul_rn(__dmul_rn(dx3p[k + 2], lam), c));
+      c = __dmul_rn(c, __dsub_rn(1.0, lam));
+    }
+    return dec ? __dmul_rn(c, f) : c;
+  }
+  // the FP32 state: each process rounds its result to FP32, as the separate
+  // kernels store it
+  __device__ __forceinline__ float apply32(int k, float v) {
+    if (k < kt) {
+      const double c = (double)v;
+      aw = __dadd_rn(aw, __dmul_rn(__dmul_rn(dx3p[k + 2], lam), c));
+      v = __double2float_rn(__dmul_rn(c, __dsub_rn(1.0, lam)));
+    }
+    return dec ? __double2float_rn(__dmul_rn((double)v, f)) : v;
+  }
+};
+
+struct NoEpi {};
+
+// Epilogue parameters of bin b of member m for the column at ij (z sweep).
+// A daughter bin (Y90) is overwritten from its parent after the sweep, so its
+// epilogue does nothing.
+__device__ __forceinline__ ZEpi zepi_setup(const MemberDev& m, int b, long long ij) {
+  ZEpi e;
+  e.lam = 0.0;
+  e.kt = 0;
+  e.dx3p = m.dx3p;
+  e.aw = 0.0;
+  e.f = 1.0;
+  e.dec = false;
+  const bool daughter = (m.daughter_mask >> b) & 1ull;
+  if (((m.wet_mask >> b) & 1ull) && !daughter) {
+    const double lam = __dmul_rn(__dmul_rn(m.dt, m.wet_a), m.powpb[ij]);
+    e.lam = lam > 1.0 ? 1.0 : lam;
+    e.kt = m.ktop[ij];
+    e.aw = m.awet[(long long)b * m.nx * m.ny + ij];  // the sum starts from the deposit
+  }
+  const int r = m.rad_r[b];
+  if (m.radf && r >= 0 && !daughter) {
+    e.f = m.radf[r];
+    e.dec = true;
+  }
+  return e;
+}
+
+// The column's deposits after the march: the wet deposit takes the
+// scavenged sum, then both deposits decay with the bin (the dry deposit has
+// already taken this step's flux).
+__device__ __forceinline__ void zepi_finish(const MemberDev& m, const ZEpi& e, int b, long long ij) {
+  const long long q = (long long)b * m.nx * m.ny + ij;
+  if (m.awet && (e.kt > 0 || e.dec)) {
+    const double w = (e.kt > 0) ? e.aw : m.awet[q];
+    m.awet[q] = e.dec ? __dmul_rn(w, e.f) : w;
+  }
+  if (e.dec) m.acum[q] = __dmul_rn(m.acum[q], e.f);
+}
 
 // Precision-form state value of element at (c32, plus c32lo when kept).
 __host__ __device__ __forceinline__ double state32(const MemberDev& m, long long at) {

@@ -40,6 +40,8 @@ struct RadioArgs {
   float* gh32;              // decays the halo cells of the state as well
   long long ngh;            // halo layer elements per bin
   const double* fdev;       // ensemble: the member's {fact[nr], pfact[nr]} in device memory, or null
+  int tail;                 // after the z sweep's epilogue: only the daughters' cells and
+                            // deposits (set from the parent), and every bin's halo layers
 };
 
 // per-species output reductions of nc_IO_out_res (mod_nc_IO.F90:3206-4335)

@@ -116,6 +116,7 @@ struct FusedArgs {
   int* err;
   int bpb;
   long long wait_limit;    // polls before a grid barrier gives up (kSpinLimit by default)
+  int epi;                 // the z phase runs the wet deposition and decay epilogue
 };
 
 }  // namespace f3d

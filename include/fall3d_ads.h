@@ -37,6 +37,8 @@ typedef struct {
 #define F3D_PREC_FP32 1 /* FP32 state and stencil; FP64 deposit, budget, CFL */
 #define F3D_PREC_FP32C 2 /* FP32 stencil on a compensated state: FP32 pair hi + lo
                             (~48 bits), conservative FP64 final update per cell */
+/* The two precision forms address a bin's cells with 32-bit offsets: their
+ * grids need (nx+1)(ny+1)(nz+1) < 2^31 (creation fails otherwise). */
 
 /* Limiters (mod_Phys.F90:58-61) and time marching (mod_Phys.F90:64-65). */
 #define F3D_LIMITER_MINMOD 1
@@ -329,6 +331,17 @@ int f3d_set_wait_limit(long long polls);
  * calls; a point that has not converged within it returns flag 2
  * (mod_Phys.F90:944-948).  maxit = -1 restores 1000. */
 int f3d_set_vset_maxit(int maxit);
+/* Process-wide choice of how the steps run wet deposition and radioactive
+ * decay (phys_wet_deposition and phys_radionuclides after the sweeps,
+ * mod_F3D.F90:1493-1520).  on = 1 (the default): as the z sweep's epilogue,
+ * each cell scavenged and decayed as it leaves the sweep and the column's
+ * deposits updated by the thread that owns them, with a separate pass left
+ * only for Y90 bins (set from their Sr90 parent) and the kept boundary halo
+ * layers.  on = 0: as separate passes over the state after the z sweep.
+ * The exact form gives the same bits either way; the compensated precision
+ * form rounds the pair once instead of after each process.  Takes effect at
+ * the next step (an ensemble re-captures its step graphs). */
+int f3d_set_zsweep_epilogue(int on);
 
 /* Mass in the volume for callers that cannot allocate device memory.  No
  * counterpart in the reference: a variant of f3d_ads_mass_volume for code

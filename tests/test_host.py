@@ -100,6 +100,11 @@ def test_capi_rejects_bad_arguments_without_gpu(built_lib):
     d = F3DDims(4, 4, 4, 2)
     assert lib().f3d_ads_create(C.byref(d), 9, 2, 0, 0, C.byref(h)) == 1
     assert "limiter" in last_error()
+    # the precision forms' 32-bit pencil offsets: (nx+1)(ny+1)(nz+1) < 2^31
+    d = F3DDims(2000, 2000, 600, 2)
+    for prec in (1, 2):
+        assert lib().f3d_ads_create(C.byref(d), 2, 2, prec, 0, C.byref(h)) == 1
+        assert "2^31" in last_error()
 
 
 def test_partition_members_balances_load():
