@@ -216,10 +216,10 @@ def run_aux(args, local):
     ms["step_plain"] = round(ms["step_plain"] / K, 4)
     dom.phys_wet_deposition(8.4e-5, 0.79, pre, pblh, cat, wl.diam)
     dom.phys_radionuclides(cat, spe)
-    set_zsweep_epilogue(False)  # separate passes after the z sweep
-    timed("step_wet_decay_separate", steps)
-    ms["step_wet_decay_separate"] = round(ms["step_wet_decay_separate"] / K, 4)
-    set_zsweep_epilogue(True)  # the default: inside the z sweep
+    set_zsweep_epilogue(True)  # inside the z sweep
+    timed("step_wet_decay_zsweep_epilogue", steps)
+    ms["step_wet_decay_zsweep_epilogue"] = round(ms["step_wet_decay_zsweep_epilogue"] / K, 4)
+    set_zsweep_epilogue(False)  # the default: separate passes after the z sweep
     timed("step_wet_decay", steps)
     ms["step_wet_decay"] = round(ms["step_wet_decay"] / K, 4)
     dom.set_gravity_current(g.lon_p[g.nx // 2], g.lat_p[g.ny // 2], -3600.0, 1e9, 430.0, 0.1, 0.02, 0.2, 1e6,

@@ -418,8 +418,8 @@ def set_vset_maxit(maxit: int):
 
 
 def set_zsweep_epilogue(on: bool = True):
-    """Wet deposition and decay inside the z sweep (True, the default) or
-    as separate passes after it (f3d_set_zsweep_epilogue)."""
+    """Wet deposition and decay inside the z sweep (True) or as separate
+    passes after it (False, the library's default; f3d_set_zsweep_epilogue)."""
     check(lib().f3d_set_zsweep_epilogue(int(bool(on))), "f3d_set_zsweep_epilogue")
 
 

@@ -98,9 +98,6 @@ __device__ __forceinline__ float half_phid(float d1, float d0) {
 #ifndef F3D_PF_L2
 #define F3D_PF_L2 0
 #endif
-#ifndef F3D_Z_EDGE_CMP
-#define F3D_Z_EDGE_CMP 1
-#endif
 // Element offsets along a pencil (p * stride within one bin of one member,
 // and the face offsets likewise): 32-bit, which cuts the index arithmetic of
 // the sweeps (4-9% faster); the hosts accept precision-form grids only while
@@ -112,9 +109,6 @@ __device__ __forceinline__ float half_phid(float d1, float d0) {
 typedef int pstride_t;
 #else
 typedef long long pstride_t;
-#endif
-#ifndef F3D_Z_EDGE_PLAIN
-#define F3D_Z_EDGE_PLAIN 0
 #endif
 __device__ __forceinline__ void prefetch_line(const void* p) {
   if (F3D_PF_L2) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
@@ -143,11 +137,6 @@ struct Ops32 {
   // x pencils: shared-memory staging of the rows (the compensated form also
   // stages the low part, in narrower chunks so that both tiles fit)
   static constexpr int XW = CMP ? F3D_CMP_XW : 32;
-  // z pencils are short (tens of levels): the head, steady and edge bodies
-  // all run within a few blocks of each other; with kEdgeOnly the march
-  // runs the edge body for every block after the head, a smaller code
-  // footprint at a higher cost per step
-  static constexpr bool kEdgeOnly = (DIR == DIR_Z) && (CMP ? F3D_Z_EDGE_CMP : F3D_Z_EDGE_PLAIN);
   XTile<float, (TM == 2) ? 1 : 2, XW> xt;
   XLoTile<XW> lt;
   // EPI (z): the column's wet deposition and decay (an empty struct otherwise)

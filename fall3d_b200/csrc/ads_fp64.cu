@@ -60,7 +60,6 @@ struct Ops64 {
   double dt, hdt;
   XTile<double> xt;    // x pencils: shared-memory staging of the rows
   ZEpi epi;            // EPI: the column's wet deposition and decay
-  static constexpr bool kEdgeOnly = false;
 
   __device__ __forceinline__ double load_c(int p) const {
     if constexpr (DIR == DIR_X) {

@@ -247,7 +247,7 @@ namespace f3d {
 constexpr long long kDefaultWaitLimit = 1LL << 25;  // = kSpinLimit (step_dev.cuh)
 static std::atomic<long long> g_wait_limit{kDefaultWaitLimit};
 static std::atomic<int> g_vset_maxit{1000};
-static std::atomic<int> g_zepi{1};
+static std::atomic<int> g_zepi{0};
 long long wait_limit() { return g_wait_limit.load(); }
 int vset_maxit() { return g_vset_maxit.load(); }
 int zsweep_epilogue() { return g_zepi.load(); }

@@ -539,7 +539,7 @@ struct March {
 #pragma unroll 1
     for (int T0 = 8; T0 <= t_last; T0 += 8) {
       o.stage_begin(T0);
-      if (!Ops::kEdgeOnly && T0 + 7 <= n - 2) {
+      if (T0 + 7 <= n - 2) {
         block8<false>(T0);  // interior: the steady body
       } else {
         iter_v<0>(T0);

@@ -333,14 +333,16 @@ int f3d_set_wait_limit(long long polls);
 int f3d_set_vset_maxit(int maxit);
 /* Process-wide choice of how the steps run wet deposition and radioactive
  * decay (phys_wet_deposition and phys_radionuclides after the sweeps,
- * mod_F3D.F90:1493-1520).  on = 1 (the default): as the z sweep's epilogue,
- * each cell scavenged and decayed as it leaves the sweep and the column's
- * deposits updated by the thread that owns them, with a separate pass left
- * only for Y90 bins (set from their Sr90 parent) and the kept boundary halo
- * layers.  on = 0: as separate passes over the state after the z sweep.
- * The exact form gives the same bits either way; the compensated precision
- * form rounds the pair once instead of after each process.  Takes effect at
- * the next step (an ensemble re-captures its step graphs). */
+ * mod_F3D.F90:1493-1520).  on = 0 (the default): as separate passes over the
+ * state after the z sweep.  on = 1: as the z sweep's epilogue, each cell
+ * scavenged and decayed as it leaves the sweep and the column's deposits
+ * updated by the thread that owns them, with a separate pass left only for
+ * Y90 bins (set from their Sr90 parent) and the kept boundary halo layers.
+ * The exact and plain FP32 forms give the same bits either way; the
+ * compensated form rounds its pair once instead of after each process.  The
+ * epilogue saves the passes' memory traffic but adds FP64 arithmetic to the
+ * issue-bound sweep, and measured slower on a B200.  Takes effect at the
+ * next step (an ensemble re-captures its step graphs). */
 int f3d_set_zsweep_epilogue(int on);
 
 /* Mass in the volume for callers that cannot allocate device memory.  No

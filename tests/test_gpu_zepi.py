@@ -9,8 +9,8 @@ plain FP32 form must agree bit for bit: concentration (halo layers included),
 dry and wet deposits, in the single domain and in every member of an
 ensemble in both execution modes.  The compensated form rounds its pair once
 after both processes instead of after each, so it agrees to ~2^-42 of the field's magnitude.
-The oracle comparisons of the wet-deposition tests run the epilogue (the
-default) against the reference's order of whole passes.
+The oracle comparisons of the wet-deposition tests run the separate passes
+(the default); equality with them carries the oracle's bits to the epilogue.
 """
 import numpy as np
 import pytest
@@ -27,7 +27,7 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture
 def restore_epilogue():
     yield
-    set_zsweep_epilogue(True)
+    set_zsweep_epilogue(False)
 
 
 def _domain_run(oracle_mod, precision, fused, keep_halo, nsteps=4, dt=40.0):
