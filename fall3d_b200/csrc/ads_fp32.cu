@@ -209,12 +209,6 @@ struct Ops32 {
   __device__ __forceinline__ float rk_full(float c, float k) const { return fmaf(dt, k, c); }
   __device__ __forceinline__ float rk_final(float nw, float k) const { return fmaf(dt6, k, nw); }
 
-  // Compensated final update of cell p (CMP): c(p) = hi + lo advanced by
-  // dtf (H(p+1) - H(p)) / dxb(p) and split back into hi + lo.  The difference of
-  // the two FP32 face sums is formed exactly and 1/dxb carries ~48 bits, so
-  // the cell's change times its volume is the two face sums it shares with
-  // its neighbours to ~2^-47: the sweep conserves mass to ~1e-14 of the
-  // transported mass, and the state carries ~48 bits.
   // low part of cell p (y, z: global, with an L1 prefetch of a later cell's
   // line; x: the staged tile)
   __device__ __forceinline__ float lo_fetch(int p) {
@@ -229,6 +223,12 @@ struct Ops32 {
     if constexpr (DIR == DIR_X) lt.at(p) = v;
     else lop[(pstride_t)p * cs] = v;
   }
+  // Compensated final update of cell p (CMP): c(p) = hi + lo advanced by
+  // dtf (H(p+1) - H(p)) / dxb(p) and split back into hi + lo.  The difference of
+  // the two FP32 face sums is formed exactly and 1/dxb carries ~48 bits, so
+  // the cell's change times its volume is the two face sums it shares with
+  // its neighbours to ~2^-47: the sweep conserves mass to ~1e-14 of the
+  // transported mass, and the state carries ~48 bits.
   __device__ __forceinline__ float final_cmp(float chi, float clo, float hl, float hr, int p) {
 #if F3D_CMP_EFT
     // In FP32 pair arithmetic (error-free transformations; every operation
