@@ -22,6 +22,16 @@
 #ifndef F3D_V64
 #define F3D_V64 1
 #endif
+// Element offsets along a pencil within one bin: 32-bit with F3D_STRIDE32_64
+// (grids with (nx+1)(ny+1)(nz+1) < 2^31), else 64-bit.
+#ifndef F3D_STRIDE32_64
+#define F3D_STRIDE32_64 0
+#endif
+#if F3D_STRIDE32_64
+typedef int pstride64_t;
+#else
+typedef long long pstride64_t;
+#endif
 
 namespace f3d {
 
@@ -50,10 +60,10 @@ __device__ __forceinline__ double limiter64(double d1, double d0) {
 template <int LIM, int DIR, bool EPI = false>
 struct Ops64 {
   double* cp;
-  long long cs;
+  pstride64_t cs;
   const double* vel;   // current face velocity, face f at vel[f * vs]
   const double* vsub;  // z: settling velocity of the bin at the same faces
-  long long vs;
+  pstride64_t vs;
   const double* kk;    // 0.5 (k(f) + k(f-1)) at face f, same stride
   const double4* geo;  // {dxp(p), 1/dxp(p), dxb(p), 1/dxb(p)} at geo[p + 1]
   int nf;              // cells of the pencil (faces 0..nf)
@@ -66,11 +76,11 @@ struct Ops64 {
       return xt.load(p);
     } else {
       // the line of a later position into L1 ahead of its load
-      if (F3D_PF64) asm volatile("prefetch.global.L1 [%0];" ::"l"(cp + (long long)min(p + 8, nf - 1) * cs));
+      if (F3D_PF64) asm volatile("prefetch.global.L1 [%0];" ::"l"(cp + (pstride64_t)min(p + 8, nf - 1) * cs));
       return cp[p * cs];
     }
   }
-  __device__ __forceinline__ double load_last() const { return cp[(long long)(nf - 1) * cs]; }
+  __device__ __forceinline__ double load_last() const { return cp[(pstride64_t)(nf - 1) * cs]; }
   __device__ __forceinline__ void store_c(int p, double v) {
     if constexpr (DIR == DIR_X) xt.store(p, v);
     else if constexpr (EPI) cp[p * cs] = epi.apply(p, v);
@@ -82,7 +92,7 @@ struct Ops64 {
   __device__ __forceinline__ void stage_finish() { if constexpr (DIR == DIR_X) xt.finish(); }
   __device__ __forceinline__ FaceV<double> face(int f) const {
     if (F3D_PF64) {
-      const long long fp = (long long)min(f + 8, nf) * vs;
+      const pstride64_t fp = (pstride64_t)min(f + 8, nf) * vs;
       asm volatile("prefetch.global.L1 [%0];" ::"l"(vel + fp));
       asm volatile("prefetch.global.L1 [%0];" ::"l"(kk + fp));
       if (DIR == DIR_Z) asm volatile("prefetch.global.L1 [%0];" ::"l"(vsub + fp));
@@ -208,11 +218,11 @@ __device__ __forceinline__ void sweep64_pencil(const MemberDev& m, long long pen
     j = (int)(pen / nx);
     n = nz;
     o.cp = m.c64 + (long long)b * nz * ny * nx + (long long)j * nx + i;
-    o.cs = (long long)nx * ny;
+    o.cs = (pstride64_t)nx * ny;
     long long fo = (long long)j * nx + i;
     o.vel = m.wcur + fo;
     o.kk = m.kkf[2] + fo;
-    o.vs = (long long)nx * ny;
+    o.vs = (pstride64_t)nx * ny;
     o.vsub = m.vs + (long long)b * (nz + 1) * ny * nx + fo;
     area = m.dx2b[j + 1] * m.dx1b[i + 1];
     if constexpr (EPI) o.epi = zepi_setup(m, b, fo);
@@ -280,8 +290,13 @@ __global__ void __launch_bounds__(128, F3D_FP64_MINB) k_sweep64(const MemberDev*
   extern __shared__ __align__(16) unsigned char f3d_smem[];
   sweep64_item<DIR, LIM, TM, EPI>(members, work[blockIdx.x], bpb, f3d_smem);
 }
+#ifdef F3D_FP64_XMINB
+#define F3D_SWEEP64X_BOUNDS __launch_bounds__(128, F3D_FP64_XMINB)
+#else
+#define F3D_SWEEP64X_BOUNDS __launch_bounds__(128)
+#endif
 template <int LIM, int TM>
-__global__ void __launch_bounds__(128) k_sweep64x(const MemberDev* __restrict__ members,
+__global__ void F3D_SWEEP64X_BOUNDS k_sweep64x(const MemberDev* __restrict__ members,
                                                   const WorkItem* __restrict__ work, int bpb) {
   extern __shared__ __align__(16) unsigned char f3d_smem[];
   sweep64_item<DIR_X, LIM, TM>(members, work[blockIdx.x], bpb, f3d_smem);
