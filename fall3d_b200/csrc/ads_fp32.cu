@@ -634,7 +634,10 @@ __device__ __noinline__ void sweep32_item_call(MemberDev* members, WorkItem w, i
 // themselves) and meet at bounded grid barriers between phases.  Launched
 // cooperatively so that every block is resident.
 template <int LIM, int TM, bool CMP>
-__global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
+#ifndef F3D_FUSED32_BLOCKS
+#define F3D_FUSED32_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(128, F3D_FUSED32_BLOCKS) k_fused32(FusedArgs a) {
   extern __shared__ __align__(16) unsigned char f3d_smem[];
   __shared__ int slot;
   __shared__ double sa[128], sb[128];
@@ -661,9 +664,13 @@ __global__ void __launch_bounds__(128, 3) k_fused32(FusedArgs a) {
   }
 }
 
-int fused32_smem() {
-  return 4 * std::max(XTile<float, 2>::BYTES,
-                      XTile<float, 2, F3D_CMP_XW>::BYTES + XLoTile<F3D_CMP_XW>::BYTES);
+// Dynamic shared memory of the persistent kernel: the x sweep's staging of
+// this time marching and form, for the 4 warps of a block.
+int fused32_smem(int tm, int cmp) {
+  if (cmp)
+    return 4 * ((tm == 2 ? XTile<float, 1, F3D_CMP_XW>::BYTES : XTile<float, 2, F3D_CMP_XW>::BYTES) +
+                XLoTile<F3D_CMP_XW>::BYTES);
+  return 4 * (tm == 2 ? XTile<float, 1>::BYTES : XTile<float, 2>::BYTES);
 }
 
 template <bool CMP>

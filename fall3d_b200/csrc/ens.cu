@@ -74,7 +74,7 @@ void launch_set_steps(MemberDev* members, int n, const double* dt, const double*
 void launch_advance_clock(MemberDev* members, int n, cudaStream_t st);
 void launch_finalize_dt(MemberDev* members, int n, const double* red, double cfl, double run_end,
                         cudaStream_t st);
-int fused32_smem();
+int fused32_smem(int tm, int cmp);
 int fused64_smem();
 const void* fused32_func(int lim, int tm, int cmp);
 const void* fused64_func(int lim, int tm);
@@ -1013,7 +1013,7 @@ namespace {
 int fused_setup(f3d_ens* e, const void** func, int* smem) {
   const bool f32 = e->prec == F3D_PREC_FP32;
   *func = f32 ? fused32_func(e->lim, e->tm, e->cmp) : fused64_func(e->lim, e->tm);
-  *smem = f32 ? fused32_smem() : fused64_smem();
+  *smem = f32 ? fused32_smem(e->tm, e->cmp) : fused64_smem();
   ECK(cudaFuncSetAttribute(*func, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem));
   int per_sm = 0;
   ECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, *func, 128, *smem));
