@@ -7,6 +7,7 @@ Run: python -m fall3d_b200.build  (or call build()).
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -60,11 +61,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nv = nvcc()
     common = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-I" + os.path.join(HERE, "..", "include")]
-    for (f, fl), o in zip(present, objs):
-        cmd = [nv, "-c", os.path.join(CSRC, f), "-o", o] + common + fl
-        if verbose:
+    cmds = [[nv, "-c", os.path.join(CSRC, f), "-o", o] + common + fl for (f, fl), o in zip(present, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+    # the translation units are independent: compile them side by side
+    # (the two sweep files take minutes each)
+    workers = max(1, min(len(cmds), os.cpu_count() or 1))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=workers) as pool:
+        for r in pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args, r.stdout, r.stderr)
     tmp = LIB + ".tmp"
     cmd = [nv, "-shared", "-o", tmp] + objs + ARCH + ["-cudart=static"]
     if verbose:
