@@ -95,6 +95,12 @@ __device__ __forceinline__ float half_phid(float d1, float d0) {
 #ifndef F3D_C_PF
 #define F3D_C_PF 8
 #endif
+#ifndef F3D_C_PF_Z
+#define F3D_C_PF_Z F3D_C_PF
+#endif
+#ifndef F3D_FACE_PF_Z
+#define F3D_FACE_PF_Z F3D_FACE_PF
+#endif
 #ifndef F3D_PF_L2
 #define F3D_PF_L2 0
 #endif
@@ -146,7 +152,8 @@ struct Ops32 {
     if constexpr (DIR == DIR_X) {
       return xt.load(p);
     } else {
-      if constexpr (F3D_C_PF > 0) prefetch_line(cp + (pstride_t)min(p + F3D_C_PF, nf - 1) * cs);
+      constexpr int pf = (DIR == DIR_Z) ? F3D_C_PF_Z : F3D_C_PF;
+      if constexpr (pf > 0) prefetch_line(cp + (pstride_t)min(p + pf, nf - 1) * cs);
       return cp[p * cs];
     }
   }
@@ -173,8 +180,9 @@ struct Ops32 {
     if constexpr (DIR == DIR_X && CMP) lt.finish();
   }
   __device__ __forceinline__ FaceV<float> face(int f) const {
-    if constexpr (F3D_FACE_PF > 0) {
-      const pstride_t fp = (pstride_t)min(f + F3D_FACE_PF, nf) * vs;
+    constexpr int fpf = (DIR == DIR_Z) ? F3D_FACE_PF_Z : F3D_FACE_PF;
+    if constexpr (fpf > 0) {
+      const pstride_t fp = (pstride_t)min(f + fpf, nf) * vs;
       prefetch_line(fd + fp);
       if constexpr (DIR == DIR_Z) prefetch_line(vsub + fp);
     }

@@ -17,6 +17,10 @@
 #include "f3d_common.cuh"
 #endif
 
+#ifndef F3D_HALF_TAIL
+#define F3D_HALF_TAIL 0
+#endif
+
 namespace f3d {
 
 template <class T>
@@ -546,10 +550,14 @@ struct March {
         iter_v<1>(T0 + 1);
         iter_v<2>(T0 + 2);
         iter_v<3>(T0 + 3);
-        iter_v<4>(T0 + 4);
-        iter_v<5>(T0 + 5);
-        iter_v<6>(T0 + 6);
-        iter_v<7>(T0 + 7);
+        // the last block stops at t_last when that is in its first half
+        // (steps past t_last store nothing; n is warp-uniform)
+        if (!F3D_HALF_TAIL || T0 + 4 <= t_last) {
+          iter_v<4>(T0 + 4);
+          iter_v<5>(T0 + 5);
+          iter_v<6>(T0 + 6);
+          iter_v<7>(T0 + 7);
+        }
       }
       o.stage_end(T0);
     }
