@@ -17,6 +17,8 @@
 #include "f3d_common.cuh"
 #endif
 
+// F3D_HALF_TAIL: the last block of the RK4 V march skips its second half
+// when t = n + 7 falls in the first (on in the precision form's sweeps).
 #ifndef F3D_HALF_TAIL
 #define F3D_HALF_TAIL 0
 #endif
