@@ -279,6 +279,20 @@ def load_traffic(kernel: str, workload: str, algorithmic: float = None):
         return None
 
 
+def traffic_source(kernel: str, workload: str) -> str:
+    """Where load_traffic's figure for this kernel and workload comes from."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            direct = kernel in json.load(f).get(workload, {})
+    except Exception:
+        direct = False
+    if direct:
+        return ("ncu DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of this "
+                "kernel on the same workload")
+    return ("ncu DRAM bytes of the same kernel on the 400x300x60x20 case, as a ratio to its "
+            "algorithmic bytes, times this launch's algorithmic bytes")
+
+
 def setup_domain(wl, prec, device):
     from fall3d_b200.ads import Domain
     dom = Domain(wl.grid, wl.nbins, wl.limiter, wl.time_marching, prec, device=device)
@@ -733,8 +747,7 @@ def ens_roofline(r, K):
     return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": kind,
             "traffic": load_traffic(tkey, "ensemble", byts), "algorithmic_bytes": byts,
-            "traffic_source": "ncu DRAM bytes of the same kernel on the 400x300x60x20 case, "
-                              "as a ratio to its algorithmic bytes, times this launch's algorithmic bytes",
+            "traffic_source": traffic_source(tkey, "ensemble"),
             "launch_ms": round(t, 3),
             "phase_ms": {k: round(float(v), 3) for k, v in zip(("prep", "x", "y", "z", "flux"), per)}}
 
